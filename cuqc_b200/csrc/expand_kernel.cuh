@@ -1,0 +1,1020 @@
+// expand_kernel.cuh -- persistent branch-and-bound expansion (device code).
+//
+// One warp works on one work item at a time: a task (a node of the
+// set-enumeration tree) or a range of its branches.  A task carries its own
+// induced adjacency as bit matrices, so every degree in the reference's
+// rules becomes popc(row & mask) over ceil(t/32) words instead of a binary
+// search in the global CSR (reference: d_bsearch_array, main.cu:4339).
+//
+// Rules implemented (plain set semantics of the reference's host routines;
+// each function names the routine it follows):
+//   lookahead            main.cu:1349-1405 / 3405-3471
+//   remove-one threshold main.cu:1408-1462 / 3474-3515
+//   add one + diameter   main.cu:1465-1523, 1709-1732
+//   degree pruning       main.cu:1735-1855
+//   lower/upper bounds   main.cu:1857-1972
+//   critical vertices    main.cu:1526-1707
+//   clique check         main.cu:1974-1995
+//   Q enumeration order  main.cu:2059-2104
+//   validity tests       main.cu:2144-2198
+// The scheduler (a LIFO stack of work items with atomics, bounded waits and
+// an outstanding-work counter) replaces the reference's host level loop,
+// transfer_buffers and fill_from_buffer (main.cu:606-678, 3251-3398).
+#pragma once
+#include "qc_device.h"
+
+namespace qcb {
+
+#define QC_FULL 0xffffffffu
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ int wsum(int x)
+{
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(QC_FULL, x, o);
+    return x;
+}
+__device__ __forceinline__ long long wsum64(long long x)
+{
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(QC_FULL, x, o);
+    return x;
+}
+__device__ __forceinline__ int wmin(int x)
+{
+    for (int o = 16; o; o >>= 1) {
+        int y = __shfl_xor_sync(QC_FULL, x, o);
+        x = y < x ? y : x;
+    }
+    return x;
+}
+__device__ __forceinline__ int wmax(int x)
+{
+    for (int o = 16; o; o >>= 1) {
+        int y = __shfl_xor_sync(QC_FULL, x, o);
+        x = y > x ? y : x;
+    }
+    return x;
+}
+// inclusive prefix sum across lanes
+__device__ __forceinline__ int wscan(int x)
+{
+    int lane = lane_id();
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(QC_FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+__device__ __forceinline__ long long wscan64(long long x)
+{
+    int lane = lane_id();
+    for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(QC_FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+__device__ __forceinline__ bool bit(const uint32_t* a, int v) { return (a[v >> 5] >> (v & 31)) & 1u; }
+
+__device__ __forceinline__ int popc_and(const uint32_t* row, const uint32_t* mask, int W)
+{
+    int s = 0;
+    for (int w = 0; w < W; w++) s += __popc(row[w] & mask[w]);
+    return s;
+}
+
+// warp-cooperative bitset helpers over W words
+__device__ __forceinline__ void bs_copy(uint32_t* d, const uint32_t* s, int W)
+{
+    for (int w = lane_id(); w < W; w += 32) d[w] = s[w];
+    __syncwarp();
+}
+__device__ __forceinline__ void bs_zero(uint32_t* d, int W)
+{
+    for (int w = lane_id(); w < W; w += 32) d[w] = 0;
+    __syncwarp();
+}
+// d = bits [lo, hi)
+__device__ __forceinline__ void bs_range(uint32_t* d, int W, int lo, int hi)
+{
+    for (int w = lane_id(); w < W; w += 32) {
+        int b0 = w * 32;
+        uint32_t x = 0;
+        for (int k = 0; k < 32; k++) {
+            int v = b0 + k;
+            if (v >= lo && v < hi) x |= 1u << k;
+        }
+        d[w] = x;
+    }
+    __syncwarp();
+}
+__device__ __forceinline__ int bs_count(const uint32_t* a, int W)
+{
+    int s = 0;
+    for (int w = lane_id(); w < W; w += 32) s += __popc(a[w]);
+    return wsum(s);
+}
+__device__ __forceinline__ bool bs_empty(const uint32_t* a, int W)
+{
+    int nz = 0;
+    for (int w = lane_id(); w < W; w += 32) nz |= (a[w] != 0);
+    return !__any_sync(QC_FULL, nz);
+}
+
+// ------------------------------------------------------------------
+// per-warp state
+// ------------------------------------------------------------------
+
+struct TaskView {
+    int t, m, cov, W;
+    const int32_t* ids;
+    int32_t* l2;
+    const uint32_t* A1;
+    const uint32_t* A2;
+    unsigned long long rec;
+};
+
+__device__ __forceinline__ TaskView task_view(char* arena, unsigned long long rec)
+{
+    TaskView T;
+    const TaskHdr* h = (const TaskHdr*)(arena + rec);
+    T.t = h->t;
+    T.m = h->m;
+    T.cov = h->cov;
+    T.W = h->W;
+    T.ids = (const int32_t*)(arena + rec + rec_ids_off());
+    T.l2 = (int32_t*)(arena + rec + rec_l2_off(T.t));
+    T.A1 = (const uint32_t*)(arena + rec + rec_a1_off(T.t));
+    T.A2 = (const uint32_t*)(arena + rec + rec_a2_off(T.t, T.W));
+    T.rec = rec;
+    return T;
+}
+
+struct Ws {
+    int32_t* indeg;
+    int32_t* exdeg;
+    int32_t* aux;
+    int32_t* hist;
+    int32_t* pcnt;
+    long long* psum;
+    int32_t* sel;
+    unsigned long long* khi;
+    unsigned long long* klo;
+    uint32_t* mk[12];
+};
+
+__device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global)
+{
+    WsLayout L = ws_layout(P.max_t);
+    char* b = P.ws + (int64_t)warp_global * P.ws_stride;
+    Ws w;
+    w.indeg = (int32_t*)(b + L.indeg);
+    w.exdeg = (int32_t*)(b + L.exdeg);
+    w.aux = (int32_t*)(b + L.aux);
+    w.hist = (int32_t*)(b + L.hist);
+    w.pcnt = (int32_t*)(b + L.pref_cnt);
+    w.psum = (long long*)(b + L.pref_sum);
+    w.sel = (int32_t*)(b + L.sel);
+    w.khi = (unsigned long long*)(b + L.key_hi);
+    w.klo = (unsigned long long*)(b + L.key_lo);
+    int Wm = words_for(P.max_t) + 2;
+    uint32_t* m0 = (uint32_t*)(b + L.masks);
+    for (int i = 0; i < 12; i++) w.mk[i] = m0 + (int64_t)i * Wm;
+    return w;
+}
+
+// mask slots
+enum { MK_M = 0, MK_C = 1, MK_PRE = 2, MK_D = 3, MK_R = 4, MK_X = 5, MK_K = 6, MK_CA = 7,
+       MK_T = 8, MK_U = 9 };
+
+struct Bounds {
+    int U, L, med;
+};
+
+// ------------------------------------------------------------------
+// gamma tables (main.cu:526-533, 2144-2151)
+// ------------------------------------------------------------------
+
+__device__ __forceinline__ int md_at(const ExpandParams& P, int k)
+{
+    k = k < 0 ? 0 : k;
+    k = k >= P.mdlen ? P.mdlen - 1 : k;
+    return P.md[k];
+}
+__device__ __forceinline__ int mindeg(const ExpandParams& P, int k)
+{
+    return md_at(P, k < P.min_size ? P.min_size : k);
+}
+__device__ __forceinline__ int ubt_at(const ExpandParams& P, int d)
+{
+    d = d < 0 ? 0 : d;
+    d = d >= P.mdlen ? P.mdlen - 1 : d;
+    return P.ubt[d];
+}
+
+// main.cu:2167-2178
+__device__ __forceinline__ bool cand_valid(const ExpandParams& P, int in, int ex, int m,
+                                           const Bounds& b)
+{
+    int tot = in + ex;
+    if (tot < md_at(P, P.min_size)) return false;
+    if (tot < mindeg(P, m + ex + 1)) return false;
+    if (tot < b.med) return false;
+    if (in + b.U - 1 < md_at(P, m + b.L)) return false;
+    if (tot < mindeg(P, m + b.L)) return false;
+    return true;
+}
+// main.cu:2180-2198
+__device__ __forceinline__ bool vert_extendable(const ExpandParams& P, int in, int ex, int m,
+                                                const Bounds& b)
+{
+    int tot = in + ex;
+    if (tot < md_at(P, P.min_size)) return false;
+    if (tot < mindeg(P, m + ex)) return false;
+    if (tot < b.med) return false;
+    if (ex == 0 && in < mindeg(P, m + ex)) return false;
+    if (in + b.U < md_at(P, m + b.U)) return false;
+    if (tot < mindeg(P, m + b.L)) return false;
+    return true;
+}
+
+// ------------------------------------------------------------------
+// candidate indegree histogram -> S(k) = sum of the k largest
+// ------------------------------------------------------------------
+
+// Build the histogram of indeg over the vertices in mask `cm` (optionally
+// only those passing validity under `b`), then prefix tables over bins in
+// descending value order: pcnt[j] = #values > vmax-j, psum[j] = their sum.
+// Values are bounded by vmax (members count).  Returns the number of values.
+__device__ int build_hist(const ExpandParams& P, Ws& ws, const uint32_t* cm, int t, int vmax,
+                          bool filter_valid, int m, const Bounds& b)
+{
+    int lane = lane_id();
+    for (int j = lane; j <= vmax + 1; j += 32) ws.hist[j] = 0;
+    __syncwarp();
+    int cnt = 0;
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        if (v < t && bit(cm, v)) {
+            int in = ws.indeg[v];
+            if (!filter_valid || cand_valid(P, in, ws.exdeg[v], m, b)) {
+                int j = vmax - (in > vmax ? vmax : in);
+                atomicAdd(&ws.hist[j], 1);
+                cnt++;
+            }
+        }
+    }
+    __syncwarp();
+    // exclusive prefix over bins 0..vmax+1
+    int carry = 0;
+    long long carry_s = 0;
+    for (int base = 0; base <= vmax + 1; base += 32) {
+        int j = base + lane;
+        int c = (j <= vmax + 1) ? ws.hist[j] : 0;
+        long long s = (j <= vmax) ? (long long)c * (vmax - j) : 0;
+        int ic = wscan(c);
+        long long is = wscan64(s);
+        if (j <= vmax + 1) {
+            ws.pcnt[j] = carry + ic - c;
+            ws.psum[j] = carry_s + is - s;
+        }
+        carry += __shfl_sync(QC_FULL, ic, 31);
+        carry_s += __shfl_sync(QC_FULL, is, 31);
+    }
+    __syncwarp();
+    return wsum(cnt);
+}
+
+// sum of the k largest values (0 <= k <= total)
+__device__ __forceinline__ long long top_sum(const Ws& ws, int vmax, int k)
+{
+    // largest bin j in [0, vmax+1] with pcnt[j] <= k
+    int lo = 0, hi = vmax + 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (ws.pcnt[mid] <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    if (lo > vmax) return ws.psum[vmax + 1];
+    return ws.psum[lo] + (long long)(k - ws.pcnt[lo]) * (vmax - lo);
+}
+
+// ------------------------------------------------------------------
+// lower / upper bounds (main.cu:1857-1972).  Members: mask mm (m of them).
+// The candidate histogram must be built.  Returns true when invalid.
+// ------------------------------------------------------------------
+
+__device__ bool lu_bounds(const ExpandParams& P, Ws& ws, const uint32_t* mm, int t, int m,
+                          int ncand, int vmax, Bounds& b)
+{
+    int lane = lane_id();
+    int mi = 0x7fffffff, mt = 0x7fffffff;
+    long long si = 0;
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        if (v < t && bit(mm, v)) {
+            int in = ws.indeg[v], ex = ws.exdeg[v];
+            mi = in < mi ? in : mi;
+            mt = in + ex < mt ? in + ex : mt;
+            si += in;
+        }
+    }
+    int min_in = wmin(mi);
+    int min_tot = wmin(mt);
+    long long sum_in = wsum64(si);
+    int me = 0x7fffffff;
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        if (v < t && bit(mm, v) && ws.indeg[v] == min_in) {
+            int ex = ws.exdeg[v];
+            me = ex < me ? ex : me;
+        }
+    }
+    int min_in_ex = wmin(me);
+
+    bool invalid = false;
+    b.med = mindeg(P, m + 1);
+    if (min_in < md_at(P, m)) {
+        int lb = mindeg(P, m) - min_in;
+        // first L >= lb with !(L <= min_in_ex && min_in + L < md[m+L])
+        for (int base = lb;; base += 32) {
+            int L = base + lane;
+            bool cont = (L <= min_in_ex) && (min_in + L < md_at(P, m + L));
+            unsigned stop = __ballot_sync(QC_FULL, !cont);
+            if (stop) {
+                lb = base + __ffs(stop) - 1;
+                break;
+            }
+        }
+        if (min_in + lb < md_at(P, m + lb)) {
+            lb = ncand + 1;
+            invalid = true;
+        }
+        int ub = ubt_at(P, min_tot) + 1 - m;
+        if (ub > ncand) ub = ncand;
+        if (lb < ub) {
+            // first k in [lb, ub] with k == ub || sum_in + S(k) >= m*md[m+k]
+            int idx = ub;
+            for (int base = lb; base <= ub; base += 32) {
+                int k = base + lane;
+                bool ok = false;
+                if (k <= ub) {
+                    ok = (k == ub) ||
+                         (sum_in + top_sum(ws, vmax, k) >= (long long)m * md_at(P, m + k));
+                }
+                unsigned bal = __ballot_sync(QC_FULL, ok);
+                if (bal) {
+                    idx = base + __ffs(bal) - 1;
+                    break;
+                }
+            }
+            if (sum_in + top_sum(ws, vmax, idx) < (long long)m * md_at(P, m + idx)) {
+                lb = ub + 1;
+                invalid = true;
+            } else {
+                lb = idx;
+                int tub = idx;
+                for (int base = idx + 1; base <= ub; base += 32) {
+                    int k = base + lane;
+                    bool ok = (k <= ub) &&
+                              (sum_in + top_sum(ws, vmax, k) >= (long long)m * md_at(P, m + k));
+                    int best = wmax(ok ? k : -1);
+                    if (best > tub) tub = best;
+                }
+                if (ub > tub) ub = tub;
+                if (lb > 1) b.med = mindeg(P, m + lb);
+            }
+        }
+        b.U = ub;
+        b.L = lb;
+    } else {
+        b.U = ncand;
+        b.L = m < P.min_size ? P.min_size - m : 0;
+    }
+    if (m + b.U < P.min_size) invalid = true;
+    if (b.U < 0 || b.U < b.L) invalid = true;
+    return invalid;
+}
+
+// every member extendable? (main.cu:1749-1753)
+__device__ bool members_ok(const ExpandParams& P, Ws& ws, const uint32_t* mm, int t, int m,
+                           const Bounds& b)
+{
+    int lane = lane_id();
+    int bad = 0;
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        if (v < t && bit(mm, v) && !vert_extendable(P, ws.indeg[v], ws.exdeg[v], m, b)) bad = 1;
+    }
+    return !__any_sync(QC_FULL, bad);
+}
+
+// exdeg[v] = |N(v) & R| for v in mask `who`
+__device__ void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, const uint32_t* R)
+{
+    int lane = lane_id();
+    for (int base = 0; base < T.t; base += 32) {
+        int v = base + lane;
+        if (v < T.t && bit(who, v)) ws.exdeg[v] = popc_and(T.A1 + (int64_t)v * T.W, R, T.W);
+    }
+    __syncwarp();
+}
+
+// out = {v in in_mask : cand_valid(v)} ; rem = in_mask \ out
+__device__ void filter_valid(const ExpandParams& P, Ws& ws, const uint32_t* in_mask, int t, int W,
+                             int m, const Bounds& b, uint32_t* out, uint32_t* rem)
+{
+    int lane = lane_id();
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        bool in = v < t && bit(in_mask, v);
+        bool ok = in && cand_valid(P, ws.indeg[v], ws.exdeg[v], m, b);
+        unsigned bo = __ballot_sync(QC_FULL, ok);
+        unsigned br = __ballot_sync(QC_FULL, in && !ok);
+        if (lane == 0) {
+            out[base >> 5] = bo;
+            if (rem) rem[base >> 5] = br;
+        }
+    }
+    for (int w = words_for(t) + lane; w < W; w += 32) {
+        out[w] = 0;
+        if (rem) rem[w] = 0;
+    }
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------
+// iterative degree pruning (main.cu:1735-1855)
+// Entry: indeg/exdeg valid for M u Call with exdeg relative to Call.
+// D = diameter survivors (label 0).  On success R holds the candidates.
+// Returns true on invalid bounds or a non-extendable member.
+// ------------------------------------------------------------------
+
+__device__ bool degree_prune(const ExpandParams& P, const TaskView& T, Ws& ws, const uint32_t* M,
+                             int m, const uint32_t* Call, const uint32_t* D, uint32_t* R,
+                             Bounds& b)
+{
+    const int t = T.t, W = T.W;
+    uint32_t* X = ws.mk[MK_X];
+    uint32_t* who = ws.mk[MK_U];
+    Bounds dummy = {0, 0, 0};
+    int nc = build_hist(P, ws, D, t, m, false, m, dummy);
+    if (lu_bounds(P, ws, M, t, m, nc, m, b)) return true;
+    if (!members_ok(P, ws, M, t, m, b)) return true;
+    filter_valid(P, ws, D, t, W, m, b, R, nullptr);
+    // X = Call \ R
+    for (int w = lane_id(); w < W; w += 32) X[w] = Call[w] & ~R[w];
+    __syncwarp();
+    while (!bs_empty(R, W) && !bs_empty(X, W)) {
+        for (int w = lane_id(); w < W; w += 32) who[w] = M[w] | R[w];
+        __syncwarp();
+        recount_exdeg(T, ws, who, R);
+        int nv = build_hist(P, ws, R, t, m, true, m, b);
+        if (lu_bounds(P, ws, M, t, m, nv, m, b)) return true;
+        if (!members_ok(P, ws, M, t, m, b)) return true;
+        // R' = valid(R), X = R \ R'
+        filter_valid(P, ws, R, t, W, m, b, ws.mk[MK_T], X);
+        bs_copy(R, ws.mk[MK_T], W);
+    }
+    return false;
+}
+
+// ------------------------------------------------------------------
+// emission and allocation
+// ------------------------------------------------------------------
+
+__device__ __forceinline__ void set_status(const ExpandParams& P, int bits)
+{
+    atomicOr(&P.ctl->status, bits);
+}
+
+// write the ids of the vertices in mask `mm` (count k) as one set
+__device__ void emit_mask(const ExpandParams& P, const TaskView& T, const uint32_t* mm, int k)
+{
+    int lane = lane_id();
+    unsigned long long at = 0;
+    if (lane == 0) {
+        at = atomicAdd(&P.ctl->result_top, (unsigned long long)(k + 1));
+        if (at + k + 1 > P.ctl->result_cap) {
+            set_status(P, ST_RESULT_OVERFLOW);
+            at = ~0ull;
+        } else {
+            atomicAdd(&P.ctl->emitted, 1ull);
+            atomicAdd(&P.ctl->emitted_ints, (unsigned long long)(k + 1));
+        }
+    }
+    at = __shfl_sync(QC_FULL, at, 0);
+    if (at == ~0ull) return;
+    if (lane == 0) P.results[at] = k;
+    int written = 0;
+    for (int base = 0; base < T.t; base += 32) {
+        int v = base + lane;
+        bool in = v < T.t && bit(mm, v);
+        unsigned bal = __ballot_sync(QC_FULL, in);
+        if (in) {
+            int r = __popc(bal & ((1u << lane) - 1u));
+            P.results[at + 1 + written + r] = T.ids[v];
+        }
+        written += __popc(bal);
+    }
+}
+
+// clique check (main.cu:1974-1995): every member has indeg >= md[m]
+__device__ void check_clique(const ExpandParams& P, const TaskView& T, Ws& ws, const uint32_t* mm,
+                             int m)
+{
+    int lane = lane_id();
+    int need = md_at(P, m);
+    int bad = 0;
+    for (int base = 0; base < T.t; base += 32) {
+        int v = base + lane;
+        if (v < T.t && bit(mm, v) && ws.indeg[v] < need) bad = 1;
+    }
+    if (!__any_sync(QC_FULL, bad)) emit_mask(P, T, mm, m);
+}
+
+// ------------------------------------------------------------------
+// work stack: push / pop with per-slot hand-off and bounded waits
+// ------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+#ifdef QC_EMULATION
+    t = emu_globaltimer();
+#else
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+#endif
+    return t;
+}
+
+// lane-0 only
+__device__ bool push_item(const ExpandParams& P, WorkItem it)
+{
+    atomicAdd(&P.ctl->pending, 1);
+    int idx = atomicAdd(&P.ctl->stack_top, 1);
+    if (idx >= P.ctl->stack_cap) {
+        set_status(P, ST_TASK_OVERFLOW);
+        atomicSub(&P.ctl->pending, 1);
+        return false;
+    }
+    unsigned long long t0 = now_ns();
+    unsigned spins = 0;
+    while (atomicCAS(&P.slot[idx], 0, 2) != 0) {
+        if ((++spins & 255u) == 0) {
+            if (now_ns() - t0 > (unsigned long long)P.wait_ns || P.ctl->status) {
+                set_status(P, ST_ITER_LIMIT);
+                P.ctl->wait_fail_where = 1;
+                return false;
+            }
+        }
+        __nanosleep(64);
+    }
+    P.stack[idx] = it;
+    __threadfence();
+    atomicExch(&P.slot[idx], 1);
+    return true;
+}
+
+// lane-0 only; returns 1 item, 0 empty-and-done, -1 error/abort
+__device__ int pop_item(const ExpandParams& P, WorkItem& out)
+{
+    unsigned long long t0 = now_ns();
+    unsigned spins = 0;
+    int last_pending = -1;
+    for (;;) {
+        if (*(volatile int*)&P.ctl->status) return -1;
+        int top = *(volatile int*)&P.ctl->stack_top;
+        if (top > 0) {
+            if (atomicCAS(&P.ctl->stack_top, top, top - 1) == top) {
+                int idx = top - 1;
+                unsigned long long t1 = now_ns();
+                unsigned s2 = 0;
+                while (atomicCAS(&P.slot[idx], 1, 3) != 1) {
+                    if ((++s2 & 255u) == 0 && now_ns() - t1 > (unsigned long long)P.wait_ns) {
+                        set_status(P, ST_ITER_LIMIT);
+                        P.ctl->wait_fail_where = 2;
+                        return -1;
+                    }
+                    __nanosleep(32);
+                }
+                __threadfence();
+                const volatile WorkItem* src = &P.stack[idx];
+                out.rec = src->rec;
+                out.q_lo = src->q_lo;
+                out.q_hi = src->q_hi;
+                __threadfence();
+                atomicExch(&P.slot[idx], 0);
+                return 1;
+            }
+            continue;
+        }
+        int pend = *(volatile int*)&P.ctl->pending;
+        if (pend == 0) return 0;
+        if (pend != last_pending) {
+            last_pending = pend;
+            t0 = now_ns();
+        }
+        if ((++spins & 63u) == 0 && now_ns() - t0 > (unsigned long long)P.wait_ns) {
+            set_status(P, ST_ITER_LIMIT);
+            P.ctl->wait_fail_where = 3;
+            return -1;
+        }
+        __nanosleep(256);
+    }
+}
+
+// ------------------------------------------------------------------
+// child task: Q-sort (main.cu:2059-2104) and compacted matrices
+// ------------------------------------------------------------------
+
+// key: members first; then indeg desc, exdeg desc, l2 desc, id desc.
+__device__ __forceinline__ bool key_less(unsigned long long ah, unsigned long long al,
+                                         unsigned long long bh, unsigned long long bl)
+{
+    return ah < bh || (ah == bh && al < bl);
+}
+
+// Warp bitonic sort of n (key_hi, key_lo, sel) entries in the workspace.
+__device__ void sort_keys(Ws& ws, int n)
+{
+    int lane = lane_id();
+    int N = 1;
+    while (N < n) N <<= 1;
+    for (int i = n + lane; i < N; i += 32) {
+        ws.khi[i] = ~0ull;
+        ws.klo[i] = ~0ull;
+        ws.sel[i] = -1;
+    }
+    __syncwarp();
+    for (int k = 2; k <= N; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < N; i += 32) {
+                int p = i ^ j;
+                if (p > i) {
+                    bool up = (i & k) == 0;
+                    unsigned long long ah = ws.khi[i], al = ws.klo[i];
+                    unsigned long long bh = ws.khi[p], bl = ws.klo[p];
+                    bool gt = key_less(bh, bl, ah, al);
+                    if (gt == up) {
+                        ws.khi[i] = bh; ws.klo[i] = bl;
+                        ws.khi[p] = ah; ws.klo[p] = al;
+                        int s = ws.sel[i]; ws.sel[i] = ws.sel[p]; ws.sel[p] = s;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, const uint32_t* M,
+                            int m, const uint32_t* R, int nr)
+{
+    int lane = lane_id();
+    int tc = m + nr;
+    if (tc > P.max_t) {
+        if (lane == 0) set_status(P, ST_TOO_LARGE);
+        return;
+    }
+    // gather (key, position)
+    int written = 0;
+    for (int base = 0; base < T.t; base += 32) {
+        int v = base + lane;
+        bool isM = v < T.t && bit(M, v);
+        bool isR = v < T.t && bit(R, v);
+        bool in = isM || isR;
+        unsigned bal = __ballot_sync(QC_FULL, in);
+        if (in) {
+            int r = written + __popc(bal & ((1u << lane) - 1u));
+            unsigned long long cls = isM ? 0ull : 1ull;
+            unsigned long long in_k = 0xffffull - (unsigned long long)ws.indeg[v];
+            unsigned long long ex_k = 0xffffull - (unsigned long long)ws.exdeg[v];
+            unsigned long long l2_k = 0xffffull - (unsigned long long)T.l2[v];
+            ws.khi[r] = (cls << 48) | (in_k << 32) | (ex_k << 16) | l2_k;
+            ws.klo[r] = 0xffffffffull - (unsigned long long)(unsigned)T.ids[v];
+            ws.sel[r] = v;
+        }
+        written += __popc(bal);
+    }
+    __syncwarp();
+    sort_keys(ws, tc);
+    int Wc = words_for(tc);
+    unsigned long long bytes = rec_bytes(tc, Wc);
+    unsigned long long at = 0;
+    if (lane == 0) {
+        at = atomicAdd(&P.ctl->arena_top, bytes);
+        if (at + bytes > P.ctl->arena_cap) {
+            set_status(P, ST_TASK_OVERFLOW);
+            at = ~0ull;
+        }
+    }
+    at = __shfl_sync(QC_FULL, at, 0);
+    if (at == ~0ull) return;
+    char* rec = P.arena + at;
+    if (lane == 0) {
+        TaskHdr* h = (TaskHdr*)rec;
+        h->t = tc;
+        h->m = m;
+        h->cov = 0;
+        h->W = Wc;
+    }
+    int32_t* cid = (int32_t*)(rec + rec_ids_off());
+    int32_t* cl2 = (int32_t*)(rec + rec_l2_off(tc));
+    uint32_t* c1 = (uint32_t*)(rec + rec_a1_off(tc));
+    uint32_t* c2 = (uint32_t*)(rec + rec_a2_off(tc, Wc));
+    for (int i = lane; i < tc; i += 32) {
+        cid[i] = T.ids[ws.sel[i]];
+        cl2[i] = 0;
+    }
+    // compacted rows: child bit j of row i = parent bit sel[j] of row sel[i]
+    for (int i = 0; i < tc; i++) {
+        const uint32_t* r1 = T.A1 + (int64_t)ws.sel[i] * T.W;
+        const uint32_t* r2 = T.A2 + (int64_t)ws.sel[i] * T.W;
+        for (int w = 0; w < Wc; w++) {
+            int j = w * 32 + lane;
+            bool b1 = false, b2 = false;
+            if (j < tc) {
+                int pj = ws.sel[j];
+                b1 = bit(r1, pj);
+                b2 = bit(r2, pj);
+            }
+            unsigned w1 = __ballot_sync(QC_FULL, b1);
+            unsigned w2 = __ballot_sync(QC_FULL, b2);
+            if (lane == 0) {
+                c1[(int64_t)i * Wc + w] = w1;
+                c2[(int64_t)i * Wc + w] = w2;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        atomicAdd(&P.ctl->children, 1ull);
+        atomicMax(&P.ctl->max_task, tc);
+        __threadfence();
+        WorkItem it;
+        it.rec = at;
+        it.q_lo = -1;
+        it.q_hi = -1;
+        push_item(P, it);
+    }
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------
+// one branch: add parent position q (main.cu:1086-1178)
+// ------------------------------------------------------------------
+
+__device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, int q)
+{
+    const int t = T.t, W = T.W;
+    int lane = lane_id();
+    uint32_t* M = ws.mk[MK_M];
+    uint32_t* PRE = ws.mk[MK_PRE];
+    uint32_t* D = ws.mk[MK_D];
+    uint32_t* R = ws.mk[MK_R];
+    uint32_t* CA = ws.mk[MK_CA];
+    uint32_t* Kc = ws.mk[MK_K];
+    uint32_t* who = ws.mk[MK_U];
+
+    // members M u {q}; candidates before q
+    bs_range(M, W, 0, T.m);
+    if (lane == 0) M[q >> 5] |= 1u << (q & 31);
+    __syncwarp();
+    bs_range(PRE, W, T.m, q);
+    int m1 = T.m + 1;
+    // degrees for members and PRE (add one vertex, main.cu:1465-1492)
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        if (v < t && (bit(M, v) || bit(PRE, v))) {
+            const uint32_t* row = T.A1 + (int64_t)v * W;
+            ws.indeg[v] = popc_and(row, M, W);
+            ws.exdeg[v] = popc_and(row, PRE, W);
+        }
+    }
+    // diameter pruning (main.cu:1709-1732): PRE & N2(q)
+    const uint32_t* r2q = T.A2 + (int64_t)q * W;
+    for (int w = lane; w < W; w += 32) D[w] = PRE[w] & r2q[w];
+    __syncwarp();
+    if (lane == 0) atomicAdd(&P.ctl->branches, 1ull);
+
+    Bounds b = {0, 0, 0};
+    if (degree_prune(P, T, ws, M, m1, PRE, D, R, b)) {
+        if (m1 >= P.min_size) check_clique(P, T, ws, M, m1);
+        return;
+    }
+
+    // critical-vertex pruning (main.cu:1526-1707)
+    int critv = md_at(P, m1 + b.L);
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        bool k = v < t && bit(M, v) && ws.indeg[v] + ws.exdeg[v] == critv && ws.exdeg[v] > 0;
+        unsigned bal = __ballot_sync(QC_FULL, k);
+        if (lane == 0) Kc[base >> 5] = bal;
+    }
+    for (int w = words_for(t) + lane; w < W; w += 32) Kc[w] = 0;
+    __syncwarp();
+    // CA = R & OR over critical members of A1 rows
+    for (int w = lane; w < W; w += 32) {
+        uint32_t acc = 0;
+        for (int base = 0; base < t; base += 32) {
+            uint32_t kw = Kc[base >> 5];
+            while (kw) {
+                int v = base + __ffs(kw) - 1;
+                kw &= kw - 1;
+                acc |= T.A1[(int64_t)v * W + w];
+            }
+        }
+        CA[w] = acc & R[w];
+    }
+    __syncwarp();
+    int nca = bs_count(CA, W);
+    int m2 = m1;
+    uint32_t* C2 = ws.mk[MK_C];
+    uint32_t* D2 = ws.mk[MK_D];
+    if (nca > 0) {
+        // add the critical-adjacent candidates; 2-hop counts to them
+        int bad = 0;
+        for (int base = 0; base < t; base += 32) {
+            int v = base + lane;
+            if (v < t && (bit(M, v) || bit(R, v))) {
+                int d = popc_and(T.A1 + (int64_t)v * W, CA, W);
+                ws.indeg[v] += d;
+                ws.exdeg[v] -= d;
+                int a = popc_and(T.A2 + (int64_t)v * W, CA, W);
+                ws.aux[v] = a;
+                if (bit(M, v) && a != nca) bad = 1;
+                if (bit(CA, v) && a < nca - 1) bad = 1;
+            }
+        }
+        if (__any_sync(QC_FULL, bad)) return;
+        for (int w = lane; w < W; w += 32) {
+            M[w] |= CA[w];
+            C2[w] = R[w] & ~CA[w];
+        }
+        __syncwarp();
+        m2 = m1 + nca;
+        // diameter pruning against the added vertices (main.cu:1689-1697)
+        for (int base = 0; base < t; base += 32) {
+            int v = base + lane;
+            bool in = v < t && bit(C2, v) && ws.aux[v] == nca;
+            unsigned bal = __ballot_sync(QC_FULL, in);
+            if (lane == 0) D2[base >> 5] = bal;
+        }
+        for (int w = words_for(t) + lane; w < W; w += 32) D2[w] = 0;
+        __syncwarp();
+    } else {
+        bs_copy(C2, R, W);
+        bs_copy(D2, R, W);
+    }
+    (void)who;
+    uint32_t* R2 = ws.mk[MK_R];
+    Bounds b2 = {0, 0, 0};
+    bool fail2 = degree_prune(P, T, ws, M, m2, C2, D2, R2, b2);
+    if (m2 >= P.min_size) check_clique(P, T, ws, M, m2);
+    if (fail2) return;
+    int nr = bs_count(R2, W);
+    if (nr > 0) write_child(P, T, ws, M, m2, R2, nr);
+}
+
+// ------------------------------------------------------------------
+// a work item: fresh task (lookahead, branch range) or a branch range
+// ------------------------------------------------------------------
+
+__device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
+{
+    TaskView T = task_view(P.arena, it.rec);
+    const int t = T.t, W = T.W, m = T.m;
+    int lane = lane_id();
+    if (t > P.max_t) {
+        if (lane == 0) set_status(P, ST_TOO_LARGE);
+        return;
+    }
+    int q_lo = it.q_lo, q_hi = it.q_hi;
+    if (q_lo < 0) {
+        if (lane == 0) {
+            atomicAdd(&P.ctl->tasks, 1ull);
+            atomicMax(&P.ctl->max_task, t);
+        }
+        uint32_t* MM = ws.mk[MK_M];
+        uint32_t* CC = ws.mk[MK_C];
+        bs_range(MM, W, 0, m);
+        bs_range(CC, W, m, t);
+        int nc = t - m;
+        // task degrees
+        for (int base = 0; base < t; base += 32) {
+            int v = base + lane;
+            if (v < t) {
+                const uint32_t* row = T.A1 + (int64_t)v * W;
+                ws.indeg[v] = popc_and(row, MM, W);
+                ws.exdeg[v] = popc_and(row, CC, W);
+            }
+        }
+        __syncwarp();
+        // lookahead (main.cu:1349-1405)
+        int need_t = md_at(P, t);
+        int bad = 0;
+        for (int v = lane; v < m; v += 32)
+            if (ws.indeg[v] + ws.exdeg[v] < need_t) bad = 1;
+        if (!__any_sync(QC_FULL, bad)) {
+            int bad2 = 0;
+            for (int v = m + lane; v < t; v += 32) {
+                int l2 = popc_and(T.A2 + (int64_t)v * W, CC, W);
+                T.l2[v] = l2;
+                if (l2 < nc - 1 || ws.indeg[v] + ws.exdeg[v] < need_t) bad2 = 1;
+            }
+            __syncwarp();
+            if (!__any_sync(QC_FULL, bad2)) {
+                uint32_t* all = ws.mk[MK_T];
+                bs_range(all, W, 0, t);
+                if (lane == 0) atomicAdd(&P.ctl->lookahead_hits, 1ull);
+                emit_mask(P, T, all, t);
+                return;
+            }
+        }
+        // branches executed before a member fails on removal (main.cu:1092-1099)
+        int need = mindeg(P, m);
+        int qmax = m + T.cov;
+        for (int v = 0; v < m; v++) {
+            int k = need - ws.indeg[v];
+            if (k <= 0) continue;
+            // position of the k-th candidate neighbour of v
+            const uint32_t* row = T.A1 + (int64_t)v * W;
+            int pos = t - 1;
+            int seen = 0;
+            for (int base = 0; base < W * 32; base += 32 * 32) {
+                int w = (base >> 5) + lane;
+                uint32_t x = (w < W) ? (row[w] & CC[w]) : 0u;
+                int c = __popc(x);
+                int inc = wscan(c);
+                int tot = __shfl_sync(QC_FULL, inc, 31);
+                if (seen + tot >= k) {
+                    int need_here = k - seen;
+                    unsigned hit = __ballot_sync(QC_FULL, inc >= need_here && inc - c < need_here);
+                    int src = __ffs(hit) - 1;
+                    int before = __shfl_sync(QC_FULL, inc - c, src);
+                    uint32_t xw = __shfl_sync(QC_FULL, x, src);
+                    int r = need_here - before; // r-th set bit of xw (1-based)
+                    for (int s = 1; s < r; s++) xw &= xw - 1;
+                    int wsrc = (base >> 5) + src;
+                    pos = wsrc * 32 + __ffs(xw) - 1;
+                    break;
+                }
+                seen += tot;
+            }
+            qmax = pos > qmax ? pos : qmax;
+        }
+        q_lo = qmax > t - 1 ? t - 1 : qmax;
+        q_hi = t - 1;
+        if (m + T.cov >= t) return; // no branchable candidate
+        int nb = q_hi - q_lo + 1;
+        if (nb > P.split) {
+            __syncwarp();
+            __threadfence();
+            if (lane == 0) {
+                for (int hi = q_hi - P.split; hi >= q_lo; hi -= P.split) {
+                    WorkItem s;
+                    s.rec = it.rec;
+                    s.q_hi = hi;
+                    s.q_lo = hi - P.split + 1 < q_lo ? q_lo : hi - P.split + 1;
+                    if (!push_item(P, s)) break;
+                }
+            }
+            __syncwarp();
+            q_lo = q_hi - P.split + 1;
+        }
+    }
+    for (int q = q_hi; q >= q_lo; q--) {
+        if (*(volatile int*)&P.ctl->status) return;
+        expand_branch(P, T, ws, q);
+    }
+}
+
+// ------------------------------------------------------------------
+// the persistent kernel
+// ------------------------------------------------------------------
+
+__global__ void expand_kernel(ExpandParams P)
+{
+    int lane = lane_id();
+    int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    Ws ws = ws_view(P, warp_global);
+    for (;;) {
+        WorkItem it;
+        int r = 0;
+        if (lane == 0) r = pop_item(P, it);
+        r = __shfl_sync(QC_FULL, r, 0);
+        if (r <= 0) break;
+        it.rec = __shfl_sync(QC_FULL, it.rec, 0);
+        it.q_lo = __shfl_sync(QC_FULL, it.q_lo, 0);
+        it.q_hi = __shfl_sync(QC_FULL, it.q_hi, 0);
+        __threadfence();
+        process_item(P, ws, it);
+        __syncwarp();
+        __threadfence();
+        if (lane == 0) atomicSub(&P.ctl->pending, 1);
+    }
+}
+
+} // namespace qcb

@@ -1,0 +1,366 @@
+// host.cpp -- graph I/O, gamma tables, level-0 root, maximal filter (host side).
+#include "host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+
+namespace qcb {
+
+// ------------------------------------------------------------------
+// serialized graph I/O
+// ------------------------------------------------------------------
+
+namespace {
+
+struct Tok {
+    const char* p;
+    const char* e;
+    bool next(int64_t& v)
+    {
+        while (p < e && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t' || *p == '\f' ||
+                         *p == '\v'))
+            p++;
+        if (p >= e) return false;
+        bool neg = false;
+        if (*p == '-' || *p == '+') {
+            neg = *p == '-';
+            p++;
+        }
+        if (p >= e || *p < '0' || *p > '9') return false;
+        int64_t x = 0;
+        while (p < e && *p >= '0' && *p <= '9') x = x * 10 + (*p++ - '0');
+        v = neg ? -x : x;
+        return true;
+    }
+};
+
+void put_num(std::string& s, int64_t v)
+{
+    char b[24];
+    int k = snprintf(b, sizeof(b), "%lld", (long long)v);
+    s.append(b, (size_t)k);
+}
+
+} // namespace
+
+std::string read_serialized(const char* path, HostGraph& g)
+{
+    FILE* f = fopen(path, "rb");
+    if (!f) return std::string("cannot open graph file ") + path;
+    std::string buf;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (sz > 0) {
+        buf.resize((size_t)sz);
+        if (fread(&buf[0], 1, (size_t)sz, f) != (size_t)sz) {
+            fclose(f);
+            return "short read on graph file";
+        }
+    }
+    fclose(f);
+    Tok t{buf.data(), buf.data() + buf.size()};
+    int64_t n, m, m2;
+    if (!t.next(n) || !t.next(m) || !t.next(m2)) return "missing header (n, 2|E|, #2-hop)";
+    if (n < 0 || n > INT32_MAX || m < 0 || m2 < 0) return "bad header values";
+    g.n = (int32_t)n;
+    g.adj.resize((size_t)m);
+    g.off.resize((size_t)n + 1);
+    g.adj2.resize((size_t)m2);
+    g.off2.resize((size_t)n + 1);
+    int64_t v;
+    for (int64_t i = 0; i < m; i++) {
+        if (!t.next(v)) return "truncated 1-hop neighbour list";
+        g.adj[(size_t)i] = (int32_t)v;
+    }
+    for (int64_t i = 0; i <= n; i++) {
+        if (!t.next(v)) return "truncated 1-hop offsets";
+        g.off[(size_t)i] = v;
+    }
+    for (int64_t i = 0; i < m2; i++) {
+        if (!t.next(v)) return "truncated 2-hop neighbour list";
+        g.adj2[(size_t)i] = (int32_t)v;
+    }
+    for (int64_t i = 0; i <= n; i++) {
+        if (!t.next(v)) return "truncated 2-hop offsets";
+        g.off2[(size_t)i] = v;
+    }
+    return "";
+}
+
+std::string write_serialized(const HostGraph& g, const char* path)
+{
+    FILE* f = fopen(path, "wb");
+    if (!f) return std::string("cannot open ") + path + " for writing";
+    std::string s;
+    auto flush = [&] {
+        fwrite(s.data(), 1, s.size(), f);
+        s.clear();
+    };
+    put_num(s, g.n); s += '\n';
+    put_num(s, (int64_t)g.adj.size()); s += '\n';
+    put_num(s, (int64_t)g.adj2.size()); s += '\n';
+    auto row = [&](const auto& a) {
+        for (size_t i = 0; i < a.size(); i++) {
+            if (i) s += ' ';
+            put_num(s, (int64_t)a[i]);
+            if (s.size() > (1u << 20)) flush();
+        }
+        s += '\n';
+    };
+    row(g.adj);
+    row(g.off);
+    row(g.adj2);
+    row(g.off2);
+    flush();
+    fclose(f);
+    return "";
+}
+
+std::string validate(const HostGraph& g, bool need_twohop)
+{
+    const int32_t n = g.n;
+    if ((int64_t)g.off.size() != (int64_t)n + 1) return "1-hop offsets must have n+1 entries";
+    if (g.off[0] != 0 || g.off[(size_t)n] != (int64_t)g.adj.size())
+        return "1-hop offsets must start at 0 and end at 2|E|";
+    for (int32_t v = 0; v < n; v++) {
+        if (g.off[(size_t)v + 1] < g.off[(size_t)v]) return "1-hop offsets decrease";
+        for (int64_t e = g.off[(size_t)v]; e < g.off[(size_t)v + 1]; e++) {
+            int32_t w = g.adj[(size_t)e];
+            if (w < 0 || w >= n) return "1-hop neighbour id out of range";
+            if (w == v) return "self loop in 1-hop list";
+            if (e > g.off[(size_t)v] && g.adj[(size_t)e - 1] >= w)
+                return "1-hop rows must be sorted ascending without duplicates";
+        }
+    }
+    // symmetry: w in N(v) <=> v in N(w)
+    for (int32_t v = 0; v < n; v++) {
+        for (int64_t e = g.off[(size_t)v]; e < g.off[(size_t)v + 1]; e++) {
+            int32_t w = g.adj[(size_t)e];
+            const int32_t* b = g.adj.data() + g.off[(size_t)w];
+            const int32_t* z = g.adj.data() + g.off[(size_t)w + 1];
+            if (!std::binary_search(b, z, v)) return "graph is not undirected (asymmetric 1-hop rows)";
+        }
+    }
+    if (!need_twohop) return "";
+    if ((int64_t)g.off2.size() != (int64_t)n + 1) return "2-hop offsets must have n+1 entries";
+    if (g.off2[0] != 0 || g.off2[(size_t)n] != (int64_t)g.adj2.size())
+        return "2-hop offsets must start at 0 and end at the 2-hop count";
+    for (int32_t v = 0; v < n; v++) {
+        if (g.off2[(size_t)v + 1] < g.off2[(size_t)v]) return "2-hop offsets decrease";
+        for (int64_t e = g.off2[(size_t)v]; e < g.off2[(size_t)v + 1]; e++) {
+            int32_t w = g.adj2[(size_t)e];
+            if (w < 0 || w >= n) return "2-hop neighbour id out of range";
+            if (e > g.off2[(size_t)v] && g.adj2[(size_t)e - 1] >= w)
+                return "2-hop rows must be sorted ascending without duplicates";
+        }
+    }
+    return "";
+}
+
+// ------------------------------------------------------------------
+// gamma tables
+// ------------------------------------------------------------------
+
+void gamma_tables(double gamma, int n, int min_size, std::vector<int32_t>& md,
+                  std::vector<int32_t>& ubt)
+{
+    int len = std::max(n, min_size) + 3;
+    md.assign((size_t)len, 0);
+    ubt.assign((size_t)len, 0);
+    for (int i = 1; i < len; i++) md[(size_t)i] = (int32_t)std::ceil(gamma * (double)(i - 1));
+    for (int d = 0; d < len; d++) ubt[(size_t)d] = (int32_t)std::floor((double)d / gamma);
+}
+
+// ------------------------------------------------------------------
+// level 0 (main.cu:846-998)
+// ------------------------------------------------------------------
+
+void build_root(const HostGraph& g, const int32_t* md, int min_size, std::vector<int32_t>& ids,
+                int& cov)
+{
+    const int32_t n = g.n;
+    const int need = md[min_size];
+    std::vector<int32_t> label((size_t)n), exdeg((size_t)n), l2((size_t)n);
+    std::vector<int32_t> rem, rmv;
+    rem.reserve((size_t)n);
+    rmv.reserve((size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+        exdeg[(size_t)i] = (int32_t)(g.off[(size_t)i + 1] - g.off[(size_t)i]);
+        l2[(size_t)i] = g.off2.empty() ? 0 : (int32_t)(g.off2[(size_t)i + 1] - g.off2[(size_t)i]);
+        if (exdeg[(size_t)i] >= need && l2[(size_t)i] >= min_size - 1) {
+            label[(size_t)i] = 0;
+            rem.push_back(i);
+        } else {
+            label[(size_t)i] = -1;
+            rmv.push_back(i);
+        }
+    }
+    // recount while fewer than half of the previous candidates survive
+    int64_t ncand = n;
+    while ((int64_t)rem.size() < ncand / 2) {
+        ncand = (int64_t)rem.size();
+        for (int32_t u : rem) exdeg[(size_t)u] = 0;
+        for (int32_t u : rem)
+            for (int64_t e = g.off[(size_t)u]; e < g.off[(size_t)u + 1]; e++) {
+                int32_t w = g.adj[(size_t)e];
+                if (label[(size_t)w] == 0) exdeg[(size_t)w]++;
+            }
+        std::vector<int32_t> keep;
+        rmv.clear();
+        for (int32_t u : rem) {
+            if (exdeg[(size_t)u] >= need) keep.push_back(u);
+            else {
+                label[(size_t)u] = -1;
+                rmv.push_back(u);
+            }
+        }
+        rem.swap(keep);
+    }
+    // cascade the last removals
+    for (size_t k = 0; k < rmv.size(); k++) {
+        int32_t u = rmv[k];
+        for (int64_t e = g.off[(size_t)u]; e < g.off[(size_t)u + 1]; e++) {
+            int32_t w = g.adj[(size_t)e];
+            if (label[(size_t)w] == 0) {
+                if (--exdeg[(size_t)w] < need) {
+                    label[(size_t)w] = -1;
+                    rmv.push_back(w);
+                }
+            }
+        }
+    }
+    // cover vertex: first label-0 vertex of maximum exdeg (strictly > 0)
+    int32_t best = 0, best_i = 0;
+    for (int32_t i = 0; i < n; i++)
+        if (label[(size_t)i] == 0 && exdeg[(size_t)i] > best) {
+            best = exdeg[(size_t)i];
+            best_i = i;
+        }
+    ids.clear();
+    cov = 0;
+    std::vector<int32_t> surv;
+    for (int32_t i = 0; i < n; i++)
+        if (label[(size_t)i] == 0) surv.push_back(i);
+    if (surv.empty()) return;
+    label[(size_t)best_i] = 3;
+    for (int64_t e = g.off[(size_t)best_i]; e < g.off[(size_t)best_i + 1]; e++) {
+        int32_t w = g.adj[(size_t)e];
+        if (label[(size_t)w] == 0) label[(size_t)w] = 2;
+    }
+    // Q order: covered (2), candidates (0), cover (3); then exdeg, 2-hop
+    // size, id, all descending (indeg is 0 for every root vertex)
+    auto rank = [](int32_t l) { return l == 2 ? 0 : (l == 0 ? 1 : 2); };
+    std::sort(surv.begin(), surv.end(), [&](int32_t a, int32_t b) {
+        int ra = rank(label[(size_t)a]), rb = rank(label[(size_t)b]);
+        if (ra != rb) return ra < rb;
+        if (exdeg[(size_t)a] != exdeg[(size_t)b]) return exdeg[(size_t)a] > exdeg[(size_t)b];
+        if (l2[(size_t)a] != l2[(size_t)b]) return l2[(size_t)a] > l2[(size_t)b];
+        return a > b;
+    });
+    ids = surv;
+    for (int32_t u : surv)
+        if (label[(size_t)u] == 2) cov++;
+}
+
+// ------------------------------------------------------------------
+// maximal filter (host)
+// ------------------------------------------------------------------
+
+void maximal_sets(const int32_t* flat, int64_t nints, std::vector<int32_t>& out, int64_t& nsets)
+{
+    struct S {
+        int64_t at;
+        int32_t len;
+    };
+    std::vector<S> sets;
+    std::vector<int32_t> pool;
+    pool.reserve((size_t)nints);
+    int32_t maxid = -1;
+    for (int64_t p = 0; p < nints;) {
+        int32_t k = flat[p];
+        S s{(int64_t)pool.size(), k};
+        pool.insert(pool.end(), flat + p + 1, flat + p + 1 + k);
+        std::sort(pool.begin() + s.at, pool.end());
+        if (k > 0) maxid = std::max(maxid, pool.back());
+        sets.push_back(s);
+        p += 1 + k;
+    }
+    auto less = [&](const S& a, const S& b) {
+        return std::lexicographical_compare(pool.begin() + a.at, pool.begin() + a.at + a.len,
+                                            pool.begin() + b.at, pool.begin() + b.at + b.len);
+    };
+    auto equal = [&](const S& a, const S& b) {
+        return a.len == b.len &&
+               std::equal(pool.begin() + a.at, pool.begin() + a.at + a.len, pool.begin() + b.at);
+    };
+    std::sort(sets.begin(), sets.end(), less);
+    sets.erase(std::unique(sets.begin(), sets.end(), equal), sets.end());
+    // posting lists
+    std::vector<int64_t> start((size_t)maxid + 2, 0);
+    for (auto& s : sets)
+        for (int32_t i = 0; i < s.len; i++) start[(size_t)pool[(size_t)(s.at + i)] + 1]++;
+    for (size_t v = 1; v < start.size(); v++) start[v] += start[v - 1];
+    std::vector<int64_t> fill(start.begin(), start.end() - 1);
+    std::vector<int32_t> post((size_t)start.back());
+    for (size_t si = 0; si < sets.size(); si++)
+        for (int32_t i = 0; i < sets[si].len; i++)
+            post[(size_t)fill[(size_t)pool[(size_t)(sets[si].at + i)]]++] = (int32_t)si;
+    out.clear();
+    nsets = 0;
+    for (size_t si = 0; si < sets.size(); si++) {
+        const S& s = sets[si];
+        bool keep = true;
+        if (s.len > 0) {
+            int32_t best = pool[(size_t)s.at];
+            for (int32_t i = 1; i < s.len; i++) {
+                int32_t v = pool[(size_t)(s.at + i)];
+                if (start[(size_t)v + 1] - start[(size_t)v] < start[(size_t)best + 1] - start[(size_t)best])
+                    best = v;
+            }
+            for (int64_t e = start[(size_t)best]; e < start[(size_t)best + 1] && keep; e++) {
+                const S& t = sets[(size_t)post[(size_t)e]];
+                if (t.len <= s.len) continue;
+                if (std::includes(pool.begin() + t.at, pool.begin() + t.at + t.len,
+                                  pool.begin() + s.at, pool.begin() + s.at + s.len))
+                    keep = false;
+            }
+        }
+        if (keep) {
+            out.push_back(s.len);
+            out.insert(out.end(), pool.begin() + s.at, pool.begin() + s.at + s.len);
+            nsets++;
+        }
+    }
+}
+
+std::string write_result(const int32_t* flat, int64_t nints, const char* path)
+{
+    FILE* f = fopen(path, "wb");
+    if (!f) return std::string("cannot open ") + path + " for writing";
+    std::string s;
+    for (int64_t p = 0; p < nints;) {
+        int32_t k = flat[p];
+        put_num(s, k);
+        s += ' ';
+        for (int32_t i = 0; i < k; i++) {
+            put_num(s, flat[p + 1 + i]);
+            s += ' ';
+        }
+        s += '\n';
+        p += 1 + k;
+        if (s.size() > (1u << 20)) {
+            fwrite(s.data(), 1, s.size(), f);
+            s.clear();
+        }
+    }
+    fwrite(s.data(), 1, s.size(), f);
+    fclose(f);
+    return "";
+}
+
+} // namespace qcb

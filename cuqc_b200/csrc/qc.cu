@@ -1,0 +1,536 @@
+// qc.cu -- libqc.so: C ABI (include/qc.h) over the B200 expansion kernel.
+//
+// Flow of qc_mine (replaces Mike12041204/cuQC search() + RemoveNonMax(),
+// main.cu:535-692 and 4939-4960):
+//   1. gamma tables (md, ubt) on the host, exactly as the reference computes
+//      them in double, uploaded once per call;
+//   2. level 0 on the host (main.cu:846-998) -> root ids + covered count;
+//   3. root task record built on the device from the CSR (one warp per root
+//      vertex scans its 1-hop and 2-hop rows, 128-bit coalesced by lanes);
+//   4. one persistent launch of expand_kernel drains the device work stack;
+//   5. emitted sets copied back, maximal filter, lexicographic order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/qc.h"
+#include "expand_kernel.cuh"
+#include "host.h"
+
+using namespace qcb;
+
+// ------------------------------------------------------------------
+// errors
+// ------------------------------------------------------------------
+
+static thread_local std::string g_err;
+
+static qc_status fail(qc_status s, const std::string& msg)
+{
+    g_err = msg;
+    return s;
+}
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(e_ == cudaErrorMemoryAllocation ? QC_ERR_NOMEM : QC_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));          \
+    } while (0)
+
+extern "C" const char* qc_status_str(qc_status s)
+{
+    switch (s) {
+    case QC_OK: return "ok";
+    case QC_ERR_ARGS: return "invalid argument";
+    case QC_ERR_IO: return "file error";
+    case QC_ERR_FORMAT: return "malformed graph";
+    case QC_ERR_CUDA: return "CUDA error";
+    case QC_ERR_NOMEM: return "out of memory";
+    case QC_ERR_TASK_OVERFLOW: return "task stack or record arena exhausted";
+    case QC_ERR_RESULT_OVERFLOW: return "result buffer exhausted";
+    case QC_ERR_ITER_LIMIT: return "bounded device wait gave up";
+    case QC_ERR_TOO_LARGE: return "task too large";
+    case QC_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char* qc_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------------------
+// objects
+// ------------------------------------------------------------------
+
+struct qc_graph {
+    HostGraph h;
+};
+
+struct qc_result {
+    std::vector<int32_t> sets;
+    int64_t nsets = 0;
+    std::vector<int32_t> emitted;
+    int64_t emitted_sets = 0;
+    qc_stats st{};
+};
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T> T* as() const { return (T*)p; }
+};
+
+} // namespace
+
+struct qc_context {
+    qc_config cfg{};
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws;
+    int32_t pos_n = 0;
+    int64_t arena_bytes = 0, stack_slots = 0, result_ints = 0;
+    int64_t launches = 0;
+};
+
+extern "C" void qc_config_default(qc_config* c)
+{
+    std::memset(c, 0, sizeof(*c));
+    c->device = 0;
+    c->wait_limit_ms = 10000;
+}
+
+extern "C" qc_status qc_context_create(const qc_config* cfg, qc_context** out)
+{
+    if (!out) return fail(QC_ERR_ARGS, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(QC_ERR_NO_DEVICE, "no CUDA device visible");
+    std::unique_ptr<qc_context> c(new qc_context());
+    if (cfg) c->cfg = *cfg;
+    else qc_config_default(&c->cfg);
+    if (c->cfg.device < 0 || c->cfg.device >= ndev) return fail(QC_ERR_ARGS, "bad device ordinal");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& e : c->ev) CK(cudaEventCreate(&e));
+    c->arena_bytes = c->cfg.arena_bytes > 0 ? c->cfg.arena_bytes : (256ll << 20);
+    c->stack_slots = c->cfg.stack_slots > 0 ? c->cfg.stack_slots : (1ll << 20);
+    c->result_ints = c->cfg.result_ints > 0 ? c->cfg.result_ints : (16ll << 20);
+    if (c->cfg.wait_limit_ms <= 0) c->cfg.wait_limit_ms = 10000;
+    *out = c.release();
+    return QC_OK;
+}
+
+extern "C" void qc_context_free(qc_context* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->cfg.device);
+    for (DevBuf* b : {&c->off, &c->adj, &c->off2, &c->adj2, &c->pos, &c->ids, &c->md, &c->ubt,
+                      &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws})
+        b->release();
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+// ------------------------------------------------------------------
+// graphs
+// ------------------------------------------------------------------
+
+extern "C" qc_status qc_graph_read_serialized(const char* path, qc_graph** out)
+{
+    if (!path || !out) return fail(QC_ERR_ARGS, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<qc_graph> g(new qc_graph());
+    std::string e = read_serialized(path, g->h);
+    if (!e.empty()) {
+        if (e.rfind("cannot open", 0) == 0) return fail(QC_ERR_IO, e);
+        return fail(QC_ERR_FORMAT, e);
+    }
+    e = validate(g->h, true);
+    if (!e.empty()) return fail(QC_ERR_FORMAT, e);
+    *out = g.release();
+    return QC_OK;
+}
+
+extern "C" qc_status qc_graph_from_csr2(int32_t n, const int64_t* off, const int32_t* adj,
+                                        const int64_t* off2, const int32_t* adj2, qc_graph** out)
+{
+    if (!out || n < 0 || (n > 0 && (!off || !off2))) return fail(QC_ERR_ARGS, "bad CSR arguments");
+    *out = nullptr;
+    std::unique_ptr<qc_graph> g(new qc_graph());
+    g->h.n = n;
+    g->h.off.assign(off, off + n + 1);
+    if (off[n] > 0 && !adj) return fail(QC_ERR_ARGS, "adj is NULL");
+    g->h.adj.assign(adj, adj + off[n]);
+    g->h.off2.assign(off2, off2 + n + 1);
+    if (off2[n] > 0 && !adj2) return fail(QC_ERR_ARGS, "adj2 is NULL");
+    g->h.adj2.assign(adj2, adj2 + off2[n]);
+    std::string e = validate(g->h, true);
+    if (!e.empty()) return fail(QC_ERR_FORMAT, e);
+    *out = g.release();
+    return QC_OK;
+}
+
+extern "C" qc_status qc_graph_write_serialized(const qc_graph* g, const char* path)
+{
+    if (!g || !path) return fail(QC_ERR_ARGS, "NULL argument");
+    std::string e = write_serialized(g->h, path);
+    return e.empty() ? QC_OK : fail(QC_ERR_IO, e);
+}
+
+extern "C" int32_t qc_graph_num_vertices(const qc_graph* g) { return g ? g->h.n : 0; }
+extern "C" int64_t qc_graph_num_entries(const qc_graph* g) { return g ? (int64_t)g->h.adj.size() : 0; }
+extern "C" int64_t qc_graph_num_twohop(const qc_graph* g) { return g ? (int64_t)g->h.adj2.size() : 0; }
+extern "C" const int64_t* qc_graph_offsets(const qc_graph* g) { return g ? g->h.off.data() : nullptr; }
+extern "C" const int32_t* qc_graph_neighbors(const qc_graph* g) { return g ? g->h.adj.data() : nullptr; }
+extern "C" const int64_t* qc_graph_twohop_offsets(const qc_graph* g) { return g ? g->h.off2.data() : nullptr; }
+extern "C" const int32_t* qc_graph_twohop_neighbors(const qc_graph* g) { return g ? g->h.adj2.data() : nullptr; }
+extern "C" void qc_graph_free(qc_graph* g) { delete g; }
+
+// ------------------------------------------------------------------
+// device kernels: root task record
+// ------------------------------------------------------------------
+
+__global__ void root_pos_kernel(const int32_t* ids, int t, int32_t* pos, int set)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < t) pos[ids[i]] = set ? i : -1;
+}
+
+// one warp per root vertex: mark its 1-hop and 2-hop neighbours inside the root
+__global__ void root_rows_kernel(const int64_t* off, const int32_t* adj, const int64_t* off2,
+                                 const int32_t* adj2, const int32_t* ids, int t, int W,
+                                 const int32_t* pos, uint32_t* A1, uint32_t* A2)
+{
+    int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < t; i += nw) {
+        int u = ids[i];
+        uint32_t* r1 = A1 + (int64_t)i * W;
+        uint32_t* r2 = A2 + (int64_t)i * W;
+        for (int64_t e = off[u] + lane; e < off[u + 1]; e += 32) {
+            int p = pos[adj[e]];
+            if (p >= 0) atomicOr(&r1[p >> 5], 1u << (p & 31));
+        }
+        for (int64_t e = off2[u] + lane; e < off2[u + 1]; e += 32) {
+            int p = pos[adj2[e]];
+            if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
+        }
+    }
+}
+
+// ------------------------------------------------------------------
+// mining
+// ------------------------------------------------------------------
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+double ms_since(clk::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+}
+
+template <class T> cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s)
+{
+    cudaError_t e = b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+} // namespace
+
+static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
+                          qc_result* r)
+{
+    auto t_all = clk::now();
+    const HostGraph& h = g->h;
+    cudaStream_t s = c->stream;
+    CK(cudaSetDevice(c->cfg.device));
+
+    // graph -> device (timed as load)
+    auto t_load = clk::now();
+    CK(upload(c->off, h.off, s));
+    CK(upload(c->adj, h.adj, s));
+    CK(upload(c->off2, h.off2, s));
+    CK(upload(c->adj2, h.adj2, s));
+    if (c->pos_n < h.n || !c->pos.p) {
+        CK(c->pos.ensure(sizeof(int32_t) * (size_t)std::max(h.n, 1)));
+        CK(cudaMemsetAsync(c->pos.p, 0xff, sizeof(int32_t) * (size_t)std::max(h.n, 1), s));
+        c->pos_n = h.n;
+    }
+    CK(cudaStreamSynchronize(s));
+    r->st.load_ms = ms_since(t_load);
+
+    // enumeration: level 0 + device expansion
+    auto t_enum = clk::now();
+    std::vector<int32_t> md, ubt;
+    gamma_tables(gamma, h.n, min_size, md, ubt);
+    std::vector<int32_t> ids;
+    int cov = 0;
+    build_root(h, md.data(), min_size, ids, cov);
+    r->st.root_size = (int64_t)ids.size();
+    if (ids.empty()) {
+        r->st.enum_ms = ms_since(t_enum);
+        r->st.total_ms = ms_since(t_all);
+        return QC_OK;
+    }
+    const int t = (int)ids.size();
+    const int W = words_for(t);
+    CK(upload(c->md, md, s));
+    CK(upload(c->ubt, ubt, s));
+    CK(upload(c->ids, ids, s));
+
+    int wpb = c->cfg.warps_per_block > 0 ? c->cfg.warps_per_block : 8;
+    int resident = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
+    if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
+    // a persistent launch: never more blocks than can be resident at once
+    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : resident;
+    int blocks = c->sms * bps;
+    int nwarps = blocks * wpb;
+    WsLayout L = ws_layout(t);
+    CK(c->ws.ensure((size_t)L.total * nwarps));
+    CK(c->ctl.ensure(sizeof(Control)));
+
+    std::vector<int32_t> flat;
+    for (int attempt = 0;; attempt++) {
+        CK(c->arena.ensure((size_t)c->arena_bytes));
+        CK(c->stack.ensure(sizeof(WorkItem) * (size_t)c->stack_slots));
+        CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
+        CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
+        CK(cudaMemsetAsync(c->slot.p, 0, sizeof(int32_t) * (size_t)c->stack_slots, s));
+
+        uint64_t rb = rec_bytes(t, W);
+        if ((int64_t)rb > c->arena_bytes) {
+            c->arena_bytes = (int64_t)rb * 4;
+            continue;
+        }
+        CK(cudaEventRecord(c->ev[0], s));
+        // root record: header, ids, zero l2 and matrices, then rows
+        char* rec = c->arena.as<char>();
+        CK(cudaMemsetAsync(rec, 0, rb, s));
+        TaskHdr hd{};
+        hd.t = t;
+        hd.m = 0;
+        hd.cov = cov;
+        hd.W = W;
+        CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(rec + rec_ids_off(), ids.data(), sizeof(int32_t) * t,
+                           cudaMemcpyHostToDevice, s));
+        root_pos_kernel<<<(t + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), t,
+                                                        c->pos.as<int32_t>(), 1);
+        root_rows_kernel<<<std::min(blocks * 4, (t + 7) / 8), 256, 0, s>>>(
+            c->off.as<int64_t>(), c->adj.as<int32_t>(), c->off2.as<int64_t>(),
+            c->adj2.as<int32_t>(), c->ids.as<int32_t>(), t, W, c->pos.as<int32_t>(),
+            (uint32_t*)(rec + rec_a1_off(t)), (uint32_t*)(rec + rec_a2_off(t, W)));
+        root_pos_kernel<<<(t + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), t,
+                                                        c->pos.as<int32_t>(), 0);
+        CK(cudaGetLastError());
+        c->launches += 3;
+
+        Control ctl{};
+        ctl.arena_top = rb;
+        ctl.arena_cap = (unsigned long long)c->arena_bytes;
+        ctl.result_cap = (unsigned long long)c->result_ints;
+        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots, INT32_MAX);
+        ctl.stack_top = 1;
+        ctl.pending = 1;
+        CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
+        WorkItem root{0, -1, -1};
+        CK(cudaMemcpyAsync(c->stack.p, &root, sizeof(root), cudaMemcpyHostToDevice, s));
+        int one = 1;
+        CK(cudaMemcpyAsync(c->slot.p, &one, sizeof(one), cudaMemcpyHostToDevice, s));
+
+        ExpandParams P{};
+        P.md = c->md.as<int32_t>();
+        P.ubt = c->ubt.as<int32_t>();
+        P.mdlen = (int32_t)md.size();
+        P.min_size = min_size;
+        P.ctl = c->ctl.as<Control>();
+        P.arena = c->arena.as<char>();
+        P.stack = c->stack.as<WorkItem>();
+        P.slot = c->slot.as<int32_t>();
+        P.results = c->results.as<int32_t>();
+        P.ws = c->ws.as<char>();
+        P.ws_stride = L.total;
+        P.max_t = t;
+        P.split = 8;
+        P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
+        CK(cudaEventRecord(c->ev[1], s));
+        expand_kernel<<<blocks, wpb * 32, 0, s>>>(P);
+        CK(cudaGetLastError());
+        c->launches += 1;
+        CK(cudaEventRecord(c->ev[2], s));
+        CK(cudaMemcpyAsync(&ctl, c->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        float kms = 0;
+        cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
+
+        if (ctl.status & ST_TASK_OVERFLOW) {
+            if (ctl.arena_top > ctl.arena_cap) c->arena_bytes *= 4;
+            if (ctl.stack_top >= ctl.stack_cap) c->stack_slots *= 4;
+            if (ctl.arena_top <= ctl.arena_cap && ctl.stack_top < ctl.stack_cap) {
+                c->arena_bytes *= 2;
+                c->stack_slots *= 2;
+            }
+            if (attempt < 6) continue;
+            return fail(QC_ERR_TASK_OVERFLOW, "task arena/stack exhausted after growing");
+        }
+        if (ctl.status & ST_RESULT_OVERFLOW) {
+            c->result_ints = std::max<int64_t>(c->result_ints * 4, (int64_t)ctl.result_top * 2);
+            if (attempt < 6) continue;
+            return fail(QC_ERR_RESULT_OVERFLOW, "result buffer exhausted after growing");
+        }
+        if (ctl.status & ST_TOO_LARGE) return fail(QC_ERR_TOO_LARGE, "task larger than workspace");
+        if (ctl.status & ST_ITER_LIMIT)
+            return fail(QC_ERR_ITER_LIMIT, "device wait gave up (site " +
+                                               std::to_string(ctl.wait_fail_where) + ")");
+        r->st.tasks = (int64_t)ctl.tasks;
+        r->st.branches = (int64_t)ctl.branches;
+        r->st.children = (int64_t)ctl.children;
+        r->st.emitted = (int64_t)ctl.emitted;
+        r->st.emitted_ints = (int64_t)ctl.result_top;
+        r->st.max_task = ctl.max_task;
+        r->st.arena_peak = (int64_t)ctl.arena_top;
+        r->st.kernel_launches = c->launches;
+        flat.resize((size_t)ctl.result_top);
+        if (!flat.empty())
+            CK(cudaMemcpyAsync(flat.data(), c->results.p, sizeof(int32_t) * flat.size(),
+                               cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        r->st.enum_ms = ms_since(t_enum);
+        (void)kms;
+        break;
+    }
+
+    auto t_filter = clk::now();
+    maximal_sets(flat.data(), (int64_t)flat.size(), r->sets, r->nsets);
+    r->st.filter_ms = ms_since(t_filter);
+    r->st.maximal = r->nsets;
+    if (c->cfg.keep_emitted) {
+        r->emitted.swap(flat);
+        r->emitted_sets = r->st.emitted;
+    }
+    r->st.total_ms = ms_since(t_all);
+    return QC_OK;
+}
+
+extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                             int32_t sched, qc_result** out)
+{
+    (void)sched;
+    if (!ctx || !g || !out) return fail(QC_ERR_ARGS, "NULL argument");
+    *out = nullptr;
+    if (!(gamma >= 0.5 && gamma <= 1.0))
+        return fail(QC_ERR_ARGS, "minimum degree ratio must be between .5 and 1 inclusive");
+    if (min_size <= 1) return fail(QC_ERR_ARGS, "minimum size must be greater than 1");
+    if (g->h.off2.size() != g->h.off.size()) return fail(QC_ERR_FORMAT, "graph has no 2-hop lists");
+    std::unique_ptr<qc_result> r(new qc_result());
+    qc_status st = mine_one(ctx, g, gamma, min_size, r.get());
+    if (st != QC_OK) return st;
+    *out = r.release();
+    return QC_OK;
+}
+
+extern "C" qc_status qc_mine_batch(qc_context* ctx, const qc_graph* const* graphs,
+                                   const double* gammas, const int32_t* min_sizes, int32_t count,
+                                   qc_result** outs)
+{
+    if (!ctx || !graphs || !gammas || !min_sizes || !outs || count < 0)
+        return fail(QC_ERR_ARGS, "NULL argument");
+    for (int32_t i = 0; i < count; i++) outs[i] = nullptr;
+    for (int32_t i = 0; i < count; i++) {
+        qc_status st = qc_mine(ctx, graphs[i], gammas[i], min_sizes[i], 0, &outs[i]);
+        if (st != QC_OK) {
+            for (int32_t j = 0; j < i; j++) qc_result_free(outs[j]);
+            for (int32_t j = 0; j < count; j++) outs[j] = nullptr;
+            return st;
+        }
+    }
+    return QC_OK;
+}
+
+// ------------------------------------------------------------------
+// results
+// ------------------------------------------------------------------
+
+extern "C" int64_t qc_result_count(const qc_result* r) { return r ? r->nsets : 0; }
+extern "C" const int32_t* qc_result_sets(const qc_result* r, int64_t* n_ints)
+{
+    if (!r) return nullptr;
+    if (n_ints) *n_ints = (int64_t)r->sets.size();
+    return r->sets.data();
+}
+extern "C" const int32_t* qc_result_emitted(const qc_result* r, int64_t* n_sets, int64_t* n_ints)
+{
+    if (!r) return nullptr;
+    if (n_sets) *n_sets = r->emitted_sets;
+    if (n_ints) *n_ints = (int64_t)r->emitted.size();
+    return r->emitted.data();
+}
+extern "C" const qc_stats* qc_result_stats(const qc_result* r) { return r ? &r->st : nullptr; }
+extern "C" qc_status qc_result_write(const qc_result* r, const char* path)
+{
+    if (!r || !path) return fail(QC_ERR_ARGS, "NULL argument");
+    std::string e = write_result(r->sets.data(), (int64_t)r->sets.size(), path);
+    return e.empty() ? QC_OK : fail(QC_ERR_IO, e);
+}
+extern "C" void qc_result_free(qc_result* r) { delete r; }
+
+// qc_graph_from_csr (device 2-hop builder) lives in twohop.cu
+
+std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
+                              std::vector<int32_t>& adj2);
+
+extern "C" qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int32_t* adj,
+                                       qc_graph** out)
+{
+    if (!out || n < 0 || (n > 0 && !off)) return fail(QC_ERR_ARGS, "bad CSR arguments");
+    *out = nullptr;
+    std::unique_ptr<qc_graph> g(new qc_graph());
+    g->h.n = n;
+    g->h.off.assign(off, off + n + 1);
+    if (off[n] > 0 && !adj) return fail(QC_ERR_ARGS, "adj is NULL");
+    g->h.adj.assign(adj, adj + off[n]);
+    std::string e = validate(g->h, false);
+    if (!e.empty()) return fail(QC_ERR_FORMAT, e);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(QC_ERR_NO_DEVICE, "no CUDA device visible");
+    e = qcb_twohop_device(g->h, g->h.off2, g->h.adj2);
+    if (!e.empty()) return fail(QC_ERR_CUDA, e);
+    *out = g.release();
+    return QC_OK;
+}

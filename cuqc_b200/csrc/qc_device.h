@@ -1,0 +1,123 @@
+// qc_device.h -- types shared by the host code and the expansion kernel.
+//
+// Device data layout (all in HBM, one set per context):
+//   * graph CSR (int64 offsets, int32 sorted rows) and 2-hop CSR;
+//   * md[k] = ceil(gamma*(k-1)) and ubt[d] = floor(d/gamma) tables, computed
+//     on the host in double exactly as the reference does (main.cu:526-533,
+//     main.cu:1905), so every device test is an integer comparison;
+//   * a task-record arena: each record holds one branch-and-bound node as
+//     its vertex ids plus its induced 1-hop and 2-hop adjacency as bit
+//     matrices (row v = W words), so children never re-read the CSR;
+//   * a LIFO stack of work items (record + branch range) with per-slot
+//     hand-off flags, a control block (counters, status) and a flat buffer
+//     of emitted vertex sets [k, id_1..id_k].
+#pragma once
+#include <stdint.h>
+
+namespace qcb {
+
+constexpr int kWarp = 32;
+
+// status bits written by the device
+enum : int {
+    ST_OK = 0,
+    ST_TASK_OVERFLOW = 1,   // arena or stack exhausted
+    ST_RESULT_OVERFLOW = 2, // emitted-set buffer exhausted
+    ST_ITER_LIMIT = 4,      // a bounded wait gave up
+    ST_TOO_LARGE = 8        // task larger than the workspace supports
+};
+
+struct Control {
+    unsigned long long arena_top;  // bytes of records written
+    unsigned long long arena_cap;
+    unsigned long long result_top; // ints of emitted sets written
+    unsigned long long result_cap;
+    int stack_top;
+    int stack_cap;
+    int pending;                   // work items pushed and not yet finished
+    int status;
+    unsigned long long tasks, branches, children, emitted, emitted_ints;
+    unsigned long long lookahead_hits;
+    int max_task;
+    int active_warps;              // warps still inside the work loop
+    unsigned long long wait_fail_where; // diagnostic: which wait gave up
+};
+
+struct WorkItem {
+    unsigned long long rec; // byte offset of the task record in the arena
+    int q_lo;               // first branch position, -1: fresh task
+    int q_hi;               // last branch position (inclusive)
+};
+
+// Task record header; the record continues with
+//   int32 ids[t]            (padded to 16 B)
+//   int32 l2[t]             (lookahead 2-hop counts; 0 until computed)
+//   uint32 A1[t][W]         (A1[v] bit w: w in N(v))
+//   uint32 A2[t][W]         (A2[v] bit w: w in N2(v))
+struct TaskHdr {
+    int32_t t;   // vertices
+    int32_t m;   // members are positions [0, m)
+    int32_t cov; // covered candidates right after the members (root only)
+    int32_t W;   // words per bit row
+    int32_t pad[4];
+};
+
+__host__ __device__ inline uint64_t align16(uint64_t x) { return (x + 15) & ~uint64_t(15); }
+__host__ __device__ inline int words_for(int t) { return (t + 31) >> 5; }
+__host__ __device__ inline uint64_t rec_ids_off() { return sizeof(TaskHdr); }
+__host__ __device__ inline uint64_t rec_l2_off(int t) { return sizeof(TaskHdr) + align16(4ull * t); }
+__host__ __device__ inline uint64_t rec_a1_off(int t) { return rec_l2_off(t) + align16(4ull * t); }
+__host__ __device__ inline uint64_t rec_a2_off(int t, int W) {
+    return rec_a1_off(t) + align16(4ull * t * W);
+}
+__host__ __device__ inline uint64_t rec_bytes(int t, int W) {
+    return rec_a2_off(t, W) + align16(4ull * t * W);
+}
+
+struct ExpandParams {
+    const int32_t* md;   // md[0 .. mdlen)
+    const int32_t* ubt;  // floor(d / gamma), d in [0 .. mdlen)
+    int32_t mdlen;
+    int32_t min_size;
+    Control* ctl;
+    char* arena;
+    WorkItem* stack;
+    int32_t* slot;       // 0 free, 1 full, 2 being written, 3 being read
+    int32_t* results;
+    char* ws;            // per-warp workspace
+    int64_t ws_stride;   // bytes per warp
+    int32_t max_t;       // largest task the workspace holds
+    int32_t split;       // branches per work item before splitting
+    int64_t wait_ns;     // give up a wait after this long without progress
+};
+
+// Per-warp workspace layout for tasks of up to max_t vertices.
+struct WsLayout {
+    int64_t indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
+    int64_t total;
+};
+
+__host__ __device__ inline WsLayout ws_layout(int max_t)
+{
+    WsLayout L;
+    int64_t t = max_t + 64;
+    int64_t tp = 1; // the child sort pads to a power of two
+    while (tp < max_t) tp <<= 1;
+    tp += 64;
+    int64_t W = words_for(max_t) + 2;
+    int64_t o = 0;
+    L.indeg = o;    o += align16(4 * t);
+    L.exdeg = o;    o += align16(4 * t);
+    L.aux = o;      o += align16(4 * t);
+    L.hist = o;     o += align16(4 * (t + 2));
+    L.pref_cnt = o; o += align16(4 * (t + 2));
+    L.pref_sum = o; o += align16(8 * (t + 2));
+    L.sel = o;      o += align16(4 * tp);
+    L.key_hi = o;   o += align16(8 * tp);
+    L.key_lo = o;   o += align16(8 * tp);
+    L.masks = o;    o += align16(4 * W * 12);
+    L.total = align16(o);
+    return L;
+}
+
+} // namespace qcb

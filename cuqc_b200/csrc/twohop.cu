@@ -1,0 +1,194 @@
+// twohop.cu -- 2-hop lists on the GPU (replaces the offline preprocessing of
+// Mike12041204/cuQC adjToSer.cpp:115-156):
+//     N2(v) = sorted(N(v) u N(N(v)) minus {v})
+//
+// One warp per vertex.  Each warp owns a bitmap of n bits in global memory
+// (L2-resident for moderate n) and a list of the bitmap words it touched.
+// Lanes stream N(v) and every N(u), u in N(v), with coalesced loads and set
+// bits with atomicOr; a word seen for the first time is appended to the
+// touched list.  Pass 1 counts set bits per vertex, a scan gives the offsets,
+// pass 2 repeats the marking, sorts the touched word indices (warp bitonic)
+// and writes each word's set bits in order -- ascending ids -- then clears
+// the touched words.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/qc.h"
+#include "host.h"
+
+using namespace qcb;
+
+namespace {
+
+constexpr int kTwohopWarpsPerBlock = 8;
+
+__device__ void mark_row(const int64_t* off, const int32_t* adj, int v, uint32_t* bm,
+                         int32_t* touched, int* ntouched, int lane)
+{
+    auto mark = [&](int w) {
+        uint32_t b = 1u << (w & 31);
+        uint32_t old = atomicOr(&bm[w >> 5], b);
+        if (old == 0) {
+            int k = atomicAdd(ntouched, 1);
+            touched[k] = w >> 5;
+        }
+    };
+    for (int64_t e = off[v] + lane; e < off[v + 1]; e += 32) mark(adj[e]);
+    for (int64_t e = off[v]; e < off[v + 1]; e++) {
+        int u = adj[e];
+        for (int64_t f = off[u] + lane; f < off[u + 1]; f += 32) {
+            int w = adj[f];
+            if (w != v) mark(w);
+        }
+    }
+    __syncwarp();
+}
+
+// pass 1: counts; pass 2: write rows (off2 known)
+__global__ void twohop_kernel(int n, const int64_t* off, const int32_t* adj, uint32_t* bitmaps,
+                              int64_t bm_words, int32_t* touched_all, int64_t touched_cap,
+                              int* ntouched_all, int64_t* count_out, const int64_t* off2,
+                              int32_t* adj2)
+{
+    int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nw = (gridDim.x * blockDim.x) >> 5;
+    uint32_t* bm = bitmaps + (int64_t)warp * bm_words;
+    int32_t* touched = touched_all + (int64_t)warp * touched_cap;
+    int* nt = ntouched_all + warp;
+    for (int v = warp; v < n; v += nw) {
+        if (lane == 0) *nt = 0;
+        __syncwarp();
+        mark_row(off, adj, v, bm, touched, nt, lane);
+        // a self loop in N(v) keeps v (as the reference keeps it); v is never
+        // added through N(N(v))
+        int k = *(volatile int*)nt;
+        if (!off2) {
+            int c = 0;
+            for (int i = lane; i < k; i += 32) c += __popc(bm[touched[i]]);
+            for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0) count_out[v] = c;
+        } else {
+            // sort touched word indices ascending (bitonic, padded with INT_MAX)
+            int N = 1;
+            while (N < k) N <<= 1;
+            for (int i = k + lane; i < N; i += 32) touched[i] = 0x7fffffff;
+            __syncwarp();
+            for (int s = 2; s <= N; s <<= 1)
+                for (int j = s >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < N; i += 32) {
+                        int p = i ^ j;
+                        if (p > i) {
+                            int a = touched[i], b = touched[p];
+                            bool up = (i & s) == 0;
+                            if ((a > b) == up) {
+                                touched[i] = b;
+                                touched[p] = a;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            // write ids in ascending order
+            int64_t base = off2[v];
+            int carry = 0;
+            for (int c0 = 0; c0 < k; c0 += 32) {
+                int i = c0 + lane;
+                uint32_t word = i < k ? bm[touched[i]] : 0u;
+                int cnt = __popc(word);
+                int inc = cnt;
+                for (int o = 1; o < 32; o <<= 1) {
+                    int y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += y;
+                }
+                int at = carry + inc - cnt;
+                int wbase = i < k ? touched[i] * 32 : 0;
+                while (word) {
+                    int b = __ffs(word) - 1;
+                    word &= word - 1;
+                    adj2[base + at++] = wbase + b;
+                }
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < k; i += 32) bm[touched[i]] = 0;
+        __syncwarp();
+    }
+}
+
+std::string g_th_err;
+
+} // namespace
+
+#define TCK(call)                                                              \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) {                                               \
+            g_th_err = std::string(#call) + ": " + cudaGetErrorString(e_);     \
+            goto done;                                                         \
+        }                                                                      \
+    } while (0)
+
+// Build 2-hop lists on device 0.  Returns "" or an error message.
+std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
+                              std::vector<int32_t>& adj2)
+{
+    const int n = h.n;
+    off2.assign((size_t)n + 1, 0);
+    adj2.clear();
+    if (n == 0) return "";
+    int64_t *d_off = nullptr, *d_cnt = nullptr, *d_off2 = nullptr;
+    int32_t *d_adj = nullptr, *d_touched = nullptr, *d_adj2 = nullptr;
+    uint32_t* d_bm = nullptr;
+    int* d_nt = nullptr;
+    int sms = 0;
+    int64_t bm_words = ((int64_t)n + 31) / 32;
+    int64_t touched_cap = 1;
+    int blocks = 0, nwarps = 0;
+    std::vector<int64_t> cnt;
+    g_th_err.clear();
+    while (touched_cap < bm_words) touched_cap <<= 1;
+    TCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+    blocks = sms * 2;
+    nwarps = blocks * kTwohopWarpsPerBlock;
+    TCK(cudaMalloc(&d_off, sizeof(int64_t) * (n + 1)));
+    TCK(cudaMalloc(&d_adj, sizeof(int32_t) * std::max<size_t>(h.adj.size(), 1)));
+    TCK(cudaMalloc(&d_cnt, sizeof(int64_t) * n));
+    TCK(cudaMalloc(&d_bm, sizeof(uint32_t) * bm_words * nwarps));
+    TCK(cudaMalloc(&d_touched, sizeof(int32_t) * touched_cap * nwarps));
+    TCK(cudaMalloc(&d_nt, sizeof(int) * nwarps));
+    TCK(cudaMemset(d_bm, 0, sizeof(uint32_t) * bm_words * nwarps));
+    TCK(cudaMemcpy(d_off, h.off.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
+    if (!h.adj.empty())
+        TCK(cudaMemcpy(d_adj, h.adj.data(), sizeof(int32_t) * h.adj.size(), cudaMemcpyHostToDevice));
+    twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32>>>(n, d_off, d_adj, d_bm, bm_words, d_touched,
+                                                         touched_cap, d_nt, d_cnt, nullptr, nullptr);
+    TCK(cudaGetLastError());
+    cnt.resize((size_t)n);
+    TCK(cudaMemcpy(cnt.data(), d_cnt, sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
+    for (int v = 0; v < n; v++) off2[(size_t)v + 1] = off2[(size_t)v] + cnt[(size_t)v];
+    adj2.resize((size_t)off2[(size_t)n]);
+    TCK(cudaMalloc(&d_off2, sizeof(int64_t) * (n + 1)));
+    TCK(cudaMalloc(&d_adj2, sizeof(int32_t) * std::max<size_t>(adj2.size(), 1)));
+    TCK(cudaMemcpy(d_off2, off2.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
+    twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32>>>(n, d_off, d_adj, d_bm, bm_words, d_touched,
+                                                         touched_cap, d_nt, nullptr, d_off2, d_adj2);
+    TCK(cudaGetLastError());
+    if (!adj2.empty())
+        TCK(cudaMemcpy(adj2.data(), d_adj2, sizeof(int32_t) * adj2.size(), cudaMemcpyDeviceToHost));
+done:
+    cudaFree(d_off);
+    cudaFree(d_adj);
+    cudaFree(d_cnt);
+    cudaFree(d_bm);
+    cudaFree(d_touched);
+    cudaFree(d_nt);
+    cudaFree(d_off2);
+    cudaFree(d_adj2);
+    return g_th_err;
+}

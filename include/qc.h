@@ -1,0 +1,155 @@
+/*
+ * qc.h -- C ABI of the B200 maximal gamma-quasi-clique miner (libqc.so).
+ *
+ * Plain C: pointers, sizes and status codes; no exits inside the library.
+ * Ownership: every object the library creates is released with the
+ * matching qc_*_free.  Threading: one host thread per qc_context at a time;
+ * distinct contexts may be used concurrently (each owns its CUDA stream and
+ * device buffers).
+ *
+ * The reference cuQC (Mike12041204/cuQC) has no library interface; its only
+ * "plugin API" is the process CLI (main.cu:416-519) over a serialized graph
+ * file (main.cu:82-131) and a result file (main.cu:4641-4652, 4881-4937).
+ * Each entry point below names the reference routine whose job it takes
+ * over, so a maintainer can see which part of main.cu a call replaces.
+ */
+#ifndef QC_H
+#define QC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    QC_OK = 0,
+    QC_ERR_ARGS = 1,            /* argument out of range (gamma, min_size, NULL) */
+    QC_ERR_IO = 2,              /* a file could not be opened, read or written   */
+    QC_ERR_FORMAT = 3,          /* malformed serialized graph                    */
+    QC_ERR_CUDA = 4,            /* CUDA runtime error (message: qc_last_error)   */
+    QC_ERR_NOMEM = 5,           /* host or device allocation failed              */
+    QC_ERR_TASK_OVERFLOW = 6,   /* device task stack or record arena exhausted   */
+    QC_ERR_RESULT_OVERFLOW = 7, /* device result buffer exhausted                */
+    QC_ERR_ITER_LIMIT = 8,      /* a bounded device wait gave up                 */
+    QC_ERR_TOO_LARGE = 9,       /* a task exceeds the supported vertex count     */
+    QC_ERR_NO_DEVICE = 10       /* no CUDA device / library built without it     */
+} qc_status;
+
+/* Human-readable text for a status code. */
+const char* qc_status_str(qc_status s);
+/* Detail of the last failure on the calling thread (never NULL). */
+const char* qc_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* graphs                                                               */
+/* ------------------------------------------------------------------ */
+
+typedef struct qc_graph qc_graph; /* host CSR (+ 2-hop CSR) of an undirected graph */
+
+/* Parse the reference's serialized graph file: n, 2|E|, #2-hop entries,
+ * 1-hop neighbours, 1-hop offsets, 2-hop neighbours, 2-hop offsets,
+ * whitespace separated.  Replaces CPU_Graph(ifstream&) (main.cu:96-121). */
+qc_status qc_graph_read_serialized(const char* path, qc_graph** out);
+
+/* Adopt a CSR (offsets int64[n+1], sorted neighbour rows int32[off[n]]) and
+ * the matching 2-hop CSR.  The arrays are copied.  Replaces the loader's
+ * arrays of CPU_Graph (main.cu:89-94). */
+qc_status qc_graph_from_csr2(int32_t n, const int64_t* off, const int32_t* adj,
+                             const int64_t* off2, const int32_t* adj2, qc_graph** out);
+
+/* Adopt a 1-hop CSR and build the 2-hop lists
+ * sorted(N(v) u N(N(v)) minus {v}) on the GPU.  Replaces the offline
+ * adjToSer preprocessing (adjToSer.cpp:115-156). */
+qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int32_t* adj, qc_graph** out);
+
+/* Write the graph in the serialized format (adjToSer.cpp:159-204). */
+qc_status qc_graph_write_serialized(const qc_graph* g, const char* path);
+
+int32_t qc_graph_num_vertices(const qc_graph* g);
+int64_t qc_graph_num_entries(const qc_graph* g);   /* 2|E|            */
+int64_t qc_graph_num_twohop(const qc_graph* g);    /* 2-hop entries  */
+/* Read-only views of the host arrays (valid until qc_graph_free). */
+const int64_t* qc_graph_offsets(const qc_graph* g);
+const int32_t* qc_graph_neighbors(const qc_graph* g);
+const int64_t* qc_graph_twohop_offsets(const qc_graph* g);
+const int32_t* qc_graph_twohop_neighbors(const qc_graph* g);
+void qc_graph_free(qc_graph* g);
+
+/* ------------------------------------------------------------------ */
+/* contexts                                                             */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    int32_t device;              /* CUDA device ordinal                               */
+    int32_t warps_per_block;     /* 0: autotuned                                      */
+    int32_t blocks_per_sm;       /* 0: autotuned                                      */
+    int64_t arena_bytes;         /* task-record arena; 0: default                     */
+    int64_t stack_slots;         /* task stack capacity; 0: default                   */
+    int64_t result_ints;         /* emitted-set buffer (ints); 0: default             */
+    int32_t keep_emitted;        /* 1: keep the raw emitted multiset in the result    */
+    int32_t wait_limit_ms;       /* bound on any device wait without progress; 0: 10000 */
+} qc_config;
+
+/* Fill a config with defaults (device 0, everything autotuned). */
+void qc_config_default(qc_config* cfg);
+
+typedef struct qc_context qc_context;
+
+/* Create a context: CUDA stream + device buffers sized by cfg.
+ * Replaces allocate_memory (main.cu:695-843). */
+qc_status qc_context_create(const qc_config* cfg, qc_context** out);
+void qc_context_free(qc_context* ctx);
+
+/* ------------------------------------------------------------------ */
+/* mining                                                               */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    double load_ms;        /* host->device copy of the graph                  */
+    double enum_ms;        /* level 0 + expansion on the device (CUDA events)  */
+    double filter_ms;      /* non-maximal removal on the device               */
+    double total_ms;       /* whole call, host wall clock                      */
+    int64_t tasks;         /* tasks expanded                                   */
+    int64_t branches;      /* add-one-vertex branches                          */
+    int64_t children;      /* child tasks written                              */
+    int64_t emitted;       /* quasi-cliques emitted before the maximal filter  */
+    int64_t emitted_ints;  /* ints of emitted sets (sizes + ids)               */
+    int64_t maximal;       /* sets in the result                               */
+    int64_t root_size;     /* vertices in the root task                        */
+    int64_t max_task;      /* largest task                                     */
+    int64_t arena_peak;    /* bytes of task records written                    */
+    int64_t kernel_launches;
+} qc_stats;
+
+typedef struct qc_result qc_result;
+
+/* Enumerate the maximal gamma-quasi-cliques of size >= min_size.
+ * gamma in [0.5, 1], min_size > 1 (main.cu:437-446).  sched is accepted for
+ * CLI compatibility (0 dynamic / 1 static, main.cu:447-453); the device work
+ * queue is always dynamic.  Replaces search() + RemoveNonMax()
+ * (main.cu:535-692, 4939-4960). */
+qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                  int32_t sched, qc_result** out);
+
+/* Mine `count` independent instances in one persistent launch (each with
+ * its own graph, gamma and min_size).  outs[i] receives instance i's result. */
+qc_status qc_mine_batch(qc_context* ctx, const qc_graph* const* graphs, const double* gammas,
+                        const int32_t* min_sizes, int32_t count, qc_result** outs);
+
+/* Result access.  Sets are sorted ascending and listed in lexicographic
+ * order of their id sequences, as the reference's result file. */
+int64_t qc_result_count(const qc_result* r);
+/* Flat [k, id_1 .. id_k] per set; *n_ints receives the length. */
+const int32_t* qc_result_sets(const qc_result* r, int64_t* n_ints);
+/* Raw emitted multiset (only with keep_emitted), flat [k, ids..]. */
+const int32_t* qc_result_emitted(const qc_result* r, int64_t* n_sets, int64_t* n_ints);
+const qc_stats* qc_result_stats(const qc_result* r);
+/* Write "<k> v1 .. vk \n" lines (main.cu:4641-4652). */
+qc_status qc_result_write(const qc_result* r, const char* path);
+void qc_result_free(qc_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QC_H */

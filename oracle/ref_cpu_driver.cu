@@ -1,0 +1,107 @@
+// ref_cpu_driver.cu -- TEST INFRASTRUCTURE: runs the reference cuQC's own
+// serial CPU enumeration (its host routines initialize_tasks, h_expand_level,
+// flush_cliques, RemoveNonMax) without touching a GPU.
+//
+// The reference source is compiled from where it lies (the include path is
+// given by oracle/Makefile); nothing of it is copied here.  The reference's
+// `main` is renamed so this file can provide an extern "C" entry point.  Only
+// the host-side allocation of the reference's allocate_memory (main.cu:695-843)
+// is restated, with capacities chosen by the caller, because the reference's
+// version also allocates ~35 GB of device memory.
+//
+// The loop mirrors the reference's host loop (main.cu:576-590) but keeps
+// calling h_expand_level until the enumeration is complete, i.e. the
+// reference's own CPU path with CPU_LEVELS raised to infinity.  Cliques are
+// flushed to the temp file after every level (main.cu:580-582 flushes only
+// above a threshold; flushing more often changes nothing but memory use).
+#define main cuqc_reference_main
+#include "main.cu"
+#undef main
+
+extern "C" int refcpu_run(const char* graph_path, const char* gamma_str, int min_size,
+                          const char* temp_path, const char* out_path,
+                          long long task_vertex_cap, long long buffer_vertex_cap,
+                          long long buffer_task_cap, long long clique_cap,
+                          long long* levels_out)
+{
+    ifstream gs(graph_path, ios::in);
+    if (!gs.is_open()) return -1;
+    CPU_Graph hg(gs);
+    gs.close();
+    minimum_degree_ratio = atof(gamma_str);
+    minimum_clique_size = min_size;
+    calculate_minimum_degrees(hg);
+
+    CPU_Data hd;
+    CPU_Cliques hc;
+    hd.tasks1_count = new uint64_t;
+    hd.tasks1_offset = new uint64_t[EXPAND_THRESHOLD + 1];
+    hd.tasks1_vertices = new Vertex[task_vertex_cap];
+    hd.tasks1_offset[0] = 0;
+    *hd.tasks1_count = 0;
+    hd.tasks2_count = new uint64_t;
+    hd.tasks2_offset = new uint64_t[EXPAND_THRESHOLD + 1];
+    hd.tasks2_vertices = new Vertex[task_vertex_cap];
+    hd.tasks2_offset[0] = 0;
+    *hd.tasks2_count = 0;
+    hd.buffer_count = new uint64_t;
+    hd.buffer_offset = new uint64_t[buffer_task_cap];
+    hd.buffer_vertices = new Vertex[buffer_vertex_cap];
+    hd.buffer_offset[0] = 0;
+    *hd.buffer_count = 0;
+    hd.current_level = new uint64_t;
+    hd.maximal_expansion = new bool;
+    hd.dumping_cliques = new bool;
+    *hd.current_level = 0;
+    *hd.maximal_expansion = false;
+    *hd.dumping_cliques = false;
+    int nn = hg.number_of_vertices + 1;
+    hd.vertex_order_map = new int[nn];
+    hd.remaining_candidates = new int[2 * nn];
+    hd.removed_candidates = new int[2 * nn];
+    hd.remaining_count = new int;
+    hd.removed_count = new int;
+    hd.candidate_indegs = new int[2 * nn];
+    memset(hd.vertex_order_map, -1, sizeof(int) * nn);
+    hc.cliques_count = new uint64_t;
+    hc.cliques_vertex = new int[clique_cap];
+    hc.cliques_offset = new uint64_t[clique_cap];
+    hc.cliques_offset[0] = 0;
+    *hc.cliques_count = 0;
+
+    ofstream temp(temp_path);
+    initialize_tasks(hg, hd);
+    long long levels = 0;
+    while (!*hd.maximal_expansion) {
+        h_expand_level(hg, hd, hc);
+        flush_cliques(hc, temp);
+        levels++;
+    }
+    flush_cliques(hc, temp);
+    temp.close();
+    if (levels_out) *levels_out = levels;
+
+    // RemoveNonMax dereferences an empty prefix tree (main.cu:4834); only
+    // call it when the temp file holds at least one set.
+    int rc = 0;
+    {
+        ifstream chk(temp_path);
+        int first;
+        if (chk >> first) {
+            RemoveNonMax((char*)temp_path, (char*)out_path);
+        } else {
+            ofstream empty(out_path);
+            rc = 1;
+        }
+    }
+    delete hd.tasks1_count; delete[] hd.tasks1_offset; delete[] hd.tasks1_vertices;
+    delete hd.tasks2_count; delete[] hd.tasks2_offset; delete[] hd.tasks2_vertices;
+    delete hd.buffer_count; delete[] hd.buffer_offset; delete[] hd.buffer_vertices;
+    delete hd.current_level; delete hd.maximal_expansion; delete hd.dumping_cliques;
+    delete[] hd.vertex_order_map; delete[] hd.remaining_candidates;
+    delete[] hd.removed_candidates; delete hd.remaining_count; delete hd.removed_count;
+    delete[] hd.candidate_indegs;
+    delete hc.cliques_count; delete[] hc.cliques_vertex; delete[] hc.cliques_offset;
+    delete[] minimum_degrees;
+    return rc;
+}

@@ -1,0 +1,66 @@
+"""Builds and drives the CPU-emulated expansion kernel (TEST INFRASTRUCTURE).
+
+The product kernel source is compiled by g++ against tests/emu/cuda_emu.h;
+each emulated lane is a host thread.  Used only by the CPU test suite.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+SO = os.path.join(HERE, "_build", "libqc_emu.so")
+SRCS = [os.path.join(HERE, "emu_expand.cpp"), os.path.join(ROOT, "cuqc_b200", "csrc", "host.cpp")]
+DEPS = SRCS + [os.path.join(HERE, "cuda_emu.h"),
+               os.path.join(ROOT, "cuqc_b200", "csrc", "expand_kernel.cuh"),
+               os.path.join(ROOT, "cuqc_b200", "csrc", "qc_device.h"),
+               os.path.join(ROOT, "cuqc_b200", "csrc", "host.h")]
+
+_lib = None
+
+
+def build():
+    newest = max(os.path.getmtime(p) for p in DEPS)
+    if os.path.exists(SO) and os.path.getmtime(SO) >= newest:
+        return
+    os.makedirs(os.path.dirname(SO), exist_ok=True)
+    subprocess.check_call(["g++", "-std=c++20", "-O1", "-g", "-pthread", "-shared", "-fPIC",
+                           "-Wno-unused-variable", "-o", SO] + SRCS)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(SO)
+        P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+        L.emu_mine.argtypes = [C.c_int, P64, P32, P64, P32, C.c_double, C.c_int, C.c_int, C.c_int,
+                               C.c_longlong, P64, C.POINTER(P32), P64]
+        L.emu_mine.restype = C.c_int
+        L.emu_free.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20):
+    """Emitted multiset (flat [k, ids..]) and counters of the emulated kernel."""
+    L = lib()
+    off, adj = np.ascontiguousarray(g.off, np.int64), np.ascontiguousarray(g.adj, np.int32)
+    off2, adj2 = np.ascontiguousarray(g.off2, np.int64), np.ascontiguousarray(g.adj2, np.int32)
+    ni = C.c_int64()
+    buf = C.POINTER(C.c_int32)()
+    cnt = np.zeros(8, np.int64)
+    st = L.emu_mine(int(g.n), off.ctypes.data_as(P64 := C.POINTER(C.c_int64)),
+                    adj.ctypes.data_as(C.POINTER(C.c_int32)), off2.ctypes.data_as(P64),
+                    adj2.ctypes.data_as(C.POINTER(C.c_int32)), float(gamma), int(min_size),
+                    int(warps), int(split), int(arena_bytes), C.byref(ni), C.byref(buf),
+                    cnt.ctypes.data_as(P64))
+    flat = np.zeros(0, np.int32)
+    if ni.value:
+        flat = np.ctypeslib.as_array(buf, shape=(ni.value,)).copy()
+        L.emu_free(C.cast(buf, C.c_void_p))
+    keys = ["tasks", "branches", "children", "emitted", "lookahead_hits", "status", "max_task",
+            "arena_bytes"]
+    return flat, dict(zip(keys, (int(x) for x in cnt))), st

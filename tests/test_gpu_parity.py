@@ -1,0 +1,106 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference, on a B200."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import cuqc_b200 as Q
+from conftest import GOLDEN, golden_cases, load_case, parse_result
+from cuqc_b200 import graphs
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+CASES = golden_cases()
+
+
+def canon(flat):
+    return sorted(tuple(sorted(s)) for s in oracle.unpack(flat))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = Q.Context(device=0, keep_emitted=True)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_golden_case(ctx, case):
+    g, path, gamma, ms, _ = load_case(case)
+    res = ctx.mine(g, float(gamma), ms)
+    want_flat, st = oracle.mine(g, float(gamma), ms, "clean")
+    # the device emits exactly the oracle's multiset of quasi-cliques
+    assert canon(res.emitted) == canon(want_flat)
+    assert res.stats["tasks"] == st["tasks"]
+    assert res.stats["branches"] == st["branches"]
+    assert res.sets == oracle.maximal(want_flat)
+    refbin = os.path.join(GOLDEN, case["name"] + ".refbin.result")
+    if os.path.exists(refbin):
+        assert res.text() == open(refbin).read()
+
+
+@pytest.mark.parametrize("seed", range(300, 316))
+def test_random_graphs(ctx, seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(20, 120))
+    p = float(rng.uniform(0.05, 0.35))
+    g = graphs.random_small(n, p, seed, planted=int(rng.integers(0, 5)),
+                            size=int(rng.integers(6, 18)), density=float(rng.uniform(0.85, 1)))
+    gamma = [0.7, 0.75, 0.8, 0.85, 0.9, 0.95, 1.0][seed % 7]
+    ms = int(rng.integers(4, 10))
+    want_flat, st = oracle.mine(g, gamma, ms, "clean")
+    res = ctx.mine(g, gamma, ms)
+    assert canon(res.emitted) == canon(want_flat)
+    assert res.sets == oracle.maximal(want_flat)
+
+
+def test_small_arena_grows_and_stays_exact():
+    g = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
+    with Q.Context(device=0, arena_bytes=1 << 16, stack_slots=64, result_ints=256) as c:
+        res = c.mine(g, 0.8, 10)
+    assert res.sets == oracle.solve(g, 0.8, 10)[0]
+
+
+def test_repeated_calls_reuse_context(ctx):
+    g = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
+    a = ctx.mine(g, 0.8, 10).sets
+    b = ctx.mine(g, 0.8, 10).sets
+    assert a == b == oracle.solve(g, 0.8, 10)[0]
+
+
+def test_empty_result(ctx):
+    case = [c for c in CASES if c["refcpu_maximal"] == 0][0]
+    g, path, gamma, ms, _ = load_case(case)
+    res = ctx.mine(g, float(gamma), ms)
+    assert res.sets == []
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_device_twohop_matches(seed):
+    g = graphs.random_small(200, 0.04 + 0.02 * seed, seed, planted=2, size=12)
+    base = graphs.Graph(n=g.n, off=g.off, adj=g.adj)
+    dg = Q.DeviceGraph.from_graph(base)
+    back = dg.to_graph()
+    assert np.array_equal(back.off2, g.off2) and np.array_equal(back.adj2, g.adj2)
+
+
+def test_cli_matches_reference_binary_output():
+    case = [c for c in CASES if c["name"] == "er1000_planted"][0]
+    g, path, gamma, ms, _ = load_case(case)
+    d = tempfile.mkdtemp()
+    out = os.path.join(d, "out.txt")
+    rc, stdout = Q.cli(path, gamma, ms, out, 0, cwd=d)
+    assert rc == 0, stdout
+    lines = [l.split(":")[1] if l.startswith("--->") else l for l in stdout.splitlines()]
+    assert stdout.splitlines()[0] == ">:PRE-PROCESSING"
+    assert ">:NUMBER OF MAXIMAL CLIQUES: 1365" in stdout
+    assert stdout.splitlines()[-1] == ">:PROGRAM END"
+    for key in ("LOADING TIME", "ENUMERATION TIME", "REMOVE NON-MAX TIME", "TOTAL TIME"):
+        assert ("--->:%s: " % key) in stdout
+    got = open(out).read()
+    refbin = os.path.join(GOLDEN, case["name"] + ".refbin.result")
+    expect = open(refbin).read() if os.path.exists(refbin) else oracle.result_text(
+        oracle.solve(g, float(gamma), ms, "clean")[0])
+    assert got == expect
