@@ -36,7 +36,7 @@ EXPORTS = [
     "qc_graph_from_csr", "qc_graph_write_serialized", "qc_graph_num_vertices",
     "qc_graph_num_entries", "qc_graph_num_twohop", "qc_graph_offsets", "qc_graph_neighbors",
     "qc_graph_twohop_offsets", "qc_graph_twohop_neighbors", "qc_graph_free", "qc_config_default",
-    "qc_context_create", "qc_context_free", "qc_mine", "qc_mine_batch", "qc_result_count",
+    "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
 ]
 
@@ -58,7 +58,9 @@ class Stats(C.Structure):
     _fields_ = [("load_ms", C.c_double), ("enum_ms", C.c_double), ("filter_ms", C.c_double),
                 ("total_ms", C.c_double)] + [(k, C.c_int64) for k in (
                     "tasks", "branches", "children", "emitted", "emitted_ints", "maximal",
-                    "root_size", "max_task", "arena_peak", "kernel_launches")]
+                    "root_size", "max_task", "arena_peak", "kernel_launches")] + [
+                    ("kernel_ms", C.c_double)] + [(k, C.c_int64) for k in (
+                    "parent_vertices", "p_rows", "child_vertices")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -101,6 +103,9 @@ def lib():
         L.qc_config_default.argtypes = [C.POINTER(Config)]
         L.qc_context_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
         L.qc_context_free.argtypes = [vp]
+        L.qc_context_upload.argtypes = [vp, vp]
+        L.qc_context_stream.argtypes = [vp]
+        L.qc_context_stream.restype = vp
         L.qc_mine.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.POINTER(vp)]
         L.qc_mine_batch.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_double), P32, C.c_int32,
                                     C.POINTER(vp)]
@@ -232,6 +237,17 @@ class Context:
             return Result(sets=_flat_to_sets(flat), stats=st, emitted=emitted)
         finally:
             L.qc_result_free(r)
+
+    def upload(self, g):
+        """Stage a graph on the device; later mine() calls on it skip the copy."""
+        dg = g if isinstance(g, DeviceGraph) else DeviceGraph.from_graph(g)
+        _check(lib().qc_context_upload(self.h, dg.h))
+        return dg
+
+    @property
+    def stream(self):
+        """The context's cudaStream_t as an integer."""
+        return lib().qc_context_stream(self.h)
 
     def mine(self, g, gamma, min_size, sched=0):
         dg = g if isinstance(g, DeviceGraph) else DeviceGraph.from_graph(g)

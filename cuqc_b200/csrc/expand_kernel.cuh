@@ -751,6 +751,7 @@ __device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, co
     __syncwarp();
     if (lane == 0) {
         atomicAdd(&P.ctl->children, 1ull);
+        atomicAdd(&P.ctl->child_vertices, (unsigned long long)tc);
         atomicMax(&P.ctl->max_task, tc);
         __threadfence();
         WorkItem it;
@@ -797,7 +798,13 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
     const uint32_t* r2q = T.A2 + (int64_t)q * W;
     for (int w = lane; w < W; w += 32) D[w] = PRE[w] & r2q[w];
     __syncwarp();
-    if (lane == 0) atomicAdd(&P.ctl->branches, 1ull);
+    if (lane == 0) {
+        atomicAdd(&P.ctl->branches, 1ull);
+        atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
+        int pid = T.ids[q];
+        atomicAdd(&P.ctl->p_rows, (unsigned long long)((P.off[pid + 1] - P.off[pid]) +
+                                                       (P.off2[pid + 1] - P.off2[pid])));
+    }
 
     Bounds b = {0, 0, 0};
     if (degree_prune(P, T, ws, M, m1, PRE, D, R, b)) {

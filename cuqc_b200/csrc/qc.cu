@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -69,8 +70,11 @@ extern "C" const char* qc_last_error(void) { return g_err.c_str(); }
 // objects
 // ------------------------------------------------------------------
 
+static std::atomic<unsigned long long> g_graph_serial{1};
+
 struct qc_graph {
     HostGraph h;
+    unsigned long long serial = g_graph_serial.fetch_add(1); // identity for device caches
 };
 
 struct qc_result {
@@ -114,6 +118,7 @@ struct qc_context {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws;
     int32_t pos_n = 0;
+    unsigned long long resident = 0; // serial of the graph whose CSR is on the device
     int64_t arena_bytes = 0, stack_slots = 0, result_ints = 0;
     int64_t launches = 0;
 };
@@ -279,18 +284,12 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     cudaStream_t s = c->stream;
     CK(cudaSetDevice(c->cfg.device));
 
-    // graph -> device (timed as load)
+    // graph -> device (timed as load; skipped when already resident)
     auto t_load = clk::now();
-    CK(upload(c->off, h.off, s));
-    CK(upload(c->adj, h.adj, s));
-    CK(upload(c->off2, h.off2, s));
-    CK(upload(c->adj2, h.adj2, s));
-    if (c->pos_n < h.n || !c->pos.p) {
-        CK(c->pos.ensure(sizeof(int32_t) * (size_t)std::max(h.n, 1)));
-        CK(cudaMemsetAsync(c->pos.p, 0xff, sizeof(int32_t) * (size_t)std::max(h.n, 1), s));
-        c->pos_n = h.n;
+    if (c->resident != g->serial) {
+        qc_status us = qc_context_upload(c, g);
+        if (us != QC_OK) return us;
     }
-    CK(cudaStreamSynchronize(s));
     r->st.load_ms = ms_since(t_load);
 
     // enumeration: level 0 + device expansion
@@ -374,6 +373,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaMemcpyAsync(c->slot.p, &one, sizeof(one), cudaMemcpyHostToDevice, s));
 
         ExpandParams P{};
+        P.off = c->off.as<int64_t>();
+        P.off2 = c->off2.as<int64_t>();
         P.md = c->md.as<int32_t>();
         P.ubt = c->ubt.as<int32_t>();
         P.mdlen = (int32_t)md.size();
@@ -423,6 +424,10 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         r->st.emitted = (int64_t)ctl.emitted;
         r->st.emitted_ints = (int64_t)ctl.result_top;
         r->st.max_task = ctl.max_task;
+        r->st.parent_vertices = (int64_t)ctl.parent_vertices;
+        r->st.p_rows = (int64_t)ctl.p_rows;
+        r->st.child_vertices = (int64_t)ctl.child_vertices;
+        r->st.kernel_ms = kms;
         r->st.arena_peak = (int64_t)ctl.arena_top;
         r->st.kernel_launches = c->launches;
         flat.resize((size_t)ctl.result_top);
@@ -431,7 +436,6 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
                                cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         r->st.enum_ms = ms_since(t_enum);
-        (void)kms;
         break;
     }
 
@@ -446,6 +450,29 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     r->st.total_ms = ms_since(t_all);
     return QC_OK;
 }
+
+extern "C" qc_status qc_context_upload(qc_context* c, const qc_graph* g)
+{
+    if (!c || !g) return fail(QC_ERR_ARGS, "NULL argument");
+    const HostGraph& h = g->h;
+    cudaStream_t s = c->stream;
+    CK(cudaSetDevice(c->cfg.device));
+    c->resident = 0;
+    CK(upload(c->off, h.off, s));
+    CK(upload(c->adj, h.adj, s));
+    CK(upload(c->off2, h.off2, s));
+    CK(upload(c->adj2, h.adj2, s));
+    if (c->pos_n < h.n || !c->pos.p) {
+        CK(c->pos.ensure(sizeof(int32_t) * (size_t)std::max(h.n, 1)));
+        CK(cudaMemsetAsync(c->pos.p, 0xff, sizeof(int32_t) * (size_t)std::max(h.n, 1), s));
+        c->pos_n = h.n;
+    }
+    CK(cudaStreamSynchronize(s));
+    c->resident = g->serial;
+    return QC_OK;
+}
+
+extern "C" void* qc_context_stream(qc_context* c) { return c ? (void*)c->stream : nullptr; }
 
 extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
                              int32_t sched, qc_result** out)

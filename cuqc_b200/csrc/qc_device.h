@@ -38,6 +38,7 @@ struct Control {
     int status;
     unsigned long long tasks, branches, children, emitted, emitted_ints;
     unsigned long long lookahead_hits;
+    unsigned long long parent_vertices, p_rows, child_vertices;
     int max_task;
     int active_warps;              // warps still inside the work loop
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
@@ -75,6 +76,8 @@ __host__ __device__ inline uint64_t rec_bytes(int t, int W) {
 }
 
 struct ExpandParams {
+    const int64_t* off;  // 1-hop offsets (degrees for the work counters)
+    const int64_t* off2; // 2-hop offsets
     const int32_t* md;   // md[0 .. mdlen)
     const int32_t* ubt;  // floor(d / gamma), d in [0 .. mdlen)
     int32_t mdlen;

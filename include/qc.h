@@ -101,6 +101,15 @@ typedef struct qc_context qc_context;
 qc_status qc_context_create(const qc_config* cfg, qc_context** out);
 void qc_context_free(qc_context* ctx);
 
+/* Copy a graph to the context's device now; later qc_mine calls on the same
+ * graph skip the copy.  The reference copies its CSR inside allocate_memory
+ * (main.cu:700-711). */
+qc_status qc_context_upload(qc_context* ctx, const qc_graph* g);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or
+ * order their own work against the library's launches. */
+void* qc_context_stream(qc_context* ctx);
+
 /* ------------------------------------------------------------------ */
 /* mining                                                               */
 /* ------------------------------------------------------------------ */
@@ -120,6 +129,13 @@ typedef struct {
     int64_t max_task;      /* largest task                                     */
     int64_t arena_peak;    /* bytes of task records written                    */
     int64_t kernel_launches;
+    double kernel_ms;      /* expansion kernel alone (CUDA events)            */
+    /* work counters for the algorithmic-byte model (per expanded branch:
+     * the parent's vertex records, the added vertex's 1-hop and 2-hop rows,
+     * the child's records, the emitted sets) */
+    int64_t parent_vertices; /* sum over branches of the parent task size    */
+    int64_t p_rows;          /* sum over branches of deg(p) + |N2(p)|        */
+    int64_t child_vertices;  /* sum of child task sizes written              */
 } qc_stats;
 
 typedef struct qc_result qc_result;

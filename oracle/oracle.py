@@ -34,7 +34,8 @@ _MODES = {"host": MODE_HOST, "binary": MODE_BINARY, "clean": MODE_CLEAN}
 class Stats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "tasks", "lookahead_hits", "branches", "children", "emitted", "emitted_vertices",
-        "parent_vertices", "p_rows", "child_vertices", "max_task", "root_size")]
+        "parent_vertices", "p_rows", "child_vertices", "max_task", "root_size",
+        "stale_uses", "stale_oob")]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

@@ -69,6 +69,8 @@ typedef struct {
     int64_t child_vertices;   /* sum of written child sizes                */
     int64_t max_task;         /* largest task processed                    */
     int64_t root_size;        /* vertices in the root task                 */
+    int64_t stale_uses;       /* host rules: map lookups that hit a stale entry */
+    int64_t stale_oob;        /*   ... pointing outside the current vertex array */
 } qo_stats;
 
 typedef struct {
@@ -156,6 +158,19 @@ static void map_clear(qo_ctx* c, const qo_vtx* v, int lo, int hi)
     } else {
         for (int64_t i = 0; i < c->dirty.n; i++) c->pos[c->dirty.v[i]] = -1;
         c->dirty.n = 0;
+    }
+}
+
+/* diagnostic for host rules: a lookup of id `x` returned position p that
+ * does not hold x in the current array v[0..n) */
+static inline void note_lookup(qo_ctx* c, const qo_vtx* v, int n, int x, int p)
+{
+    if (p < 0) return;
+    if (p >= n) {
+        c->st.stale_uses++;
+        c->st.stale_oob++;
+    } else if (v[p].id != x) {
+        c->st.stale_uses++;
     }
 }
 
@@ -462,6 +477,7 @@ static int lookahead(qo_ctx* c, qo_vtx* v, int t, int m, int nc)
         int u = v[i].id;
         for (int64_t e = c->off2[u]; e < c->off2[u + 1]; e++) {
             int p = c->pos[c->adj2[e]];
+            note_lookup(c, v, t, c->adj2[e], p);
             /* a stale host-map position can point past this task; the
              * reference's write then lands outside the task's records */
             if (p >= m && p < t) v[p].l2++;
@@ -488,6 +504,7 @@ static int remove_one(qo_ctx* c, qo_vtx* v, int* tot, int* nc, int m)
     int u = v[*tot].id;
     for (int64_t e = c->off[u]; e < c->off[u + 1]; e++) {
         int p = c->pos[c->adj[e]];
+        note_lookup(c, v, *tot, c->adj[e], p);
         if (p > -1 && p < *tot) {
             v[p].exdeg--;
             if (p < m && v[p].indeg + v[p].exdeg < need) {
@@ -510,6 +527,7 @@ static void diameter(qo_ctx* c, qo_vtx* w, int p, int tot, int m)
     for (int i = m; i < tot; i++) w[i].label = -1;
     for (int64_t e = c->off2[p]; e < c->off2[p + 1]; e++) {
         int q = c->pos[c->adj2[e]];
+        note_lookup(c, w, tot, c->adj2[e], q);
         if (q >= m && q < tot) {
             w[q].label = 0;
             c->cind[c->nrem++] = w[q].indeg;
@@ -530,6 +548,7 @@ static int add_one(qo_ctx* c, qo_vtx* w, int* tot, int* nc, int* m, qo_bounds* b
     map_set(c, w, 0, *tot);
     for (int64_t e = c->off[p]; e < c->off[p + 1]; e++) {
         int q = c->pos[c->adj[e]];
+        note_lookup(c, w, *tot, c->adj[e], q);
         if (q > -1 && q < *tot) {
             w[q].indeg++;
             w[q].exdeg--;

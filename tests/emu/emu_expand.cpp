@@ -77,6 +77,8 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     std::vector<char> ws((size_t)(L.total * warps));
 
     ExpandParams P{};
+    P.off = off;
+    P.off2 = off2;
     P.md = md.data();
     P.ubt = ubt.data();
     P.mdlen = (int32_t)md.size();

@@ -46,6 +46,26 @@ def test_device_rules_match_reference_binary(case):
     if os.path.exists(refbin):
         with open(refbin) as f:
             assert oracle.result_text(clean) == f.read()
+        # the binary's temp.txt: every set it emitted, maximal or not
+        tok = open(os.path.join(GOLDEN, case["name"] + ".refbin.temp")).read().split()
+        ref_em, p = [], 0
+        while p < len(tok):
+            k = int(tok[p])
+            ref_em.append(tuple(sorted(int(x) for x in tok[p + 1:p + 1 + k])))
+            p += 1 + k
+        flat, _ = oracle.mine(g, float(gamma), ms, "binary")
+        assert sorted(ref_em) == sorted(tuple(sorted(s)) for s in oracle.unpack(flat))
+    else:
+        assert case["refbin"] != "ok"
+
+
+def test_reference_binary_outputs_present():
+    ok = [c["name"] for c in CASES if c["refbin"] == "ok"]
+    assert len(ok) >= 14
+    faulted = [c["name"] for c in CASES if c["refbin"].startswith("failed")]
+    # the reference binary faulted on these (illegal memory access); see
+    # tests/golden/refbin_logs
+    assert set(faulted) == {"small01", "small10", "er1000_planted"}
 
 
 def test_reference_cpu_path_can_emit_a_non_quasi_clique():
