@@ -1,0 +1,343 @@
+"""Benchmark: maximal gamma-quasi-clique enumeration on the B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg1|cfg2|...]
+
+A step is one full mining pass over one instance: level 0, the persistent
+expansion kernel and the device non-maximal removal (everything qc_mine does
+once the graph is resident in HBM).  `value` is instances/s over the K timed
+steps, device-timed with CUDA events on the library's own stream; L2 is
+flushed (a 256 MiB write) before every step and the flush is not timed.
+`e2e` is the same metric through the public C ABI from host arrays: graph
+construction from host CSR, host->device copy, mining, and the device->host
+read of the result, all inside the timed region.
+
+Under torchrun (N > 1) every rank mines its own replica of the instance on its
+own GPU (instances are independent: weak scaling, no data-path collective);
+the elapsed time is the max over ranks.
+
+--impl reference times the reference's own CPU implementation of the path (its
+host routines, compiled from the reference sources into
+oracle/_ref/libqc_refcpu.so) on the host cores, one instance per core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cuqc_b200 import graphs  # noqa: E402
+
+WORKLOADS = {
+    # Erdos-Renyi G(1000, 0.02) + 5 disjoint planted groups of 30 at 0.95
+    "cfg1": dict(desc="ER G(n=1000,p=0.02) + 5 planted groups of 30 @0.95, gamma=0.9, min_size=20",
+                 gen="erdos_renyi_planted",
+                 kw=dict(n=1000, p=0.02, groups=5, group_size=30, density=0.95, seed=1),
+                 gamma="0.9", min_size=20),
+    # Chung-Lu n=8000, exponent 2.1, mean degree 40 + 200 planted groups
+    "cfg2": dict(desc="Chung-Lu n=8000 beta=2.1 mean deg 40 + 200 planted groups 15-60 @0.85-1.0, "
+                      "gamma=0.8, min_size=15",
+                 gen="chung_lu_planted",
+                 kw=dict(n=8000, beta=2.1, mean_degree=40, n_groups=200, size_range=(15, 60),
+                         density_range=(0.85, 1.0), seed=2),
+                 gamma="0.8", min_size=15),
+}
+DEFAULT_WORKLOAD = "cfg1"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_graph(w):
+    spec = WORKLOADS[w]
+    return getattr(graphs, spec["gen"])(**spec["kw"]), spec
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU path
+# ---------------------------------------------------------------------------
+
+def _refcpu_one(args):
+    path, gamma, ms = args
+    from oracle import oracle
+    d = tempfile.mkdtemp(prefix="refcpu_")
+    t = {}
+    import io
+    import contextlib
+    with contextlib.redirect_stdout(io.StringIO()):
+        text, _ = oracle.refcpu_run(path, gamma, ms, workdir=d, times=t)
+    return t["enum_ms"] + t["rm_ms"], text.count("\n")
+
+
+def cpu_reference_rate(path, spec, procs, instances):
+    """instances/s of the reference CPU path: `instances` runs on `procs`
+    processes (spawned); each run's time excludes file parsing."""
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_refcpu_one, [(path, spec["gamma"], spec["min_size"])] * instances)
+    wall = time.perf_counter() - t0
+    per = [r[0] for r in res]
+    # throughput from the per-run enumeration+removal times, `procs` at a time
+    busy_s = sum(per) / 1000.0 / procs
+    return instances / busy_s, per, wall, res[0][1]
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = args.workload
+    g, spec = make_graph(w)
+    d = tempfile.mkdtemp()
+    path = os.path.join(d, "g.txt")
+    graphs.write_serialized(g, path)
+    from oracle import oracle
+    if not oracle.refcpu_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libqc_refcpu.so absent"}))
+        return
+    procs = max(1, os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        cpu_reference_rate(path, spec, procs, procs)
+    rates, step_ms = [], []
+    for _ in range(args.steps):
+        r, per, wall, nmax = cpu_reference_rate(path, spec, procs, procs)
+        rates.append(r)
+        step_ms.append(statistics.mean(per))
+    value = statistics.mean(rates)
+    line = {
+        "impl": "reference", "metric": "instances/s (maximal gamma-quasi-clique enumeration)",
+        "value": value, "unit": "instances/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": w, "desc": spec["desc"], "parallelism": "one instance per core"},
+        "cpu_baseline": {"value": value, "unit": "instances/s", "cores": procs,
+                         "kind": "reference",
+                         "sample": "%d full instances per step, one per core; time = the "
+                                   "reference's enumeration + RemoveNonMax (file parse excluded)"
+                                   % procs},
+        "e2e": {"value": value, "unit": "instances/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "maximal": nmax,
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+
+    import cuqc_b200 as Q
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    w = args.workload
+    g, spec = make_graph(w)
+    gamma, ms = float(spec["gamma"]), spec["min_size"]
+    ctx = Q.Context(device=local)
+    dg = ctx.upload(g)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        res = ctx.mine(dg, gamma, ms)
+    ref_sets = res.sets
+    stats = []
+    barrier()
+    launches0 = res.stats["kernel_launches"]
+    with ClockSampler(local) as clocks:
+        elapsed = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            res = ctx.mine(dg, gamma, ms)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            elapsed += e0.elapsed_time(e1)
+            stats.append(res.stats)
+            assert res.sets == ref_sets
+        barrier()
+    launches = res.stats["kernel_launches"] - launches0
+    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_max = float(t.item())
+    value = world * args.steps / (elapsed_max / 1000.0)
+
+    # e2e: from host CSR arrays through the C ABI, result read back
+    barrier()
+    e2e_t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dg2 = Q.DeviceGraph.from_graph(g)
+        r2 = ctx.mine(dg2, gamma, ms)
+        dg2.close()
+        assert r2.sets == ref_sets
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - e2e_t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / float(te.item())
+    h2d = 8 * (g.n + 1) * 2 + 4 * g.m + 4 * g.m2
+    d2h = 4 * sum(1 + len(s) for s in ref_sets)
+
+    if rank == 0:
+        st = stats[-1]
+        kernel_ms = statistics.mean(s["kernel_ms"] for s in stats)
+        # algorithmic bytes per launch: per expanded branch 16 B per parent vertex
+        # record + 4 B per entry of the added vertex's 1-hop and 2-hop rows
+        # + 16 B per child vertex record + 4 B per emitted int
+        b_alg = 16 * st["parent_vertices"] + 4 * st["p_rows"] + 16 * st["child_vertices"] + \
+            4 * st["emitted_ints"]
+        peak, peak_kind = load_peaks()
+        achieved = b_alg / (kernel_ms / 1000.0) / 1e9
+        line = {
+            "metric": "instances/s (maximal gamma-quasi-clique enumeration)",
+            "value": value, "unit": "instances/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator: %s)" % spec["desc"],
+            "config": {"workload": w, "n": g.n, "gamma": spec["gamma"], "min_size": ms,
+                       "l2": "flushed before every step (256 MiB write, untimed)",
+                       "parallelism": "replicas (one instance per GPU per step)"},
+            "enum_ms": statistics.mean(s["enum_ms"] for s in stats),
+            "kernel_ms": kernel_ms,
+            "filter_ms": statistics.mean(s["filter_ms"] for s in stats),
+            "tasks": st["tasks"], "branches": st["branches"],
+            "tasks_per_s": st["tasks"] / (elapsed_max / args.steps / 1000.0),
+            "maximal": len(ref_sets),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "expand_kernel", "peak_source": peak_kind,
+                         "alg_bytes_per_launch": b_alg},
+            "e2e": {"value": e2e_value, "unit": "instances/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        if args.cpu_baseline and world == 1:
+            from oracle import oracle
+            if oracle.refcpu_available():
+                d = tempfile.mkdtemp()
+                path = os.path.join(d, "g.txt")
+                graphs.write_serialized(g, path)
+                procs = 1
+                rate, per, wall, nmax = cpu_reference_rate(path, spec, procs, args.cpu_instances)
+                line["cpu_baseline"] = {
+                    "value": rate, "unit": "instances/s", "cores": procs, "kind": "reference",
+                    "sample": "%d full instance(s) on 1 core; the reference's own CPU path "
+                              "(enumeration + RemoveNonMax, file parse excluded)"
+                              % args.cpu_instances}
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-instances", type=int, default=8)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -496,11 +496,12 @@ __device__ void emit_mask(const ExpandParams& P, const TaskView& T, const uint32
     unsigned long long at = 0;
     if (lane == 0) {
         at = atomicAdd(&P.ctl->result_top, (unsigned long long)(k + 1));
-        if (at + k + 1 > P.ctl->result_cap) {
+        unsigned long long idx = atomicAdd(&P.ctl->emitted, 1ull);
+        if (at + k + 1 > P.ctl->result_cap || idx >= P.ctl->set_cap) {
             set_status(P, ST_RESULT_OVERFLOW);
             at = ~0ull;
         } else {
-            atomicAdd(&P.ctl->emitted, 1ull);
+            P.set_starts[idx] = at;
             atomicAdd(&P.ctl->emitted_ints, (unsigned long long)(k + 1));
         }
     }
@@ -582,13 +583,25 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
 {
     unsigned long long t0 = now_ns();
     unsigned spins = 0;
+    unsigned backoff = 64;
     int last_pending = -1;
     for (;;) {
         if (*(volatile int*)&P.ctl->status) return -1;
+        if (P.deadline_ns && now_ns() > P.deadline_ns) {
+            set_status(P, ST_DEADLINE);
+            return -1;
+        }
         int top = *(volatile int*)&P.ctl->stack_top;
         if (top > 0) {
+            backoff = 64;
             if (atomicCAS(&P.ctl->stack_top, top, top - 1) == top) {
                 int idx = top - 1;
+                // a failed push (stack full) leaves stack_top above the
+                // capacity; such an index has no slot behind it
+                if (idx >= P.ctl->stack_cap) {
+                    set_status(P, ST_TASK_OVERFLOW);
+                    return -1;
+                }
                 unsigned long long t1 = now_ns();
                 unsigned s2 = 0;
                 while (atomicCAS(&P.slot[idx], 1, 3) != 1) {
@@ -616,12 +629,15 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
             last_pending = pend;
             t0 = now_ns();
         }
-        if ((++spins & 63u) == 0 && now_ns() - t0 > (unsigned long long)P.wait_ns) {
+        if ((++spins & 15u) == 0 && now_ns() - t0 > (unsigned long long)P.wait_ns) {
             set_status(P, ST_ITER_LIMIT);
             P.ctl->wait_fail_where = 3;
             return -1;
         }
-        __nanosleep(256);
+        // idle: back off (64 ns doubling to ~4 us) so waiting warps leave the
+        // issue slots and the stack's cache line to the working ones
+        __nanosleep(backoff);
+        backoff = backoff < 4096 ? backoff * 2 : 4096;
     }
 }
 
@@ -886,6 +902,374 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
 }
 
 // ------------------------------------------------------------------
+// register-resident path for tasks of at most 32 vertices (the bulk of the
+// search tree): lane v holds vertex v's id, 1-hop row and 2-hop row; every
+// vertex set is one 32-bit word, identical in all lanes.
+// ------------------------------------------------------------------
+
+__device__ __forceinline__ int rmin(int x)
+{
+#ifdef QC_EMULATION
+    return wmin(x);
+#else
+    return __reduce_min_sync(QC_FULL, x);
+#endif
+}
+__device__ __forceinline__ int rmax(int x)
+{
+#ifdef QC_EMULATION
+    return wmax(x);
+#else
+    return __reduce_max_sync(QC_FULL, x);
+#endif
+}
+__device__ __forceinline__ int radd(int x)
+{
+#ifdef QC_EMULATION
+    return wsum(x);
+#else
+    return __reduce_add_sync(QC_FULL, x);
+#endif
+}
+__device__ __forceinline__ unsigned ror(unsigned x)
+{
+#ifdef QC_EMULATION
+    for (int o = 16; o; o >>= 1) x |= __shfl_xor_sync(QC_FULL, x, o);
+    return x;
+#else
+    return __reduce_or_sync(QC_FULL, x);
+#endif
+}
+
+__device__ __forceinline__ bool in_set(unsigned s, int lane) { return (s >> lane) & 1u; }
+__device__ __forceinline__ unsigned low_mask(int k) { return k >= 32 ? ~0u : ((1u << k) - 1u); }
+
+struct SmallTask {
+    int t, m, cov, id, l2;
+    unsigned a1, a2;
+};
+
+// values sorted descending across lanes; returns S = sum of this lane's value
+// and all larger-ranked ones (inclusive), so S(k) = shfl(S, k-1)
+__device__ __forceinline__ int sort_desc_prefix(int v)
+{
+    int lane = lane_id();
+    // bitonic sort ascending on -v
+    int x = -v;
+    for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            int y = __shfl_xor_sync(QC_FULL, x, j);
+            bool up = (lane & k) == 0;
+            bool lower = (lane & j) == 0;
+            int mn = x < y ? x : y, mx = x < y ? y : x;
+            x = (lower == up) ? mn : mx;
+        }
+    int val = -x; // descending values, padding lanes hold -INT_MAX.. -> guarded below
+    int s = val > 0 ? val : 0;
+    return wscan(s);
+}
+
+// LU bounds (main.cu:1857-1972) for members set M (m of them) and the
+// candidate indegree multiset given by lanes in `cs` with value `in`.
+__device__ bool lu_small(const ExpandParams& P, unsigned M, int m, unsigned cs, int in, int ex,
+                         Bounds& b)
+{
+    int lane = lane_id();
+    bool mem = in_set(M, lane);
+    int min_in = rmin(mem ? in : 0x7fffffff);
+    int min_tot = rmin(mem ? in + ex : 0x7fffffff);
+    int sum_in = radd(mem ? in : 0);
+    int min_in_ex = rmin(mem && in == min_in ? ex : 0x7fffffff);
+    int ncand = __popc(cs);
+    bool invalid = false;
+    b.med = mindeg(P, m + 1);
+    if (min_in < md_at(P, m)) {
+        int lb = mindeg(P, m) - min_in;
+        for (int base = lb;; base += 32) {
+            int L = base + lane;
+            bool cont = (L <= min_in_ex) && (min_in + L < md_at(P, m + L));
+            unsigned stop = __ballot_sync(QC_FULL, !cont);
+            if (stop) {
+                lb = base + __ffs(stop) - 1;
+                break;
+            }
+        }
+        if (min_in + lb < md_at(P, m + lb)) {
+            lb = ncand + 1;
+            invalid = true;
+        }
+        int ub = ubt_at(P, min_tot) + 1 - m;
+        if (ub > ncand) ub = ncand;
+        if (lb < ub) {
+            // S(k) for k = lane: sum of the k largest candidate indegrees
+            int incl = sort_desc_prefix(in_set(cs, lane) ? in : -1);
+            int excl = __shfl_up_sync(QC_FULL, incl, 1);
+            if (lane == 0) excl = 0;
+            int s_at_32 = __shfl_sync(QC_FULL, incl, 31);
+            // g(k) for k in [lb, ub] (ub <= 31): k == ub or sum_in + S(k) >= m*md[m+k]
+            int k = lane;
+            long long Sk = excl;
+            bool g = (k >= lb && k <= ub) &&
+                     (k == ub || (long long)sum_in + Sk >= (long long)m * md_at(P, m + k));
+            unsigned bal = __ballot_sync(QC_FULL, g);
+            int idx = bal ? __ffs(bal) - 1 : ub;
+            long long Sidx = idx < 32 ? __shfl_sync(QC_FULL, excl, idx & 31) : s_at_32;
+            if ((long long)sum_in + Sidx < (long long)m * md_at(P, m + idx)) {
+                lb = ub + 1;
+                invalid = true;
+            } else {
+                lb = idx;
+                bool g2 = (k > idx && k <= ub) &&
+                          ((long long)sum_in + Sk >= (long long)m * md_at(P, m + k));
+                unsigned b2 = __ballot_sync(QC_FULL, g2);
+                int tub = b2 ? 31 - __clz(b2) : idx;
+                if (ub > tub) ub = tub;
+                if (lb > 1) b.med = mindeg(P, m + lb);
+            }
+        }
+        b.U = ub;
+        b.L = lb;
+    } else {
+        b.U = ncand;
+        b.L = m < P.min_size ? P.min_size - m : 0;
+    }
+    if (m + b.U < P.min_size) invalid = true;
+    if (b.U < 0 || b.U < b.L) invalid = true;
+    return invalid;
+}
+
+// degree pruning fixpoint (main.cu:1735-1855) on words; `ex` is updated in place
+__device__ bool prune_small(const ExpandParams& P, unsigned a1, unsigned M, int m, unsigned Call,
+                            unsigned D, unsigned& R, int in, int& ex, Bounds& b)
+{
+    int lane = lane_id();
+    if (lu_small(P, M, m, D, in, ex, b)) return true;
+    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(P, in, ex, m, b))) return true;
+    R = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid(P, in, ex, m, b));
+    unsigned X = Call & ~R;
+    while (R && X) {
+        ex = __popc(a1 & R);
+        unsigned V = __ballot_sync(QC_FULL, in_set(R, lane) && cand_valid(P, in, ex, m, b));
+        if (lu_small(P, M, m, V, in, ex, b)) return true;
+        if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(P, in, ex, m, b))) return true;
+        unsigned R2 = __ballot_sync(QC_FULL, in_set(R, lane) && cand_valid(P, in, ex, m, b));
+        X = R & ~R2;
+        R = R2;
+    }
+    return false;
+}
+
+__device__ void emit_small(const ExpandParams& P, unsigned S, int id)
+{
+    int lane = lane_id();
+    int k = __popc(S);
+    unsigned long long at = 0;
+    if (lane == 0) {
+        at = atomicAdd(&P.ctl->result_top, (unsigned long long)(k + 1));
+        unsigned long long idx = atomicAdd(&P.ctl->emitted, 1ull);
+        if (at + k + 1 > P.ctl->result_cap || idx >= P.ctl->set_cap) {
+            set_status(P, ST_RESULT_OVERFLOW);
+            at = ~0ull;
+        } else {
+            P.set_starts[idx] = at;
+            atomicAdd(&P.ctl->emitted_ints, (unsigned long long)(k + 1));
+            P.results[at] = k;
+        }
+    }
+    at = __shfl_sync(QC_FULL, at, 0);
+    if (at == ~0ull) return;
+    if (in_set(S, lane)) P.results[at + 1 + __popc(S & low_mask(lane))] = id;
+}
+
+__device__ __forceinline__ void clique_small(const ExpandParams& P, unsigned M, int m, int in, int id)
+{
+    int lane = lane_id();
+    int need = md_at(P, m);
+    if (!__any_sync(QC_FULL, in_set(M, lane) && in < need)) emit_small(P, M, id);
+}
+
+// child record of the vertices in M2 | R2, Q-sorted, matrices compacted
+__device__ void child_small(const ExpandParams& P, const SmallTask& T, unsigned M2, int m2,
+                            unsigned R2, int in, int ex)
+{
+    int lane = lane_id();
+    unsigned S = M2 | R2;
+    int tc = __popc(S);
+    unsigned long long hi = ~0ull, lo = ~0ull;
+    if (in_set(S, lane)) {
+        unsigned long long cls = in_set(M2, lane) ? 0ull : 1ull;
+        hi = (cls << 48) | ((0xffffull - (unsigned long long)in) << 32) |
+             ((0xffffull - (unsigned long long)ex) << 16) | (0xffffull - (unsigned long long)T.l2);
+        lo = ((0xffffffffull - (unsigned long long)(unsigned)T.id) << 5) | (unsigned long long)lane;
+    }
+    // bitonic sort ascending on (hi, lo); lo carries the source lane
+    for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            unsigned long long oh = __shfl_xor_sync(QC_FULL, hi, j);
+            unsigned long long ol = __shfl_xor_sync(QC_FULL, lo, j);
+            bool up = (lane & k) == 0;
+            bool lower = (lane & j) == 0;
+            bool mine_less = hi < oh || (hi == oh && lo < ol);
+            bool take_min = (lower == up);
+            if (take_min != mine_less) {
+                hi = oh;
+                lo = ol;
+            }
+        }
+    int src = (int)(lo & 31ull);
+    unsigned sa1 = __shfl_sync(QC_FULL, T.a1, src);
+    unsigned sa2 = __shfl_sync(QC_FULL, T.a2, src);
+    int sid = __shfl_sync(QC_FULL, T.id, src);
+    unsigned c1 = 0, c2 = 0;
+    for (int j = 0; j < tc; j++) {
+        int pj = __shfl_sync(QC_FULL, src, j);
+        c1 |= ((sa1 >> pj) & 1u) << j;
+        c2 |= ((sa2 >> pj) & 1u) << j;
+    }
+    unsigned long long bytes = rec_bytes(tc, 1);
+    unsigned long long at = 0;
+    if (lane == 0) {
+        at = atomicAdd(&P.ctl->arena_top, bytes);
+        if (at + bytes > P.ctl->arena_cap) {
+            set_status(P, ST_TASK_OVERFLOW);
+            at = ~0ull;
+        }
+    }
+    at = __shfl_sync(QC_FULL, at, 0);
+    if (at == ~0ull) return;
+    char* rec = P.arena + at;
+    if (lane == 0) {
+        TaskHdr* h = (TaskHdr*)rec;
+        h->t = tc;
+        h->m = m2;
+        h->cov = 0;
+        h->W = 1;
+    }
+    if (lane < tc) {
+        ((int32_t*)(rec + rec_ids_off()))[lane] = sid;
+        ((int32_t*)(rec + rec_l2_off(tc)))[lane] = 0;
+        ((uint32_t*)(rec + rec_a1_off(tc)))[lane] = c1;
+        ((uint32_t*)(rec + rec_a2_off(tc, 1)))[lane] = c2;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        atomicAdd(&P.ctl->children, 1ull);
+        atomicAdd(&P.ctl->child_vertices, (unsigned long long)tc);
+        __threadfence();
+        WorkItem it;
+        it.rec = at;
+        it.q_lo = -1;
+        it.q_hi = -1;
+        push_item(P, it);
+    }
+    __syncwarp();
+}
+
+__device__ void branch_small(const ExpandParams& P, const SmallTask& T, int q)
+{
+    int lane = lane_id();
+    unsigned Mm = low_mask(T.m);
+    unsigned M1 = Mm | (1u << q);
+    int m1 = T.m + 1;
+    unsigned PRE = low_mask(q) & ~Mm;
+    int in = __popc(T.a1 & M1);
+    int ex = __popc(T.a1 & PRE);
+    unsigned r2q = __shfl_sync(QC_FULL, T.a2, q);
+    unsigned D = PRE & r2q;
+    if (lane == 0) {
+        atomicAdd(&P.ctl->branches, 1ull);
+        atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
+    }
+    if (lane == q) {
+        atomicAdd(&P.ctl->p_rows, (unsigned long long)((P.off[T.id + 1] - P.off[T.id]) +
+                                                       (P.off2[T.id + 1] - P.off2[T.id])));
+    }
+    Bounds b = {0, 0, 0};
+    unsigned R = 0;
+    if (prune_small(P, T.a1, M1, m1, PRE, D, R, in, ex, b)) {
+        if (m1 >= P.min_size) clique_small(P, M1, m1, in, T.id);
+        return;
+    }
+    // critical vertices (main.cu:1526-1707)
+    int critv = md_at(P, m1 + b.L);
+    unsigned K = __ballot_sync(QC_FULL, in_set(M1, lane) && in + ex == critv && ex > 0);
+    unsigned CA = R & ror(in_set(K, lane) ? T.a1 : 0u);
+    int nca = __popc(CA);
+    unsigned M2 = M1, C2 = R, D2 = R;
+    int m2 = m1;
+    if (nca > 0) {
+        int d = __popc(T.a1 & CA);
+        in += d;
+        ex -= d;
+        int adj = __popc(T.a2 & CA);
+        bool bad = (in_set(M1, lane) && adj != nca) || (in_set(CA, lane) && adj < nca - 1);
+        if (__any_sync(QC_FULL, bad)) return;
+        M2 = M1 | CA;
+        m2 = m1 + nca;
+        C2 = R & ~CA;
+        D2 = __ballot_sync(QC_FULL, in_set(C2, lane) && adj == nca);
+    }
+    Bounds b2 = {0, 0, 0};
+    unsigned R2 = 0;
+    bool fail2 = prune_small(P, T.a1, M2, m2, C2, D2, R2, in, ex, b2);
+    if (m2 >= P.min_size) clique_small(P, M2, m2, in, T.id);
+    if (fail2) return;
+    if (R2) child_small(P, T, M2, m2, R2, in, ex);
+}
+
+// a fresh task of at most 32 vertices, processed whole by one warp
+__device__ void process_small(const ExpandParams& P, const TaskView& V)
+{
+    int lane = lane_id();
+    SmallTask T;
+    T.t = V.t;
+    T.m = V.m;
+    T.cov = V.cov;
+    bool act = lane < T.t;
+    T.id = act ? V.ids[lane] : -1;
+    T.a1 = act ? V.A1[lane] : 0u;
+    T.a2 = act ? V.A2[lane] : 0u;
+    T.l2 = act ? V.l2[lane] : 0;
+    const int t = T.t, m = T.m;
+    unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
+    int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
+    if (lane == 0) {
+        atomicAdd(&P.ctl->tasks, 1ull);
+        atomicMax(&P.ctl->max_task, t);
+    }
+    // lookahead (main.cu:1349-1405)
+    int need_t = md_at(P, t);
+    if (!__any_sync(QC_FULL, in_set(Mm, lane) && in + ex < need_t)) {
+        int nc = t - m;
+        if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
+        bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
+        if (!__any_sync(QC_FULL, bad)) {
+            if (lane == 0) atomicAdd(&P.ctl->lookahead_hits, 1ull);
+            emit_small(P, low_mask(t), T.id);
+            return;
+        }
+    }
+    // branches run until a member would fail on removal (main.cu:1092-1099)
+    int need = mindeg(P, m);
+    int pos = 0;
+    if (in_set(Mm, lane)) {
+        int k = need - in;
+        if (k > 0) {
+            unsigned x = T.a1 & Cm;
+            for (int s = 1; s < k; s++) x &= x - 1;
+            pos = x ? __ffs(x) - 1 : t - 1;
+        }
+    }
+    int qlo = rmax(pos);
+    qlo = qlo > m + T.cov ? qlo : m + T.cov;
+    if (qlo > t - 1) return;
+    for (int q = t - 1; q >= qlo; q--) {
+        if (*(volatile int*)&P.ctl->status) return;
+        branch_small(P, T, q);
+    }
+}
+
+// ------------------------------------------------------------------
 // a work item: fresh task (lookahead, branch range) or a branch range
 // ------------------------------------------------------------------
 
@@ -899,6 +1283,10 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
         return;
     }
     int q_lo = it.q_lo, q_hi = it.q_hi;
+    if (q_lo < 0 && t <= 32 && P.small_path) {
+        process_small(P, T);
+        return;
+    }
     if (q_lo < 0) {
         if (lane == 0) {
             atomicAdd(&P.ctl->tasks, 1ull);

@@ -1,0 +1,375 @@
+// filter.cu -- non-maximal removal on the GPU (replaces the reference's host
+// prefix-tree pass RemoveNonMax, Mike12041204/cuQC main.cu:4571-4960).
+//
+// Input: the emitted sets in the device result buffer, [k, id_1..id_k] each,
+// and the start offset of every set (written by the expansion kernel).
+//   1. one warp per set: sort its ids ascending into the sorted buffer and
+//      hash the set (sum of per-id 64-bit mixes, plus its size);
+//   2. radix-sort (hash, set) and drop exact duplicates (equal hash and equal
+//      contents; a hash collision with different contents keeps both);
+//   3. inverted index over the distinct sets: a counting sort of
+//      (vertex, set) incidences gives every vertex its posting list;
+//   4. one warp per distinct set S: scan the posting list of S's rarest
+//      vertex and test S against every longer set T in it by a sorted merge;
+//      S is maximal iff no such T contains it;
+//   5. the maximal sets are compacted and copied back; the host orders them
+//      lexicographically (the order the reference's prefix tree writes).
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "filter.h"
+
+namespace qcb {
+
+namespace {
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x)
+{
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+// 1. per-set sort + hash (one warp per set)
+__global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* starts, int64_t nsets,
+                                 int32_t* sorted, unsigned long long* hash, int32_t* order,
+                                 int32_t* sizes)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = warp; s < nsets; s += nw) {
+        unsigned long long a = starts[s];
+        int k = res[a];
+        const int32_t* in = res + a + 1;
+        int32_t* out = sorted + a + 1;
+        unsigned long long h = 0;
+        for (int i = lane; i < k; i += 32) {
+            out[i] = in[i];
+            h += mix64((unsigned long long)(unsigned)in[i]);
+        }
+        for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+        __syncwarp();
+        // bitonic sort of out[0..k), all compare-exchanges ascending (mirror
+        // step, then half-cleaners), so virtual +inf padding at [k, N) never
+        // moves into the real range
+        int N = 1;
+        while (N < k) N <<= 1;
+        for (int sz = 2; sz <= N; sz <<= 1) {
+            for (int j = sz >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < N; i += 32) {
+                    int p = (j == (sz >> 1)) ? (i ^ (sz - 1)) : (i ^ j);
+                    if (p > i && p < k) {
+                        int x = out[i], y = out[p];
+                        if (x > y) {
+                            out[i] = y;
+                            out[p] = x;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (lane == 0) {
+            sorted[a] = k;
+            hash[s] = mix64(h ^ ((unsigned long long)k << 40));
+            order[s] = (int32_t)s;
+            sizes[s] = k;
+        }
+    }
+}
+
+__device__ bool same_set(const int32_t* srt, unsigned long long a, unsigned long long b)
+{
+    int k = srt[a];
+    if (srt[b] != k) return false;
+    for (int i = 1; i <= k; i++)
+        if (srt[a + i] != srt[b + i]) return false;
+    return true;
+}
+
+// 2. duplicates: in hash order, a set equal to an earlier one of its hash run is dropped
+__global__ void dedupe_kernel(const int32_t* srt, const unsigned long long* starts,
+                              const unsigned long long* hsorted, const int32_t* osorted,
+                              int64_t nsets, uint8_t* keep)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsets) return;
+    unsigned long long h = hsorted[i];
+    bool dup = false;
+    for (int64_t j = i - 1; j >= 0 && hsorted[j] == h; j--) {
+        if (same_set(srt, starts[osorted[i]], starts[osorted[j]])) {
+            dup = true;
+            break;
+        }
+    }
+    keep[osorted[i]] = dup ? 0 : 1;
+}
+
+// 3a. incidence counts per vertex over kept sets
+__global__ void count_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
+                             const uint8_t* keep, int32_t* cnt)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = warp; s < nsets; s += nw) {
+        if (!keep[s]) continue;
+        unsigned long long a = starts[s];
+        int k = srt[a];
+        for (int i = lane; i < k; i += 32) atomicAdd(&cnt[srt[a + 1 + i]], 1);
+    }
+}
+
+// 3b. scatter set ids into posting lists
+__global__ void scatter_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
+                               const uint8_t* keep, int64_t* cursor, int32_t* post)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = warp; s < nsets; s += nw) {
+        if (!keep[s]) continue;
+        unsigned long long a = starts[s];
+        int k = srt[a];
+        for (int i = lane; i < k; i += 32) {
+            unsigned long long at = atomicAdd((unsigned long long*)&cursor[srt[a + 1 + i]], 1ull);
+            post[at] = (int32_t)s;
+        }
+    }
+}
+
+// is sorted set S (at a) a subset of sorted set T (at b)?  |T| > |S|
+__device__ bool subset_of(const int32_t* srt, unsigned long long a, unsigned long long b)
+{
+    int ks = srt[a], kt = srt[b];
+    int i = 0, j = 0;
+    const int32_t* S = srt + a + 1;
+    const int32_t* T = srt + b + 1;
+    while (i < ks && j < kt) {
+        if (ks - i > kt - j) return false;
+        int x = S[i], y = T[j];
+        if (x == y) { i++; j++; }
+        else if (x > y) j++;
+        else return false;
+    }
+    return i == ks;
+}
+
+// 4. superset test, one warp per kept set
+__global__ void maximal_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
+                               const uint8_t* keep, const int64_t* poff, const int32_t* post,
+                               uint8_t* maximal)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = warp; s < nsets; s += nw) {
+        if (!keep[s]) {
+            if (lane == 0) maximal[s] = 0;
+            continue;
+        }
+        unsigned long long a = starts[s];
+        int k = srt[a];
+        // rarest vertex of S
+        int64_t best_len = INT64_MAX;
+        int best_v = -1;
+        for (int i = lane; i < k; i += 32) {
+            int v = srt[a + 1 + i];
+            int64_t len = poff[v + 1] - poff[v];
+            if (len < best_len || (len == best_len && v < best_v)) {
+                best_len = len;
+                best_v = v;
+            }
+        }
+        for (int o = 16; o; o >>= 1) {
+            int64_t ol = __shfl_xor_sync(0xffffffffu, best_len, o);
+            int ov = __shfl_xor_sync(0xffffffffu, best_v, o);
+            if (ol < best_len || (ol == best_len && ov < best_v)) {
+                best_len = ol;
+                best_v = ov;
+            }
+        }
+        bool covered = false;
+        if (k > 0 && best_v >= 0) {
+            int64_t lo = poff[best_v], hi = poff[best_v + 1];
+            for (int64_t base = lo; base < hi; base += 32) {
+                int64_t e = base + lane;
+                if (e < hi) {
+                    unsigned long long b = starts[post[e]];
+                    if (srt[b] > k && subset_of(srt, a, b)) covered = true;
+                }
+                if (__any_sync(0xffffffffu, covered)) break;
+            }
+        }
+        covered = __any_sync(0xffffffffu, covered);
+        if (lane == 0) maximal[s] = covered ? 0 : 1;
+    }
+}
+
+// 5. survivors: sizes for a scan, then copy
+__global__ void survivor_len_kernel(const int32_t* srt, const unsigned long long* starts,
+                                    int64_t nsets, const uint8_t* maximal, int64_t* len)
+{
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsets) return;
+    len[s] = maximal[s] ? (int64_t)srt[starts[s]] + 1 : 0;
+}
+
+__global__ void survivor_copy_kernel(const int32_t* srt, const unsigned long long* starts,
+                                     int64_t nsets, const uint8_t* maximal, const int64_t* pos,
+                                     int32_t* out)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t s = warp; s < nsets; s += nw) {
+        if (!maximal[s]) continue;
+        unsigned long long a = starts[s];
+        int k = srt[a];
+        for (int i = lane; i <= k; i += 32) out[pos[s] + i] = srt[a + i];
+    }
+}
+
+} // namespace
+
+#define FCK(call)                                                                \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) return std::string(#call) + ": " + cudaGetErrorString(e_); \
+    } while (0)
+
+std::string FilterScratch::ensure(void** p, size_t* have, size_t need)
+{
+    if (need <= *have) return "";
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    cudaError_t e = cudaMalloc(p, need);
+    if (e != cudaSuccess) return std::string("filter scratch: ") + cudaGetErrorString(e);
+    *have = need;
+    return "";
+}
+
+void FilterScratch::release()
+{
+    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &sizes, &keep, &maximal, &cnt,
+                     &poff, &cursor, &post, &len, &pos, &out, &temp}) {
+        if (*pp) cudaFree(*pp);
+        *pp = nullptr;
+    }
+    sorted_n = hash_n = hash2_n = order_n = order2_n = sizes_n = keep_n = maximal_n = cnt_n =
+        poff_n = cursor_n = post_n = len_n = pos_n = out_n = temp_n = 0;
+}
+
+std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
+                           const unsigned long long* d_starts, int64_t nsets, int32_t n_vertices,
+                           cudaStream_t s, int sms, std::vector<int32_t>& host_out,
+                           int64_t& host_nsets, int64_t* launches)
+{
+    host_out.clear();
+    host_nsets = 0;
+    if (nsets == 0) return "";
+    std::string e;
+    const int64_t nv = std::max<int64_t>(n_vertices, 1);
+#define ENS(ptr, n, bytes)                                              \
+    e = F.ensure((void**)&F.ptr, &F.ptr##_n, (size_t)(bytes));          \
+    if (!e.empty()) return e;
+    ENS(sorted, sorted_n, sizeof(int32_t) * nints);
+    ENS(hash, hash_n, sizeof(unsigned long long) * nsets);
+    ENS(hash2, hash2_n, sizeof(unsigned long long) * nsets);
+    ENS(order, order_n, sizeof(int32_t) * nsets);
+    ENS(order2, order2_n, sizeof(int32_t) * nsets);
+    ENS(sizes, sizes_n, sizeof(int32_t) * nsets);
+    ENS(keep, keep_n, nsets);
+    ENS(maximal, maximal_n, nsets);
+    ENS(cnt, cnt_n, sizeof(int32_t) * (nv + 1));
+    ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
+    ENS(cursor, cursor_n, sizeof(int64_t) * (nv + 1));
+    ENS(len, len_n, sizeof(int64_t) * nsets);
+    ENS(pos, pos_n, sizeof(int64_t) * (nsets + 1));
+    const int blocks = sms * 8;
+    sort_hash_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
+                                            (unsigned long long*)F.hash, (int32_t*)F.order,
+                                            (int32_t*)F.sizes);
+    // radix sort (hash, order)
+    size_t tb = 0;
+    FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)F.hash,
+                                        (unsigned long long*)F.hash2, (int32_t*)F.order,
+                                        (int32_t*)F.order2, (int)nsets, 0, 64, s));
+    size_t tb2 = 0;
+    FCK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, (int32_t*)F.cnt, (int64_t*)F.poff,
+                                      (int)(nv + 1), s));
+    size_t tb3 = 0;
+    FCK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, (int64_t*)F.len, (int64_t*)F.pos,
+                                      (int)nsets, s));
+    ENS(temp, temp_n, std::max(tb, std::max(tb2, tb3)) + 256);
+    tb = F.temp_n;
+    FCK(cub::DeviceRadixSort::SortPairs(F.temp, tb, (unsigned long long*)F.hash,
+                                        (unsigned long long*)F.hash2, (int32_t*)F.order,
+                                        (int32_t*)F.order2, (int)nsets, 0, 64, s));
+    dedupe_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
+        (int32_t*)F.sorted, d_starts, (unsigned long long*)F.hash2, (int32_t*)F.order2, nsets,
+        (uint8_t*)F.keep);
+    FCK(cudaMemsetAsync(F.cnt, 0, sizeof(int32_t) * (nv + 1), s));
+    count_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
+                                        (int32_t*)F.cnt);
+    tb = F.temp_n;
+    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int32_t*)F.cnt, (int64_t*)F.poff, (int)(nv + 1),
+                                      s));
+    int64_t total = 0;
+    FCK(cudaMemcpyAsync(&total, (int64_t*)F.poff + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    FCK(cudaStreamSynchronize(s));
+    ENS(post, post_n, sizeof(int32_t) * std::max<int64_t>(total, 1));
+    FCK(cudaMemcpyAsync(F.cursor, F.poff, sizeof(int64_t) * (nv + 1), cudaMemcpyDeviceToDevice, s));
+    scatter_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
+                                          (int64_t*)F.cursor, (int32_t*)F.post);
+    maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
+                                          (int64_t*)F.poff, (int32_t*)F.post, (uint8_t*)F.maximal);
+    survivor_len_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
+        (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.maximal, (int64_t*)F.len);
+    tb = F.temp_n;
+    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos, (int)nsets, s));
+    int64_t last_pos = 0, last_len = 0;
+    FCK(cudaMemcpyAsync(&last_pos, (int64_t*)F.pos + nsets - 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s));
+    FCK(cudaMemcpyAsync(&last_len, (int64_t*)F.len + nsets - 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s));
+    FCK(cudaStreamSynchronize(s));
+    int64_t out_ints = last_pos + last_len;
+    ENS(out, out_n, sizeof(int32_t) * std::max<int64_t>(out_ints, 1));
+    survivor_copy_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets,
+                                                (uint8_t*)F.maximal, (int64_t*)F.pos,
+                                                (int32_t*)F.out);
+    FCK(cudaGetLastError());
+    if (launches) *launches += 9;
+    std::vector<int32_t> flat((size_t)out_ints);
+    if (out_ints)
+        FCK(cudaMemcpyAsync(flat.data(), F.out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
+    FCK(cudaStreamSynchronize(s));
+#undef ENS
+    // lexicographic order of the (already sorted) survivors
+    std::vector<std::pair<int64_t, int32_t>> idx;
+    for (int64_t p = 0; p < out_ints;) {
+        idx.emplace_back(p, flat[(size_t)p]);
+        p += 1 + flat[(size_t)p];
+    }
+    std::sort(idx.begin(), idx.end(), [&](const auto& x, const auto& y) {
+        return std::lexicographical_compare(flat.begin() + x.first + 1,
+                                            flat.begin() + x.first + 1 + x.second,
+                                            flat.begin() + y.first + 1,
+                                            flat.begin() + y.first + 1 + y.second);
+    });
+    host_out.reserve((size_t)out_ints);
+    for (auto& pr : idx)
+        host_out.insert(host_out.end(), flat.begin() + pr.first, flat.begin() + pr.first + 1 + pr.second);
+    host_nsets = (int64_t)idx.size();
+    return "";
+}
+
+} // namespace qcb

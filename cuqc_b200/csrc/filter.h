@@ -1,0 +1,31 @@
+// filter.h -- device non-maximal removal (filter.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace qcb {
+
+// Device scratch owned by a context, grown on demand.
+struct FilterScratch {
+    void *sorted = nullptr, *hash = nullptr, *hash2 = nullptr, *order = nullptr, *order2 = nullptr,
+         *sizes = nullptr, *keep = nullptr, *maximal = nullptr, *cnt = nullptr, *poff = nullptr,
+         *cursor = nullptr, *post = nullptr, *len = nullptr, *pos = nullptr, *out = nullptr,
+         *temp = nullptr;
+    size_t sorted_n = 0, hash_n = 0, hash2_n = 0, order_n = 0, order2_n = 0, sizes_n = 0,
+           keep_n = 0, maximal_n = 0, cnt_n = 0, poff_n = 0, cursor_n = 0, post_n = 0, len_n = 0,
+           pos_n = 0, out_n = 0, temp_n = 0;
+    std::string ensure(void** p, size_t* have, size_t need);
+    void release();
+};
+
+// Maximal sets of the emitted family (d_res with set starts d_starts) in
+// lexicographic order, flat [k, ids..] on the host.  Returns "" or an error.
+std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
+                           const unsigned long long* d_starts, int64_t nsets, int32_t n_vertices,
+                           cudaStream_t s, int sms, std::vector<int32_t>& host_out,
+                           int64_t& host_nsets, int64_t* launches);
+
+} // namespace qcb

@@ -22,6 +22,7 @@
 
 #include "../../include/qc.h"
 #include "expand_kernel.cuh"
+#include "filter.h"
 #include "host.h"
 
 using namespace qcb;
@@ -116,7 +117,8 @@ struct qc_context {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws;
+    DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts;
+    FilterScratch filt;
     int32_t pos_n = 0;
     unsigned long long resident = 0; // serial of the graph whose CSR is on the device
     int64_t arena_bytes = 0, stack_slots = 0, result_ints = 0;
@@ -158,8 +160,9 @@ extern "C" void qc_context_free(qc_context* c)
     if (!c) return;
     cudaSetDevice(c->cfg.device);
     for (DevBuf* b : {&c->off, &c->adj, &c->off2, &c->adj2, &c->pos, &c->ids, &c->md, &c->ubt,
-                      &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws})
+                      &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts})
         b->release();
+    c->filt.release();
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -254,6 +257,25 @@ __global__ void root_rows_kernel(const int64_t* off, const int32_t* adj, const i
     }
 }
 
+__global__ void globaltimer_kernel(unsigned long long* out)
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *out = t;
+}
+
+// the device's globaltimer, read through a scratch word of the control block
+static cudaError_t read_globaltimer(cudaStream_t s, Control* scratch, unsigned long long* out)
+{
+    unsigned long long* w = &scratch->wait_fail_where;
+    globaltimer_kernel<<<1, 1, 0, s>>>(w);
+    cudaError_t e = cudaMemcpyAsync(out, w, sizeof(*out), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(w, 0, sizeof(*w), s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
 // ------------------------------------------------------------------
 // mining
 // ------------------------------------------------------------------
@@ -329,6 +351,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(c->stack.ensure(sizeof(WorkItem) * (size_t)c->stack_slots));
         CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
         CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
+        const int64_t set_cap = std::max<int64_t>(c->result_ints / 4, 1024);
+        CK(c->starts.ensure(sizeof(unsigned long long) * (size_t)set_cap));
         CK(cudaMemsetAsync(c->slot.p, 0, sizeof(int32_t) * (size_t)c->stack_slots, s));
 
         uint64_t rb = rec_bytes(t, W);
@@ -363,6 +387,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         ctl.arena_top = rb;
         ctl.arena_cap = (unsigned long long)c->arena_bytes;
         ctl.result_cap = (unsigned long long)c->result_ints;
+        ctl.set_cap = (unsigned long long)set_cap;
         ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots, INT32_MAX);
         ctl.stack_top = 1;
         ctl.pending = 1;
@@ -384,11 +409,20 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.stack = c->stack.as<WorkItem>();
         P.slot = c->slot.as<int32_t>();
         P.results = c->results.as<int32_t>();
+        P.set_starts = c->starts.as<unsigned long long>();
         P.ws = c->ws.as<char>();
         P.ws_stride = L.total;
         P.max_t = t;
         P.split = 8;
+        P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
+        P.deadline_ns = 0;
+        if (c->cfg.time_limit_ms > 0) {
+            // device globaltimer is nanoseconds; read it once on the device
+            unsigned long long now = 0;
+            CK(read_globaltimer(s, c->ctl.as<Control>(), &now));
+            P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
+        }
         CK(cudaEventRecord(c->ev[1], s));
         expand_kernel<<<blocks, wpb * 32, 0, s>>>(P);
         CK(cudaGetLastError());
@@ -410,11 +444,15 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
             return fail(QC_ERR_TASK_OVERFLOW, "task arena/stack exhausted after growing");
         }
         if (ctl.status & ST_RESULT_OVERFLOW) {
-            c->result_ints = std::max<int64_t>(c->result_ints * 4, (int64_t)ctl.result_top * 2);
+            c->result_ints = std::max<int64_t>({c->result_ints * 4, (int64_t)ctl.result_top * 2,
+                                                (int64_t)ctl.emitted * 8});
             if (attempt < 6) continue;
             return fail(QC_ERR_RESULT_OVERFLOW, "result buffer exhausted after growing");
         }
         if (ctl.status & ST_TOO_LARGE) return fail(QC_ERR_TOO_LARGE, "task larger than workspace");
+        if (ctl.status & ST_DEADLINE)
+            return fail(QC_ERR_ITER_LIMIT, "time limit reached after " + std::to_string(ctl.tasks) +
+                                               " tasks, " + std::to_string(ctl.branches) + " branches");
         if (ctl.status & ST_ITER_LIMIT)
             return fail(QC_ERR_ITER_LIMIT, "device wait gave up (site " +
                                                std::to_string(ctl.wait_fail_where) + ")");
@@ -430,19 +468,26 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         r->st.kernel_ms = kms;
         r->st.arena_peak = (int64_t)ctl.arena_top;
         r->st.kernel_launches = c->launches;
-        flat.resize((size_t)ctl.result_top);
-        if (!flat.empty())
-            CK(cudaMemcpyAsync(flat.data(), c->results.p, sizeof(int32_t) * flat.size(),
-                               cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
+        if (c->cfg.keep_emitted) {
+            flat.resize((size_t)ctl.result_top);
+            if (!flat.empty())
+                CK(cudaMemcpyAsync(flat.data(), c->results.p, sizeof(int32_t) * flat.size(),
+                                   cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
         r->st.enum_ms = ms_since(t_enum);
         break;
     }
 
+    // non-maximal removal on the device
     auto t_filter = clk::now();
-    maximal_sets(flat.data(), (int64_t)flat.size(), r->sets, r->nsets);
+    std::string fe = filter_maximal(c->filt, c->results.as<int32_t>(), r->st.emitted_ints,
+                                    c->starts.as<unsigned long long>(), r->st.emitted, h.n, s,
+                                    c->sms, r->sets, r->nsets, &c->launches);
+    if (!fe.empty()) return fail(QC_ERR_CUDA, fe);
     r->st.filter_ms = ms_since(t_filter);
     r->st.maximal = r->nsets;
+    r->st.kernel_launches = c->launches;
     if (c->cfg.keep_emitted) {
         r->emitted.swap(flat);
         r->emitted_sets = r->st.emitted;

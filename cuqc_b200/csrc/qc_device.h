@@ -24,7 +24,8 @@ enum : int {
     ST_TASK_OVERFLOW = 1,   // arena or stack exhausted
     ST_RESULT_OVERFLOW = 2, // emitted-set buffer exhausted
     ST_ITER_LIMIT = 4,      // a bounded wait gave up
-    ST_TOO_LARGE = 8        // task larger than the workspace supports
+    ST_TOO_LARGE = 8,       // task larger than the workspace supports
+    ST_DEADLINE = 16        // the run's time budget ran out
 };
 
 struct Control {
@@ -32,6 +33,7 @@ struct Control {
     unsigned long long arena_cap;
     unsigned long long result_top; // ints of emitted sets written
     unsigned long long result_cap;
+    unsigned long long set_cap;    // capacity of the set-start array
     int stack_top;
     int stack_cap;
     int pending;                   // work items pushed and not yet finished
@@ -87,11 +89,14 @@ struct ExpandParams {
     WorkItem* stack;
     int32_t* slot;       // 0 free, 1 full, 2 being written, 3 being read
     int32_t* results;
+    unsigned long long* set_starts; // start offset (in results) of every emitted set
     char* ws;            // per-warp workspace
     int64_t ws_stride;   // bytes per warp
     int32_t max_t;       // largest task the workspace holds
     int32_t split;       // branches per work item before splitting
+    int32_t small_path;  // 1: tasks of <= 32 vertices use the register path
     int64_t wait_ns;     // give up a wait after this long without progress
+    unsigned long long deadline_ns; // globaltimer value to stop at (0: none)
 };
 
 // Per-warp workspace layout for tasks of up to max_t vertices.

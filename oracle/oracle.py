@@ -35,7 +35,8 @@ class Stats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "tasks", "lookahead_hits", "branches", "children", "emitted", "emitted_vertices",
         "parent_vertices", "p_rows", "child_vertices", "max_task", "root_size",
-        "stale_uses", "stale_oob")]
+        "stale_uses", "stale_oob", "tasks_le32", "tasks_le64", "tasks_le128", "tasks_gt128",
+        "branches_le32", "branches_le64", "branches_le128", "branches_gt128")]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -182,31 +183,35 @@ def refcpu_available():
     return os.path.exists(REFCPU_PATH)
 
 
-def refcpu_run(graph_path, gamma_str, min_size, workdir=None, caps=None):
+def refcpu_run(graph_path, gamma_str, min_size, workdir=None, caps=None, times=None):
     """Run the reference's serial CPU enumeration + RemoveNonMax.
 
-    Returns (result text, emitted sets from its temp file as a flat list)."""
+    Returns (result text, emitted sets from its temp file as a flat list).
+    If `times` is a dict it receives load_ms, enum_ms, rm_ms."""
     global _refcpu
     if _refcpu is None:
         L = C.CDLL(REFCPU_PATH)
         L.refcpu_run.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_char_p,
                                  C.c_longlong, C.c_longlong, C.c_longlong, C.c_longlong,
-                                 C.POINTER(C.c_longlong)]
+                                 C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
         L.refcpu_run.restype = C.c_int
         _refcpu = L
     caps = caps or (1 << 26, 1 << 28, 1 << 24, 1 << 26)
     wd = workdir or tempfile.mkdtemp(prefix="refcpu_")
     temp, out = os.path.join(wd, "temp.txt"), os.path.join(wd, "out.txt")
     lv = C.c_longlong()
+    tms = (C.c_double * 3)()
     cwd = os.getcwd()
     os.chdir(wd)  # RemoveNonMax prints only; files are explicit paths
     try:
         rc = _refcpu.refcpu_run(graph_path.encode(), str(gamma_str).encode(), int(min_size),
-                                temp.encode(), out.encode(), *caps, C.byref(lv))
+                                temp.encode(), out.encode(), *caps, C.byref(lv), tms)
     finally:
         os.chdir(cwd)
     if rc < 0:
         raise RuntimeError("reference CPU path could not read %s" % graph_path)
+    if times is not None:
+        times.update(load_ms=tms[0], enum_ms=tms[1], rm_ms=tms[2])
     with open(out) as f:
         text = f.read()
     flat = []

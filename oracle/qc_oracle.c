@@ -71,6 +71,8 @@ typedef struct {
     int64_t root_size;        /* vertices in the root task                 */
     int64_t stale_uses;       /* host rules: map lookups that hit a stale entry */
     int64_t stale_oob;        /*   ... pointing outside the current vertex array */
+    int64_t tasks_le32, tasks_le64, tasks_le128, tasks_gt128; /* task size histogram */
+    int64_t branches_le32, branches_le64, branches_le128, branches_gt128; /* by parent size */
 } qo_stats;
 
 typedef struct {
@@ -683,6 +685,10 @@ static void process_task(qo_ctx* c, qo_vtx* v, int t, qo_stack* s, qo_vtx* w)
     int expansions = nc;
     c->st.tasks++;
     if (t > c->st.max_task) c->st.max_task = t;
+    if (t <= 32) c->st.tasks_le32++;
+    else if (t <= 64) c->st.tasks_le64++;
+    else if (t <= 128) c->st.tasks_le128++;
+    else c->st.tasks_gt128++;
 
     if (lookahead(c, v, t, m, nc)) {
         c->st.lookahead_hits++;
@@ -700,6 +706,10 @@ static void process_task(qo_ctx* c, qo_vtx* v, int t, qo_stack* s, qo_vtx* w)
         int pid = w[m].id;
         c->st.branches++;
         c->st.parent_vertices += t;
+        if (t <= 32) c->st.branches_le32++;
+        else if (t <= 64) c->st.branches_le64++;
+        else if (t <= 128) c->st.branches_le128++;
+        else c->st.branches_gt128++;
         c->st.p_rows += (c->off[pid + 1] - c->off[pid]) + (c->off2[pid + 1] - c->off2[pid]);
 
         qo_bounds b = {0, 0, 0};

@@ -22,8 +22,9 @@ extern "C" int refcpu_run(const char* graph_path, const char* gamma_str, int min
                           const char* temp_path, const char* out_path,
                           long long task_vertex_cap, long long buffer_vertex_cap,
                           long long buffer_task_cap, long long clique_cap,
-                          long long* levels_out)
+                          long long* levels_out, double* times_ms)
 {
+    auto t0 = std::chrono::steady_clock::now();
     ifstream gs(graph_path, ios::in);
     if (!gs.is_open()) return -1;
     CPU_Graph hg(gs);
@@ -70,6 +71,7 @@ extern "C" int refcpu_run(const char* graph_path, const char* gamma_str, int min
     *hc.cliques_count = 0;
 
     ofstream temp(temp_path);
+    auto t1 = std::chrono::steady_clock::now();
     initialize_tasks(hg, hd);
     long long levels = 0;
     while (!*hd.maximal_expansion) {
@@ -79,6 +81,7 @@ extern "C" int refcpu_run(const char* graph_path, const char* gamma_str, int min
     }
     flush_cliques(hc, temp);
     temp.close();
+    auto t2 = std::chrono::steady_clock::now();
     if (levels_out) *levels_out = levels;
 
     // RemoveNonMax dereferences an empty prefix tree (main.cu:4834); only
@@ -93,6 +96,12 @@ extern "C" int refcpu_run(const char* graph_path, const char* gamma_str, int min
             ofstream empty(out_path);
             rc = 1;
         }
+    }
+    auto t3 = std::chrono::steady_clock::now();
+    if (times_ms) {
+        times_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        times_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        times_ms[2] = std::chrono::duration<double, std::milli>(t3 - t2).count();
     }
     delete hd.tasks1_count; delete[] hd.tasks1_offset; delete[] hd.tasks1_vertices;
     delete hd.tasks2_count; delete[] hd.tasks2_offset; delete[] hd.tasks2_vertices;

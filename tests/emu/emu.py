@@ -37,14 +37,16 @@ def lib():
         L = C.CDLL(SO)
         P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
         L.emu_mine.argtypes = [C.c_int, P64, P32, P64, P32, C.c_double, C.c_int, C.c_int, C.c_int,
-                               C.c_longlong, P64, C.POINTER(P32), P64]
+                               C.c_int, C.c_longlong, P64, C.POINTER(P32), P64, C.c_int,
+                               C.c_longlong]
         L.emu_mine.restype = C.c_int
         L.emu_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
 
-def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20):
+def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20, small_path=1, stack_cap=0,
+         result_cap=0):
     """Emitted multiset (flat [k, ids..]) and counters of the emulated kernel."""
     L = lib()
     off, adj = np.ascontiguousarray(g.off, np.int64), np.ascontiguousarray(g.adj, np.int32)
@@ -55,8 +57,9 @@ def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20):
     st = L.emu_mine(int(g.n), off.ctypes.data_as(P64 := C.POINTER(C.c_int64)),
                     adj.ctypes.data_as(C.POINTER(C.c_int32)), off2.ctypes.data_as(P64),
                     adj2.ctypes.data_as(C.POINTER(C.c_int32)), float(gamma), int(min_size),
-                    int(warps), int(split), int(arena_bytes), C.byref(ni), C.byref(buf),
-                    cnt.ctypes.data_as(P64))
+                    int(warps), int(split), int(small_path), int(arena_bytes), C.byref(ni),
+                    C.byref(buf),
+                    cnt.ctypes.data_as(P64), int(stack_cap), int(result_cap))
     flat = np.zeros(0, np.int32)
     if ni.value:
         flat = np.ctypeslib.as_array(buf, shape=(ni.value,)).copy()

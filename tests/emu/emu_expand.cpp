@@ -8,6 +8,7 @@
 #include "../../cuqc_b200/csrc/expand_kernel.cuh"
 #include "../../cuqc_b200/csrc/host.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include <vector>
 
@@ -15,8 +16,9 @@ using namespace qcb;
 
 extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
                         const int32_t* adj2, double gamma, int min_size, int warps, int split,
+                        int small_path,
                         long long arena_bytes, int64_t* out_nints, int32_t** out_buf,
-                        int64_t* counters)
+                        int64_t* counters, int stack_cap, long long result_cap)
 {
     HostGraph g;
     g.n = n;
@@ -64,8 +66,9 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     Control ctl{};
     ctl.arena_top = rec_bytes(t, W);
     ctl.arena_cap = (unsigned long long)arena_bytes;
-    ctl.result_cap = 1ull << 24;
-    ctl.stack_cap = 1 << 20;
+    ctl.result_cap = result_cap > 0 ? (unsigned long long)result_cap : (1ull << 24);
+    ctl.set_cap = ctl.result_cap / 2 + 1;
+    ctl.stack_cap = stack_cap > 0 ? stack_cap : (1 << 20);
     ctl.stack_top = 1;
     ctl.pending = 1;
     std::vector<WorkItem> stack((size_t)ctl.stack_cap);
@@ -73,6 +76,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     stack[0] = WorkItem{0, -1, -1};
     slot[0] = 1;
     std::vector<int32_t> results((size_t)ctl.result_cap);
+    std::vector<unsigned long long> set_starts((size_t)ctl.set_cap);
     WsLayout L = ws_layout(t);
     std::vector<char> ws((size_t)(L.total * warps));
 
@@ -88,10 +92,12 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     P.stack = stack.data();
     P.slot = slot.data();
     P.results = results.data();
+    P.set_starts = set_starts.data();
     P.ws = ws.data();
     P.ws_stride = L.total;
     P.max_t = t;
     P.split = split;
+    P.small_path = small_path;
     P.wait_ns = 20000000000ll;
     emu_launch(1, warps * 32, [&] { expand_kernel(P); });
 
@@ -103,7 +109,8 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     counters[5] = ctl.status;
     counters[6] = ctl.max_task;
     counters[7] = (int64_t)ctl.arena_top;
-    int64_t k = (int64_t)ctl.result_top;
+    int64_t k = std::min<int64_t>((int64_t)ctl.result_top, (int64_t)ctl.result_cap);
+    if (ctl.status) k = 0;
     int32_t* out = (int32_t*)malloc(sizeof(int32_t) * (size_t)(k > 0 ? k : 1));
     for (int64_t i = 0; i < k; i++) out[i] = results[(size_t)i];
     *out_nints = k;

@@ -12,23 +12,26 @@ def canon(flat):
     return sorted(tuple(sorted(s)) for s in oracle.unpack(flat))
 
 
-CASES = [  # (n, p, seed, planted, size, gamma, min_size, warps, split)
+CASES = [  # (n, p, seed, planted, size, gamma, min_size, warps, split); n > 32 uses both paths
     (20, 0.35, 1, 1, 7, 0.7, 4, 2, 2),
     (24, 0.3, 2, 2, 6, 0.8, 4, 1, 1000),
     (28, 0.25, 3, 1, 9, 0.9, 5, 3, 1),
     (18, 0.5, 4, 0, 0, 0.6, 4, 2, 3),
     (30, 0.2, 5, 2, 8, 1.0, 4, 2, 2),
     (26, 0.3, 6, 1, 10, 0.75, 6, 2, 4),
+    (44, 0.18, 7, 2, 12, 0.8, 6, 2, 3),
+    (40, 0.22, 8, 1, 14, 0.9, 7, 2, 4),
 ]
 
 
+@pytest.mark.parametrize("small_path", [1, 0])
 @pytest.mark.parametrize("case", CASES)
-def test_emulated_kernel_matches_oracle(case):
+def test_emulated_kernel_matches_oracle(case, small_path):
     n, p, seed, planted, size, gamma, ms, warps, split = case
     g = graphs.random_small(n, p, seed, planted=planted, size=size, density=0.95)
     want, st = oracle.mine(g, gamma, ms, "clean")
     assert st["tasks"] < 2500, "keep emulated cases small"
-    got, cnt, status = emu.mine(g, gamma, ms, warps=warps, split=split)
+    got, cnt, status = emu.mine(g, gamma, ms, warps=warps, split=split, small_path=small_path)
     assert status == 0
     assert canon(got) == canon(want)
     assert cnt["tasks"] == st["tasks"]
