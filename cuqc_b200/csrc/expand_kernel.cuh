@@ -641,6 +641,71 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
     }
 }
 
+
+// ------------------------------------------------------------------
+// record arena: size classes with lock-free free lists (lane 0 only)
+// A list head packs a 24-bit tag (bumped on every change, against ABA) and
+// the block offset / 16 + 1 (0 = empty); a free block's first 8 bytes hold
+// the next block in the same encoding without the tag.
+// ------------------------------------------------------------------
+
+constexpr unsigned long long kOffMask = (1ull << 40) - 1;
+
+__device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long long bytes, int& cls)
+{
+    cls = arena_class(bytes);
+    unsigned long long size = arena_class_bytes(cls);
+    unsigned long long* head = &P.ctl->free_head[cls];
+    for (int tries = 0; tries < 256; tries++) {
+        unsigned long long h = *(volatile unsigned long long*)head;
+        unsigned long long idx = h & kOffMask;
+        if (idx == 0) break;
+        unsigned long long off = (idx - 1) * 16;
+        unsigned long long next = *(volatile unsigned long long*)(P.arena + off) & kOffMask;
+        unsigned long long nh = (((h >> 40) + 1) << 40) | next;
+        if (atomicCAS(head, h, nh) == h) {
+            __threadfence();
+            unsigned long long live = atomicAdd(&P.ctl->arena_live, size) + size;
+            atomicMax(&P.ctl->arena_live_peak, live);
+            return off;
+        }
+    }
+    unsigned long long at = atomicAdd(&P.ctl->arena_top, size);
+    if (at + size > P.ctl->arena_cap) {
+        set_status(P, ST_TASK_OVERFLOW);
+        return ~0ull;
+    }
+    unsigned long long live = atomicAdd(&P.ctl->arena_live, size) + size;
+    atomicMax(&P.ctl->arena_live_peak, live);
+    return at;
+}
+
+__device__ void arena_free(const ExpandParams& P, unsigned long long off, int cls)
+{
+    unsigned long long size = arena_class_bytes(cls);
+    unsigned long long* head = &P.ctl->free_head[cls];
+    for (int tries = 0; tries < (1 << 20); tries++) {
+        unsigned long long h = *(volatile unsigned long long*)head;
+        *(volatile unsigned long long*)(P.arena + off) = h & kOffMask;
+        __threadfence();
+        unsigned long long nh = (((h >> 40) + 1) << 40) | (off / 16 + 1);
+        if (atomicCAS(head, h, nh) == h) {
+            atomicAdd(&P.ctl->arena_live, 0ull - size);
+            return;
+        }
+    }
+    // contention beyond any plausible bound: keep the block (a leak, not a fault)
+}
+
+// a work item on this record is finished; the last one frees the block
+__device__ void release_record(const ExpandParams& P, unsigned long long rec)
+{
+    TaskHdr* h = (TaskHdr*)(P.arena + rec);
+    int cls = *(volatile int32_t*)&h->cls;
+    __threadfence();
+    if (atomicSub(&h->refs, 1) == 1) arena_free(P, rec, cls);
+}
+
 // ------------------------------------------------------------------
 // child task: Q-sort (main.cu:2059-2104) and compacted matrices
 // ------------------------------------------------------------------
@@ -719,13 +784,8 @@ __device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, co
     int Wc = words_for(tc);
     unsigned long long bytes = rec_bytes(tc, Wc);
     unsigned long long at = 0;
-    if (lane == 0) {
-        at = atomicAdd(&P.ctl->arena_top, bytes);
-        if (at + bytes > P.ctl->arena_cap) {
-            set_status(P, ST_TASK_OVERFLOW);
-            at = ~0ull;
-        }
-    }
+    int cls = 0;
+    if (lane == 0) at = arena_alloc(P, bytes, cls);
     at = __shfl_sync(QC_FULL, at, 0);
     if (at == ~0ull) return;
     char* rec = P.arena + at;
@@ -735,6 +795,8 @@ __device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, co
         h->m = m;
         h->cov = 0;
         h->W = Wc;
+        h->refs = 1;
+        h->cls = cls;
     }
     int32_t* cid = (int32_t*)(rec + rec_ids_off());
     int32_t* cl2 = (int32_t*)(rec + rec_l2_off(tc));
@@ -1128,13 +1190,8 @@ __device__ void child_small(const ExpandParams& P, const SmallTask& T, unsigned 
     }
     unsigned long long bytes = rec_bytes(tc, 1);
     unsigned long long at = 0;
-    if (lane == 0) {
-        at = atomicAdd(&P.ctl->arena_top, bytes);
-        if (at + bytes > P.ctl->arena_cap) {
-            set_status(P, ST_TASK_OVERFLOW);
-            at = ~0ull;
-        }
-    }
+    int cls = 0;
+    if (lane == 0) at = arena_alloc(P, bytes, cls);
     at = __shfl_sync(QC_FULL, at, 0);
     if (at == ~0ull) return;
     char* rec = P.arena + at;
@@ -1144,6 +1201,8 @@ __device__ void child_small(const ExpandParams& P, const SmallTask& T, unsigned 
         h->m = m2;
         h->cov = 0;
         h->W = 1;
+        h->refs = 1;
+        h->cls = cls;
     }
     if (lane < tc) {
         ((int32_t*)(rec + rec_ids_off()))[lane] = sid;
@@ -1368,6 +1427,8 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
             __syncwarp();
             __threadfence();
             if (lane == 0) {
+                int extra = (q_hi - P.split - q_lo) / P.split + 1;
+                atomicAdd(&((TaskHdr*)(P.arena + it.rec))->refs, extra);
                 for (int hi = q_hi - P.split; hi >= q_lo; hi -= P.split) {
                     WorkItem s;
                     s.rec = it.rec;
@@ -1390,7 +1451,11 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
 // the persistent kernel
 // ------------------------------------------------------------------
 
+#ifndef QC_EMULATION
+__global__ void __launch_bounds__(256, 2) expand_kernel(ExpandParams P)
+#else
 __global__ void expand_kernel(ExpandParams P)
+#endif
 {
     int lane = lane_id();
     int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1408,7 +1473,10 @@ __global__ void expand_kernel(ExpandParams P)
         process_item(P, ws, it);
         __syncwarp();
         __threadfence();
-        if (lane == 0) atomicSub(&P.ctl->pending, 1);
+        if (lane == 0) {
+            release_record(P, it.rec);
+            atomicSub(&P.ctl->pending, 1);
+        }
     }
 }
 

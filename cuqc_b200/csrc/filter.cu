@@ -251,7 +251,10 @@ std::string FilterScratch::ensure(void** p, size_t* have, size_t need)
     *p = nullptr;
     *have = 0;
     cudaError_t e = cudaMalloc(p, need);
-    if (e != cudaSuccess) return std::string("filter scratch: ") + cudaGetErrorString(e);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return std::string("filter scratch: ") + cudaGetErrorString(e);
+    }
     *have = need;
     return "";
 }

@@ -99,6 +99,7 @@ struct DevBuf {
         n = 0;
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e == cudaSuccess) n = bytes;
+        else cudaGetLastError(); // a failed allocation must not surface at a later check
         return e;
     }
     void release()
@@ -333,7 +334,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     CK(upload(c->ubt, ubt, s));
     CK(upload(c->ids, ids, s));
 
-    int wpb = c->cfg.warps_per_block > 0 ? c->cfg.warps_per_block : 8;
+    // expand_kernel is compiled with __launch_bounds__(256, 2): at most 8 warps a block
+    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 8;
     int resident = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
     if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
@@ -356,8 +358,10 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaMemsetAsync(c->slot.p, 0, sizeof(int32_t) * (size_t)c->stack_slots, s));
 
         uint64_t rb = rec_bytes(t, W);
-        if ((int64_t)rb > c->arena_bytes) {
-            c->arena_bytes = (int64_t)rb * 4;
+        const int root_cls = arena_class(rb);
+        const uint64_t root_block = arena_class_bytes(root_cls);
+        if ((int64_t)root_block > c->arena_bytes) {
+            c->arena_bytes = (int64_t)root_block * 4;
             continue;
         }
         CK(cudaEventRecord(c->ev[0], s));
@@ -369,6 +373,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         hd.m = 0;
         hd.cov = cov;
         hd.W = W;
+        hd.refs = 1;
+        hd.cls = root_cls;
         CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(rec + rec_ids_off(), ids.data(), sizeof(int32_t) * t,
                            cudaMemcpyHostToDevice, s));
@@ -384,7 +390,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         c->launches += 3;
 
         Control ctl{};
-        ctl.arena_top = rb;
+        ctl.arena_top = root_block;
+        ctl.arena_live = root_block;
         ctl.arena_cap = (unsigned long long)c->arena_bytes;
         ctl.result_cap = (unsigned long long)c->result_ints;
         ctl.set_cap = (unsigned long long)set_cap;
@@ -413,7 +420,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.ws = c->ws.as<char>();
         P.ws_stride = L.total;
         P.max_t = t;
-        P.split = 8;
+        P.split = c->cfg.split > 0 ? c->cfg.split : 1;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
         P.deadline_ns = 0;
@@ -451,8 +458,14 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         }
         if (ctl.status & ST_TOO_LARGE) return fail(QC_ERR_TOO_LARGE, "task larger than workspace");
         if (ctl.status & ST_DEADLINE)
-            return fail(QC_ERR_ITER_LIMIT, "time limit reached after " + std::to_string(ctl.tasks) +
-                                               " tasks, " + std::to_string(ctl.branches) + " branches");
+            return fail(QC_ERR_ITER_LIMIT,
+                        "time limit reached after " + std::to_string(ctl.tasks) + " tasks, " +
+                            std::to_string(ctl.branches) + " branches, " +
+                            std::to_string(ctl.emitted) + " emitted sets, " +
+                            std::to_string(ctl.result_top) + " result ints, " +
+                            std::to_string(ctl.arena_top) + " arena bytes, stack " +
+                            std::to_string(ctl.stack_top) + ", max task " +
+                            std::to_string(ctl.max_task));
         if (ctl.status & ST_ITER_LIMIT)
             return fail(QC_ERR_ITER_LIMIT, "device wait gave up (site " +
                                                std::to_string(ctl.wait_fail_where) + ")");
@@ -466,7 +479,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         r->st.p_rows = (int64_t)ctl.p_rows;
         r->st.child_vertices = (int64_t)ctl.child_vertices;
         r->st.kernel_ms = kms;
-        r->st.arena_peak = (int64_t)ctl.arena_top;
+        r->st.arena_peak = (int64_t)ctl.arena_live_peak;
         r->st.kernel_launches = c->launches;
         if (c->cfg.keep_emitted) {
             flat.resize((size_t)ctl.result_top);

@@ -16,7 +16,17 @@
 
 namespace qcb {
 
+__host__ __device__ inline int clz64(unsigned long long x)
+{
+#if defined(__CUDA_ARCH__)
+    return __clzll((long long)x);
+#else
+    return __builtin_clzll(x);
+#endif
+}
+
 constexpr int kWarp = 32;
+constexpr int kArenaClasses = 4 * 40; // arena size classes (see arena_class)
 
 // status bits written by the device
 enum : int {
@@ -44,6 +54,9 @@ struct Control {
     int max_task;
     int active_warps;              // warps still inside the work loop
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
+    unsigned long long arena_live;      // bytes in blocks currently allocated
+    unsigned long long arena_live_peak;
+    unsigned long long free_head[kArenaClasses]; // [tag:24 | offset/16:40], 0 = empty
 };
 
 struct WorkItem {
@@ -58,12 +71,33 @@ struct WorkItem {
 //   uint32 A1[t][W]         (A1[v] bit w: w in N(v))
 //   uint32 A2[t][W]         (A2[v] bit w: w in N2(v))
 struct TaskHdr {
-    int32_t t;   // vertices
-    int32_t m;   // members are positions [0, m)
-    int32_t cov; // covered candidates right after the members (root only)
-    int32_t W;   // words per bit row
-    int32_t pad[4];
+    int32_t t;    // vertices
+    int32_t m;    // members are positions [0, m)
+    int32_t cov;  // covered candidates right after the members (root only)
+    int32_t W;    // words per bit row
+    int32_t refs; // work items that still reference this record
+    int32_t cls;  // arena size class of the record's block
+    int32_t pad[2];
 };
+
+// Arena blocks come in size classes: four steps per power of two from
+// 256 B (2^(e-1) + s*2^(e-3), s = 1..4).  Freed blocks go to a lock-free
+// free list per class (see expand_kernel.cuh).
+
+__host__ __device__ inline int arena_class(unsigned long long bytes)
+{
+    if (bytes <= 256) return 0;
+    int e = 64 - clz64(bytes - 1); // 2^(e-1) < bytes <= 2^e
+    unsigned long long half = 1ull << (e - 1), q = 1ull << (e - 3);
+    int s = (int)((bytes - half + q - 1) / q); // 1..4
+    return (e - 9) * 4 + s;                    // e = 9 -> classes 1..4 (257..512 B)
+}
+__host__ __device__ inline unsigned long long arena_class_bytes(int c)
+{
+    if (c == 0) return 256;
+    int e = (c - 1) / 4 + 9, s = (c - 1) % 4 + 1;
+    return (1ull << (e - 1)) + (unsigned long long)s * (1ull << (e - 3));
+}
 
 __host__ __device__ inline uint64_t align16(uint64_t x) { return (x + 15) & ~uint64_t(15); }
 __host__ __device__ inline int words_for(int t) { return (t + 31) >> 5; }

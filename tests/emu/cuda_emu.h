@@ -105,6 +105,20 @@ inline int atomicCAS(int* a, int cmp, int v)
     __atomic_compare_exchange_n(a, &cmp, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
     return cmp;
 }
+inline unsigned long long atomicCAS(unsigned long long* a, unsigned long long cmp,
+                                    unsigned long long v)
+{
+    __atomic_compare_exchange_n(a, &cmp, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
+    return cmp;
+}
+inline unsigned long long atomicMax(unsigned long long* a, unsigned long long v)
+{
+    unsigned long long cur = __atomic_load_n(a, __ATOMIC_SEQ_CST);
+    while (cur < v && !__atomic_compare_exchange_n(a, &cur, v, false, __ATOMIC_SEQ_CST,
+                                                   __ATOMIC_SEQ_CST)) {
+    }
+    return cur;
+}
 inline int atomicMax(int* a, int v)
 {
     int cur = __atomic_load_n(a, __ATOMIC_SEQ_CST);

@@ -44,6 +44,8 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     h->m = 0;
     h->cov = cov;
     h->W = W;
+    h->refs = 1;
+    h->cls = arena_class(rec_bytes(t, W));
     int32_t* rid = (int32_t*)(arena.data() + rec_ids_off());
     uint32_t* A1 = (uint32_t*)(arena.data() + rec_a1_off(t));
     uint32_t* A2 = (uint32_t*)(arena.data() + rec_a2_off(t, W));
@@ -64,7 +66,8 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
         }
     }
     Control ctl{};
-    ctl.arena_top = rec_bytes(t, W);
+    ctl.arena_top = arena_class_bytes(h->cls);
+    ctl.arena_live = ctl.arena_top;
     ctl.arena_cap = (unsigned long long)arena_bytes;
     ctl.result_cap = result_cap > 0 ? (unsigned long long)result_cap : (1ull << 24);
     ctl.set_cap = ctl.result_cap / 2 + 1;
@@ -108,7 +111,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     counters[4] = (int64_t)ctl.lookahead_hits;
     counters[5] = ctl.status;
     counters[6] = ctl.max_task;
-    counters[7] = (int64_t)ctl.arena_top;
+    counters[7] = (int64_t)ctl.arena_live_peak;
     int64_t k = std::min<int64_t>((int64_t)ctl.result_top, (int64_t)ctl.result_cap);
     if (ctl.status) k = 0;
     int32_t* out = (int32_t*)malloc(sizeof(int32_t) * (size_t)(k > 0 ? k : 1));
