@@ -127,7 +127,7 @@ __device__ __forceinline__ bool bs_empty(const uint32_t* a, int W)
 // ------------------------------------------------------------------
 
 struct TaskView {
-    int t, m, cov, W;
+    int t, m, cov, W, inst;
     const int32_t* ids;
     int32_t* l2;
     const uint32_t* A1;
@@ -143,6 +143,7 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
     T.m = h->m;
     T.cov = h->cov;
     T.W = h->W;
+    T.inst = h->inst;
     T.ids = (const int32_t*)(arena + rec + rec_ids_off());
     T.l2 = (int32_t*)(arena + rec + rec_l2_off(T.t));
     T.A1 = (const uint32_t*)(arena + rec + rec_a1_off(T.t));
@@ -196,46 +197,46 @@ struct Bounds {
 // gamma tables (main.cu:526-533, 2144-2151)
 // ------------------------------------------------------------------
 
-__device__ __forceinline__ int md_at(const ExpandParams& P, int k)
+__device__ __forceinline__ int md_at(const Rules& R, int k)
 {
     k = k < 0 ? 0 : k;
-    k = k >= P.mdlen ? P.mdlen - 1 : k;
-    return P.md[k];
+    k = k >= R.mdlen ? R.mdlen - 1 : k;
+    return R.md[k];
 }
-__device__ __forceinline__ int mindeg(const ExpandParams& P, int k)
+__device__ __forceinline__ int mindeg(const Rules& R, int k)
 {
-    return md_at(P, k < P.min_size ? P.min_size : k);
+    return md_at(R, k < R.min_size ? R.min_size : k);
 }
-__device__ __forceinline__ int ubt_at(const ExpandParams& P, int d)
+__device__ __forceinline__ int ubt_at(const Rules& R, int d)
 {
     d = d < 0 ? 0 : d;
-    d = d >= P.mdlen ? P.mdlen - 1 : d;
-    return P.ubt[d];
+    d = d >= R.mdlen ? R.mdlen - 1 : d;
+    return R.ubt[d];
 }
 
 // main.cu:2167-2178
-__device__ __forceinline__ bool cand_valid(const ExpandParams& P, int in, int ex, int m,
+__device__ __forceinline__ bool cand_valid(const Rules& R, int in, int ex, int m,
                                            const Bounds& b)
 {
     int tot = in + ex;
-    if (tot < md_at(P, P.min_size)) return false;
-    if (tot < mindeg(P, m + ex + 1)) return false;
+    if (tot < md_at(R, R.min_size)) return false;
+    if (tot < mindeg(R, m + ex + 1)) return false;
     if (tot < b.med) return false;
-    if (in + b.U - 1 < md_at(P, m + b.L)) return false;
-    if (tot < mindeg(P, m + b.L)) return false;
+    if (in + b.U - 1 < md_at(R, m + b.L)) return false;
+    if (tot < mindeg(R, m + b.L)) return false;
     return true;
 }
 // main.cu:2180-2198
-__device__ __forceinline__ bool vert_extendable(const ExpandParams& P, int in, int ex, int m,
+__device__ __forceinline__ bool vert_extendable(const Rules& R, int in, int ex, int m,
                                                 const Bounds& b)
 {
     int tot = in + ex;
-    if (tot < md_at(P, P.min_size)) return false;
-    if (tot < mindeg(P, m + ex)) return false;
+    if (tot < md_at(R, R.min_size)) return false;
+    if (tot < mindeg(R, m + ex)) return false;
     if (tot < b.med) return false;
-    if (ex == 0 && in < mindeg(P, m + ex)) return false;
-    if (in + b.U < md_at(P, m + b.U)) return false;
-    if (tot < mindeg(P, m + b.L)) return false;
+    if (ex == 0 && in < mindeg(R, m + ex)) return false;
+    if (in + b.U < md_at(R, m + b.U)) return false;
+    if (tot < mindeg(R, m + b.L)) return false;
     return true;
 }
 
@@ -247,7 +248,7 @@ __device__ __forceinline__ bool vert_extendable(const ExpandParams& P, int in, i
 // only those passing validity under `b`), then prefix tables over bins in
 // descending value order: pcnt[j] = #values > vmax-j, psum[j] = their sum.
 // Values are bounded by vmax (members count).  Returns the number of values.
-__device__ int build_hist(const ExpandParams& P, Ws& ws, const uint32_t* cm, int t, int vmax,
+__device__ int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* cm, int t, int vmax,
                           bool filter_valid, int m, const Bounds& b)
 {
     int lane = lane_id();
@@ -258,7 +259,7 @@ __device__ int build_hist(const ExpandParams& P, Ws& ws, const uint32_t* cm, int
         int v = base + lane;
         if (v < t && bit(cm, v)) {
             int in = ws.indeg[v];
-            if (!filter_valid || cand_valid(P, in, ws.exdeg[v], m, b)) {
+            if (!filter_valid || cand_valid(R, in, ws.exdeg[v], m, b)) {
                 int j = vmax - (in > vmax ? vmax : in);
                 atomicAdd(&ws.hist[j], 1);
                 cnt++;
@@ -305,7 +306,7 @@ __device__ __forceinline__ long long top_sum(const Ws& ws, int vmax, int k)
 // The candidate histogram must be built.  Returns true when invalid.
 // ------------------------------------------------------------------
 
-__device__ bool lu_bounds(const ExpandParams& P, Ws& ws, const uint32_t* mm, int t, int m,
+__device__ bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
                           int ncand, int vmax, Bounds& b)
 {
     int lane = lane_id();
@@ -334,24 +335,24 @@ __device__ bool lu_bounds(const ExpandParams& P, Ws& ws, const uint32_t* mm, int
     int min_in_ex = wmin(me);
 
     bool invalid = false;
-    b.med = mindeg(P, m + 1);
-    if (min_in < md_at(P, m)) {
-        int lb = mindeg(P, m) - min_in;
+    b.med = mindeg(R, m + 1);
+    if (min_in < md_at(R, m)) {
+        int lb = mindeg(R, m) - min_in;
         // first L >= lb with !(L <= min_in_ex && min_in + L < md[m+L])
         for (int base = lb;; base += 32) {
             int L = base + lane;
-            bool cont = (L <= min_in_ex) && (min_in + L < md_at(P, m + L));
+            bool cont = (L <= min_in_ex) && (min_in + L < md_at(R, m + L));
             unsigned stop = __ballot_sync(QC_FULL, !cont);
             if (stop) {
                 lb = base + __ffs(stop) - 1;
                 break;
             }
         }
-        if (min_in + lb < md_at(P, m + lb)) {
+        if (min_in + lb < md_at(R, m + lb)) {
             lb = ncand + 1;
             invalid = true;
         }
-        int ub = ubt_at(P, min_tot) + 1 - m;
+        int ub = ubt_at(R, min_tot) + 1 - m;
         if (ub > ncand) ub = ncand;
         if (lb < ub) {
             // first k in [lb, ub] with k == ub || sum_in + S(k) >= m*md[m+k]
@@ -361,7 +362,7 @@ __device__ bool lu_bounds(const ExpandParams& P, Ws& ws, const uint32_t* mm, int
                 bool ok = false;
                 if (k <= ub) {
                     ok = (k == ub) ||
-                         (sum_in + top_sum(ws, vmax, k) >= (long long)m * md_at(P, m + k));
+                         (sum_in + top_sum(ws, vmax, k) >= (long long)m * md_at(R, m + k));
                 }
                 unsigned bal = __ballot_sync(QC_FULL, ok);
                 if (bal) {
@@ -369,7 +370,7 @@ __device__ bool lu_bounds(const ExpandParams& P, Ws& ws, const uint32_t* mm, int
                     break;
                 }
             }
-            if (sum_in + top_sum(ws, vmax, idx) < (long long)m * md_at(P, m + idx)) {
+            if (sum_in + top_sum(ws, vmax, idx) < (long long)m * md_at(R, m + idx)) {
                 lb = ub + 1;
                 invalid = true;
             } else {
@@ -378,34 +379,34 @@ __device__ bool lu_bounds(const ExpandParams& P, Ws& ws, const uint32_t* mm, int
                 for (int base = idx + 1; base <= ub; base += 32) {
                     int k = base + lane;
                     bool ok = (k <= ub) &&
-                              (sum_in + top_sum(ws, vmax, k) >= (long long)m * md_at(P, m + k));
+                              (sum_in + top_sum(ws, vmax, k) >= (long long)m * md_at(R, m + k));
                     int best = wmax(ok ? k : -1);
                     if (best > tub) tub = best;
                 }
                 if (ub > tub) ub = tub;
-                if (lb > 1) b.med = mindeg(P, m + lb);
+                if (lb > 1) b.med = mindeg(R, m + lb);
             }
         }
         b.U = ub;
         b.L = lb;
     } else {
         b.U = ncand;
-        b.L = m < P.min_size ? P.min_size - m : 0;
+        b.L = m < R.min_size ? R.min_size - m : 0;
     }
-    if (m + b.U < P.min_size) invalid = true;
+    if (m + b.U < R.min_size) invalid = true;
     if (b.U < 0 || b.U < b.L) invalid = true;
     return invalid;
 }
 
 // every member extendable? (main.cu:1749-1753)
-__device__ bool members_ok(const ExpandParams& P, Ws& ws, const uint32_t* mm, int t, int m,
+__device__ bool members_ok(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
                            const Bounds& b)
 {
     int lane = lane_id();
     int bad = 0;
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
-        if (v < t && bit(mm, v) && !vert_extendable(P, ws.indeg[v], ws.exdeg[v], m, b)) bad = 1;
+        if (v < t && bit(mm, v) && !vert_extendable(R, ws.indeg[v], ws.exdeg[v], m, b)) bad = 1;
     }
     return !__any_sync(QC_FULL, bad);
 }
@@ -422,14 +423,14 @@ __device__ void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, co
 }
 
 // out = {v in in_mask : cand_valid(v)} ; rem = in_mask \ out
-__device__ void filter_valid(const ExpandParams& P, Ws& ws, const uint32_t* in_mask, int t, int W,
+__device__ void filter_valid(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* in_mask, int t, int W,
                              int m, const Bounds& b, uint32_t* out, uint32_t* rem)
 {
     int lane = lane_id();
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
         bool in = v < t && bit(in_mask, v);
-        bool ok = in && cand_valid(P, ws.indeg[v], ws.exdeg[v], m, b);
+        bool ok = in && cand_valid(R, ws.indeg[v], ws.exdeg[v], m, b);
         unsigned bo = __ballot_sync(QC_FULL, ok);
         unsigned br = __ballot_sync(QC_FULL, in && !ok);
         if (lane == 0) {
@@ -451,31 +452,31 @@ __device__ void filter_valid(const ExpandParams& P, Ws& ws, const uint32_t* in_m
 // Returns true on invalid bounds or a non-extendable member.
 // ------------------------------------------------------------------
 
-__device__ bool degree_prune(const ExpandParams& P, const TaskView& T, Ws& ws, const uint32_t* M,
-                             int m, const uint32_t* Call, const uint32_t* D, uint32_t* R,
+__device__ bool degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
+                             int m, const uint32_t* Call, const uint32_t* D, uint32_t* Rm,
                              Bounds& b)
 {
     const int t = T.t, W = T.W;
     uint32_t* X = ws.mk[MK_X];
     uint32_t* who = ws.mk[MK_U];
     Bounds dummy = {0, 0, 0};
-    int nc = build_hist(P, ws, D, t, m, false, m, dummy);
-    if (lu_bounds(P, ws, M, t, m, nc, m, b)) return true;
-    if (!members_ok(P, ws, M, t, m, b)) return true;
-    filter_valid(P, ws, D, t, W, m, b, R, nullptr);
-    // X = Call \ R
-    for (int w = lane_id(); w < W; w += 32) X[w] = Call[w] & ~R[w];
+    int nc = build_hist(P, R, ws, D, t, m, false, m, dummy);
+    if (lu_bounds(P, R, ws, M, t, m, nc, m, b)) return true;
+    if (!members_ok(P, R, ws, M, t, m, b)) return true;
+    filter_valid(P, R, ws, D, t, W, m, b, Rm, nullptr);
+    // X = Call \ Rm
+    for (int w = lane_id(); w < W; w += 32) X[w] = Call[w] & ~Rm[w];
     __syncwarp();
-    while (!bs_empty(R, W) && !bs_empty(X, W)) {
-        for (int w = lane_id(); w < W; w += 32) who[w] = M[w] | R[w];
+    while (!bs_empty(Rm, W) && !bs_empty(X, W)) {
+        for (int w = lane_id(); w < W; w += 32) who[w] = M[w] | Rm[w];
         __syncwarp();
-        recount_exdeg(T, ws, who, R);
-        int nv = build_hist(P, ws, R, t, m, true, m, b);
-        if (lu_bounds(P, ws, M, t, m, nv, m, b)) return true;
-        if (!members_ok(P, ws, M, t, m, b)) return true;
-        // R' = valid(R), X = R \ R'
-        filter_valid(P, ws, R, t, W, m, b, ws.mk[MK_T], X);
-        bs_copy(R, ws.mk[MK_T], W);
+        recount_exdeg(T, ws, who, Rm);
+        int nv = build_hist(P, R, ws, Rm, t, m, true, m, b);
+        if (lu_bounds(P, R, ws, M, t, m, nv, m, b)) return true;
+        if (!members_ok(P, R, ws, M, t, m, b)) return true;
+        // Rm' = valid(Rm), X = Rm \ Rm'
+        filter_valid(P, R, ws, Rm, t, W, m, b, ws.mk[MK_T], X);
+        bs_copy(Rm, ws.mk[MK_T], W);
     }
     return false;
 }
@@ -490,7 +491,7 @@ __device__ __forceinline__ void set_status(const ExpandParams& P, int bits)
 }
 
 // write the ids of the vertices in mask `mm` (count k) as one set
-__device__ void emit_mask(const ExpandParams& P, const TaskView& T, const uint32_t* mm, int k)
+__device__ void emit_mask(const ExpandParams& P, const Rules& R, const TaskView& T, const uint32_t* mm, int k)
 {
     int lane = lane_id();
     unsigned long long at = 0;
@@ -515,24 +516,24 @@ __device__ void emit_mask(const ExpandParams& P, const TaskView& T, const uint32
         unsigned bal = __ballot_sync(QC_FULL, in);
         if (in) {
             int r = __popc(bal & ((1u << lane) - 1u));
-            P.results[at + 1 + written + r] = T.ids[v];
+            P.results[at + 1 + written + r] = T.ids[v] + R.vbase;
         }
         written += __popc(bal);
     }
 }
 
 // clique check (main.cu:1974-1995): every member has indeg >= md[m]
-__device__ void check_clique(const ExpandParams& P, const TaskView& T, Ws& ws, const uint32_t* mm,
+__device__ void check_clique(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* mm,
                              int m)
 {
     int lane = lane_id();
-    int need = md_at(P, m);
+    int need = md_at(R, m);
     int bad = 0;
     for (int base = 0; base < T.t; base += 32) {
         int v = base + lane;
         if (v < T.t && bit(mm, v) && ws.indeg[v] < need) bad = 1;
     }
-    if (!__any_sync(QC_FULL, bad)) emit_mask(P, T, mm, m);
+    if (!__any_sync(QC_FULL, bad)) emit_mask(P, R, T, mm, m);
 }
 
 // ------------------------------------------------------------------
@@ -655,7 +656,7 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
 {
     cls = arena_class(bytes);
     unsigned long long size = arena_class_bytes(cls);
-    unsigned long long* head = &P.ctl->free_head[cls];
+    unsigned long long* head = &P.ctl->free_head[cls * kArenaShards + (blockIdx.x % kArenaShards)];
     for (int tries = 0; tries < 256; tries++) {
         unsigned long long h = *(volatile unsigned long long*)head;
         unsigned long long idx = h & kOffMask;
@@ -683,7 +684,7 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
 __device__ void arena_free(const ExpandParams& P, unsigned long long off, int cls)
 {
     unsigned long long size = arena_class_bytes(cls);
-    unsigned long long* head = &P.ctl->free_head[cls];
+    unsigned long long* head = &P.ctl->free_head[cls * kArenaShards + (blockIdx.x % kArenaShards)];
     for (int tries = 0; tries < (1 << 20); tries++) {
         unsigned long long h = *(volatile unsigned long long*)head;
         *(volatile unsigned long long*)(P.arena + off) = h & kOffMask;
@@ -750,8 +751,8 @@ __device__ void sort_keys(Ws& ws, int n)
     }
 }
 
-__device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, const uint32_t* M,
-                            int m, const uint32_t* R, int nr)
+__device__ void write_child(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
+                            int m, const uint32_t* Rm, int nr)
 {
     int lane = lane_id();
     int tc = m + nr;
@@ -764,7 +765,7 @@ __device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, co
     for (int base = 0; base < T.t; base += 32) {
         int v = base + lane;
         bool isM = v < T.t && bit(M, v);
-        bool isR = v < T.t && bit(R, v);
+        bool isR = v < T.t && bit(Rm, v);
         bool in = isM || isR;
         unsigned bal = __ballot_sync(QC_FULL, in);
         if (in) {
@@ -797,6 +798,7 @@ __device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, co
         h->W = Wc;
         h->refs = 1;
         h->cls = cls;
+        h->inst = T.inst;
     }
     int32_t* cid = (int32_t*)(rec + rec_ids_off());
     int32_t* cl2 = (int32_t*)(rec + rec_l2_off(tc));
@@ -845,14 +847,14 @@ __device__ void write_child(const ExpandParams& P, const TaskView& T, Ws& ws, co
 // one branch: add parent position q (main.cu:1086-1178)
 // ------------------------------------------------------------------
 
-__device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, int q)
+__device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, int q)
 {
     const int t = T.t, W = T.W;
     int lane = lane_id();
     uint32_t* M = ws.mk[MK_M];
     uint32_t* PRE = ws.mk[MK_PRE];
     uint32_t* D = ws.mk[MK_D];
-    uint32_t* R = ws.mk[MK_R];
+    uint32_t* Rm = ws.mk[MK_R];
     uint32_t* CA = ws.mk[MK_CA];
     uint32_t* Kc = ws.mk[MK_K];
     uint32_t* who = ws.mk[MK_U];
@@ -880,18 +882,18 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
         atomicAdd(&P.ctl->branches, 1ull);
         atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
         int pid = T.ids[q];
-        atomicAdd(&P.ctl->p_rows, (unsigned long long)((P.off[pid + 1] - P.off[pid]) +
-                                                       (P.off2[pid + 1] - P.off2[pid])));
+        atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
+                                                       (R.off2[pid + 1] - R.off2[pid])));
     }
 
     Bounds b = {0, 0, 0};
-    if (degree_prune(P, T, ws, M, m1, PRE, D, R, b)) {
-        if (m1 >= P.min_size) check_clique(P, T, ws, M, m1);
+    if (degree_prune(P, R, T, ws, M, m1, PRE, D, Rm, b)) {
+        if (m1 >= R.min_size) check_clique(P, R, T, ws, M, m1);
         return;
     }
 
     // critical-vertex pruning (main.cu:1526-1707)
-    int critv = md_at(P, m1 + b.L);
+    int critv = md_at(R, m1 + b.L);
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
         bool k = v < t && bit(M, v) && ws.indeg[v] + ws.exdeg[v] == critv && ws.exdeg[v] > 0;
@@ -911,7 +913,7 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
                 acc |= T.A1[(int64_t)v * W + w];
             }
         }
-        CA[w] = acc & R[w];
+        CA[w] = acc & Rm[w];
     }
     __syncwarp();
     int nca = bs_count(CA, W);
@@ -923,7 +925,7 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
         int bad = 0;
         for (int base = 0; base < t; base += 32) {
             int v = base + lane;
-            if (v < t && (bit(M, v) || bit(R, v))) {
+            if (v < t && (bit(M, v) || bit(Rm, v))) {
                 int d = popc_and(T.A1 + (int64_t)v * W, CA, W);
                 ws.indeg[v] += d;
                 ws.exdeg[v] -= d;
@@ -936,7 +938,7 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
         if (__any_sync(QC_FULL, bad)) return;
         for (int w = lane; w < W; w += 32) {
             M[w] |= CA[w];
-            C2[w] = R[w] & ~CA[w];
+            C2[w] = Rm[w] & ~CA[w];
         }
         __syncwarp();
         m2 = m1 + nca;
@@ -950,17 +952,17 @@ __device__ void expand_branch(const ExpandParams& P, const TaskView& T, Ws& ws, 
         for (int w = words_for(t) + lane; w < W; w += 32) D2[w] = 0;
         __syncwarp();
     } else {
-        bs_copy(C2, R, W);
-        bs_copy(D2, R, W);
+        bs_copy(C2, Rm, W);
+        bs_copy(D2, Rm, W);
     }
     (void)who;
     uint32_t* R2 = ws.mk[MK_R];
     Bounds b2 = {0, 0, 0};
-    bool fail2 = degree_prune(P, T, ws, M, m2, C2, D2, R2, b2);
-    if (m2 >= P.min_size) check_clique(P, T, ws, M, m2);
+    bool fail2 = degree_prune(P, R, T, ws, M, m2, C2, D2, R2, b2);
+    if (m2 >= R.min_size) check_clique(P, R, T, ws, M, m2);
     if (fail2) return;
     int nr = bs_count(R2, W);
-    if (nr > 0) write_child(P, T, ws, M, m2, R2, nr);
+    if (nr > 0) write_child(P, R, T, ws, M, m2, R2, nr);
 }
 
 // ------------------------------------------------------------------
@@ -1007,7 +1009,7 @@ __device__ __forceinline__ bool in_set(unsigned s, int lane) { return (s >> lane
 __device__ __forceinline__ unsigned low_mask(int k) { return k >= 32 ? ~0u : ((1u << k) - 1u); }
 
 struct SmallTask {
-    int t, m, cov, id, l2;
+    int t, m, cov, inst, id, l2;
     unsigned a1, a2;
 };
 
@@ -1033,7 +1035,7 @@ __device__ __forceinline__ int sort_desc_prefix(int v)
 
 // LU bounds (main.cu:1857-1972) for members set M (m of them) and the
 // candidate indegree multiset given by lanes in `cs` with value `in`.
-__device__ bool lu_small(const ExpandParams& P, unsigned M, int m, unsigned cs, int in, int ex,
+__device__ bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int m, unsigned cs, int in, int ex,
                          Bounds& b)
 {
     int lane = lane_id();
@@ -1044,23 +1046,23 @@ __device__ bool lu_small(const ExpandParams& P, unsigned M, int m, unsigned cs, 
     int min_in_ex = rmin(mem && in == min_in ? ex : 0x7fffffff);
     int ncand = __popc(cs);
     bool invalid = false;
-    b.med = mindeg(P, m + 1);
-    if (min_in < md_at(P, m)) {
-        int lb = mindeg(P, m) - min_in;
+    b.med = mindeg(R, m + 1);
+    if (min_in < md_at(R, m)) {
+        int lb = mindeg(R, m) - min_in;
         for (int base = lb;; base += 32) {
             int L = base + lane;
-            bool cont = (L <= min_in_ex) && (min_in + L < md_at(P, m + L));
+            bool cont = (L <= min_in_ex) && (min_in + L < md_at(R, m + L));
             unsigned stop = __ballot_sync(QC_FULL, !cont);
             if (stop) {
                 lb = base + __ffs(stop) - 1;
                 break;
             }
         }
-        if (min_in + lb < md_at(P, m + lb)) {
+        if (min_in + lb < md_at(R, m + lb)) {
             lb = ncand + 1;
             invalid = true;
         }
-        int ub = ubt_at(P, min_tot) + 1 - m;
+        int ub = ubt_at(R, min_tot) + 1 - m;
         if (ub > ncand) ub = ncand;
         if (lb < ub) {
             // S(k) for k = lane: sum of the k largest candidate indegrees
@@ -1072,56 +1074,56 @@ __device__ bool lu_small(const ExpandParams& P, unsigned M, int m, unsigned cs, 
             int k = lane;
             long long Sk = excl;
             bool g = (k >= lb && k <= ub) &&
-                     (k == ub || (long long)sum_in + Sk >= (long long)m * md_at(P, m + k));
+                     (k == ub || (long long)sum_in + Sk >= (long long)m * md_at(R, m + k));
             unsigned bal = __ballot_sync(QC_FULL, g);
             int idx = bal ? __ffs(bal) - 1 : ub;
             long long Sidx = idx < 32 ? __shfl_sync(QC_FULL, excl, idx & 31) : s_at_32;
-            if ((long long)sum_in + Sidx < (long long)m * md_at(P, m + idx)) {
+            if ((long long)sum_in + Sidx < (long long)m * md_at(R, m + idx)) {
                 lb = ub + 1;
                 invalid = true;
             } else {
                 lb = idx;
                 bool g2 = (k > idx && k <= ub) &&
-                          ((long long)sum_in + Sk >= (long long)m * md_at(P, m + k));
+                          ((long long)sum_in + Sk >= (long long)m * md_at(R, m + k));
                 unsigned b2 = __ballot_sync(QC_FULL, g2);
                 int tub = b2 ? 31 - __clz(b2) : idx;
                 if (ub > tub) ub = tub;
-                if (lb > 1) b.med = mindeg(P, m + lb);
+                if (lb > 1) b.med = mindeg(R, m + lb);
             }
         }
         b.U = ub;
         b.L = lb;
     } else {
         b.U = ncand;
-        b.L = m < P.min_size ? P.min_size - m : 0;
+        b.L = m < R.min_size ? R.min_size - m : 0;
     }
-    if (m + b.U < P.min_size) invalid = true;
+    if (m + b.U < R.min_size) invalid = true;
     if (b.U < 0 || b.U < b.L) invalid = true;
     return invalid;
 }
 
 // degree pruning fixpoint (main.cu:1735-1855) on words; `ex` is updated in place
-__device__ bool prune_small(const ExpandParams& P, unsigned a1, unsigned M, int m, unsigned Call,
-                            unsigned D, unsigned& R, int in, int& ex, Bounds& b)
+__device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, unsigned M, int m, unsigned Call,
+                            unsigned D, unsigned& Rm, int in, int& ex, Bounds& b)
 {
     int lane = lane_id();
-    if (lu_small(P, M, m, D, in, ex, b)) return true;
-    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(P, in, ex, m, b))) return true;
-    R = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid(P, in, ex, m, b));
-    unsigned X = Call & ~R;
-    while (R && X) {
-        ex = __popc(a1 & R);
-        unsigned V = __ballot_sync(QC_FULL, in_set(R, lane) && cand_valid(P, in, ex, m, b));
-        if (lu_small(P, M, m, V, in, ex, b)) return true;
-        if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(P, in, ex, m, b))) return true;
-        unsigned R2 = __ballot_sync(QC_FULL, in_set(R, lane) && cand_valid(P, in, ex, m, b));
-        X = R & ~R2;
-        R = R2;
+    if (lu_small(P, R, M, m, D, in, ex, b)) return true;
+    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(R, in, ex, m, b))) return true;
+    Rm = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid(R, in, ex, m, b));
+    unsigned X = Call & ~Rm;
+    while (Rm && X) {
+        ex = __popc(a1 & Rm);
+        unsigned V = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid(R, in, ex, m, b));
+        if (lu_small(P, R, M, m, V, in, ex, b)) return true;
+        if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(R, in, ex, m, b))) return true;
+        unsigned R2 = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid(R, in, ex, m, b));
+        X = Rm & ~R2;
+        Rm = R2;
     }
     return false;
 }
 
-__device__ void emit_small(const ExpandParams& P, unsigned S, int id)
+__device__ void emit_small(const ExpandParams& P, const Rules& R, unsigned S, int id)
 {
     int lane = lane_id();
     int k = __popc(S);
@@ -1140,18 +1142,18 @@ __device__ void emit_small(const ExpandParams& P, unsigned S, int id)
     }
     at = __shfl_sync(QC_FULL, at, 0);
     if (at == ~0ull) return;
-    if (in_set(S, lane)) P.results[at + 1 + __popc(S & low_mask(lane))] = id;
+    if (in_set(S, lane)) P.results[at + 1 + __popc(S & low_mask(lane))] = id + R.vbase;
 }
 
-__device__ __forceinline__ void clique_small(const ExpandParams& P, unsigned M, int m, int in, int id)
+__device__ __forceinline__ void clique_small(const ExpandParams& P, const Rules& R, unsigned M, int m, int in, int id)
 {
     int lane = lane_id();
-    int need = md_at(P, m);
-    if (!__any_sync(QC_FULL, in_set(M, lane) && in < need)) emit_small(P, M, id);
+    int need = md_at(R, m);
+    if (!__any_sync(QC_FULL, in_set(M, lane) && in < need)) emit_small(P, R, M, id);
 }
 
 // child record of the vertices in M2 | R2, Q-sorted, matrices compacted
-__device__ void child_small(const ExpandParams& P, const SmallTask& T, unsigned M2, int m2,
+__device__ void child_small(const ExpandParams& P, const Rules& R, const SmallTask& T, unsigned M2, int m2,
                             unsigned R2, int in, int ex)
 {
     int lane = lane_id();
@@ -1203,6 +1205,7 @@ __device__ void child_small(const ExpandParams& P, const SmallTask& T, unsigned 
         h->W = 1;
         h->refs = 1;
         h->cls = cls;
+        h->inst = T.inst;
     }
     if (lane < tc) {
         ((int32_t*)(rec + rec_ids_off()))[lane] = sid;
@@ -1224,7 +1227,7 @@ __device__ void child_small(const ExpandParams& P, const SmallTask& T, unsigned 
     __syncwarp();
 }
 
-__device__ void branch_small(const ExpandParams& P, const SmallTask& T, int q)
+__device__ void branch_small(const ExpandParams& P, const Rules& R, const SmallTask& T, int q)
 {
     int lane = lane_id();
     unsigned Mm = low_mask(T.m);
@@ -1240,21 +1243,21 @@ __device__ void branch_small(const ExpandParams& P, const SmallTask& T, int q)
         atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
     }
     if (lane == q) {
-        atomicAdd(&P.ctl->p_rows, (unsigned long long)((P.off[T.id + 1] - P.off[T.id]) +
-                                                       (P.off2[T.id + 1] - P.off2[T.id])));
+        atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[T.id + 1] - R.off[T.id]) +
+                                                       (R.off2[T.id + 1] - R.off2[T.id])));
     }
     Bounds b = {0, 0, 0};
-    unsigned R = 0;
-    if (prune_small(P, T.a1, M1, m1, PRE, D, R, in, ex, b)) {
-        if (m1 >= P.min_size) clique_small(P, M1, m1, in, T.id);
+    unsigned Rm = 0;
+    if (prune_small(P, R, T.a1, M1, m1, PRE, D, Rm, in, ex, b)) {
+        if (m1 >= R.min_size) clique_small(P, R, M1, m1, in, T.id);
         return;
     }
     // critical vertices (main.cu:1526-1707)
-    int critv = md_at(P, m1 + b.L);
+    int critv = md_at(R, m1 + b.L);
     unsigned K = __ballot_sync(QC_FULL, in_set(M1, lane) && in + ex == critv && ex > 0);
-    unsigned CA = R & ror(in_set(K, lane) ? T.a1 : 0u);
+    unsigned CA = Rm & ror(in_set(K, lane) ? T.a1 : 0u);
     int nca = __popc(CA);
-    unsigned M2 = M1, C2 = R, D2 = R;
+    unsigned M2 = M1, C2 = Rm, D2 = Rm;
     int m2 = m1;
     if (nca > 0) {
         int d = __popc(T.a1 & CA);
@@ -1265,25 +1268,26 @@ __device__ void branch_small(const ExpandParams& P, const SmallTask& T, int q)
         if (__any_sync(QC_FULL, bad)) return;
         M2 = M1 | CA;
         m2 = m1 + nca;
-        C2 = R & ~CA;
+        C2 = Rm & ~CA;
         D2 = __ballot_sync(QC_FULL, in_set(C2, lane) && adj == nca);
     }
     Bounds b2 = {0, 0, 0};
     unsigned R2 = 0;
-    bool fail2 = prune_small(P, T.a1, M2, m2, C2, D2, R2, in, ex, b2);
-    if (m2 >= P.min_size) clique_small(P, M2, m2, in, T.id);
+    bool fail2 = prune_small(P, R, T.a1, M2, m2, C2, D2, R2, in, ex, b2);
+    if (m2 >= R.min_size) clique_small(P, R, M2, m2, in, T.id);
     if (fail2) return;
-    if (R2) child_small(P, T, M2, m2, R2, in, ex);
+    if (R2) child_small(P, R, T, M2, m2, R2, in, ex);
 }
 
 // a fresh task of at most 32 vertices, processed whole by one warp
-__device__ void process_small(const ExpandParams& P, const TaskView& V)
+__device__ void process_small(const ExpandParams& P, const Rules& R, const TaskView& V)
 {
     int lane = lane_id();
     SmallTask T;
     T.t = V.t;
     T.m = V.m;
     T.cov = V.cov;
+    T.inst = V.inst;
     bool act = lane < T.t;
     T.id = act ? V.ids[lane] : -1;
     T.a1 = act ? V.A1[lane] : 0u;
@@ -1297,19 +1301,19 @@ __device__ void process_small(const ExpandParams& P, const TaskView& V)
         atomicMax(&P.ctl->max_task, t);
     }
     // lookahead (main.cu:1349-1405)
-    int need_t = md_at(P, t);
+    int need_t = md_at(R, t);
     if (!__any_sync(QC_FULL, in_set(Mm, lane) && in + ex < need_t)) {
         int nc = t - m;
         if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
         bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
         if (!__any_sync(QC_FULL, bad)) {
             if (lane == 0) atomicAdd(&P.ctl->lookahead_hits, 1ull);
-            emit_small(P, low_mask(t), T.id);
+            emit_small(P, R, low_mask(t), T.id);
             return;
         }
     }
     // branches run until a member would fail on removal (main.cu:1092-1099)
-    int need = mindeg(P, m);
+    int need = mindeg(R, m);
     int pos = 0;
     if (in_set(Mm, lane)) {
         int k = need - in;
@@ -1324,7 +1328,7 @@ __device__ void process_small(const ExpandParams& P, const TaskView& V)
     if (qlo > t - 1) return;
     for (int q = t - 1; q >= qlo; q--) {
         if (*(volatile int*)&P.ctl->status) return;
-        branch_small(P, T, q);
+        branch_small(P, R, T, q);
     }
 }
 
@@ -1337,13 +1341,14 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
     TaskView T = task_view(P.arena, it.rec);
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
+    const Rules R = P.rules[T.inst];
     if (t > P.max_t) {
         if (lane == 0) set_status(P, ST_TOO_LARGE);
         return;
     }
     int q_lo = it.q_lo, q_hi = it.q_hi;
     if (q_lo < 0 && t <= 32 && P.small_path) {
-        process_small(P, T);
+        process_small(P, R, T);
         return;
     }
     if (q_lo < 0) {
@@ -1367,7 +1372,7 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
         }
         __syncwarp();
         // lookahead (main.cu:1349-1405)
-        int need_t = md_at(P, t);
+        int need_t = md_at(R, t);
         int bad = 0;
         for (int v = lane; v < m; v += 32)
             if (ws.indeg[v] + ws.exdeg[v] < need_t) bad = 1;
@@ -1383,12 +1388,12 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
                 uint32_t* all = ws.mk[MK_T];
                 bs_range(all, W, 0, t);
                 if (lane == 0) atomicAdd(&P.ctl->lookahead_hits, 1ull);
-                emit_mask(P, T, all, t);
+                emit_mask(P, R, T, all, t);
                 return;
             }
         }
         // branches executed before a member fails on removal (main.cu:1092-1099)
-        int need = mindeg(P, m);
+        int need = mindeg(R, m);
         int qmax = m + T.cov;
         for (int v = 0; v < m; v++) {
             int k = need - ws.indeg[v];
@@ -1443,8 +1448,40 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
     }
     for (int q = q_hi; q >= q_lo; q--) {
         if (*(volatile int*)&P.ctl->status) return;
-        expand_branch(P, T, ws, q);
+        expand_branch(P, R, T, ws, q);
     }
+}
+
+
+// Self-check of a dequeued work item before any lane reads its record: the
+// offset must be 16-byte aligned and inside the written arena, and the
+// header must describe a record that fits there.  A failure records the
+// site and value and the item is skipped instead of being dereferenced.
+__device__ bool item_ok(const ExpandParams& P, const WorkItem& it)
+{
+    unsigned long long top = *(volatile unsigned long long*)&P.ctl->arena_top;
+    unsigned long long cap = P.ctl->arena_cap;
+    unsigned long long lim = top < cap ? top : cap;
+    unsigned long long site = 0, val = it.rec;
+    if ((it.rec & 15ull) != 0) site = 1;
+    else if (it.rec + sizeof(TaskHdr) > lim) site = 2;
+    else {
+        const volatile TaskHdr* h = (const volatile TaskHdr*)(P.arena + it.rec);
+        int t = h->t, W = h->W, m = h->m, inst = h->inst;
+        if (t < 1 || t > P.max_t || W != words_for(t) || m < 0 || m > t) {
+            site = 3;
+            val = ((unsigned long long)(unsigned)t << 32) | (unsigned)W;
+        } else if (it.rec + rec_bytes(t, W) > lim) site = 4;
+        else if (inst < 0 || inst >= P.nrules) site = 5;
+        else if (it.q_lo >= 0 && (it.q_hi >= t || it.q_lo > it.q_hi)) site = 6;
+    }
+    if (site) {
+        if (atomicCAS((unsigned long long*)&P.ctl->check_site, 0ull, site) == 0ull)
+            P.ctl->check_value = val;
+        set_status(P, ST_CHECK);
+        return false;
+    }
+    return true;
 }
 
 // ------------------------------------------------------------------
@@ -1463,7 +1500,10 @@ __global__ void expand_kernel(ExpandParams P)
     for (;;) {
         WorkItem it;
         int r = 0;
-        if (lane == 0) r = pop_item(P, it);
+        if (lane == 0) {
+            r = pop_item(P, it);
+            if (r > 0 && !item_ok(P, it)) r = -1;
+        }
         r = __shfl_sync(QC_FULL, r, 0);
         if (r <= 0) break;
         it.rec = __shfl_sync(QC_FULL, it.rec, 0);

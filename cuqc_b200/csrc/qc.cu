@@ -113,12 +113,23 @@ struct DevBuf {
 
 } // namespace
 
+struct BatchBufs {
+    DevBuf off, adj, off2, adj2, md, ubt, rules, meta, ids, pos, adj_at, adj2_at;
+    void release()
+    {
+        for (DevBuf* b : {&off, &adj, &off2, &adj2, &md, &ubt, &rules, &meta, &ids, &pos, &adj_at,
+                          &adj2_at})
+            b->release();
+    }
+};
+
 struct qc_context {
     qc_config cfg{};
+    BatchBufs batch;
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts;
+    DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts, rules;
     FilterScratch filt;
     int32_t pos_n = 0;
     unsigned long long resident = 0; // serial of the graph whose CSR is on the device
@@ -161,9 +172,11 @@ extern "C" void qc_context_free(qc_context* c)
     if (!c) return;
     cudaSetDevice(c->cfg.device);
     for (DevBuf* b : {&c->off, &c->adj, &c->off2, &c->adj2, &c->pos, &c->ids, &c->md, &c->ubt,
-                      &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts})
+                      &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts,
+                      &c->rules})
         b->release();
     c->filt.release();
+    c->batch.release();
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -375,6 +388,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         hd.W = W;
         hd.refs = 1;
         hd.cls = root_cls;
+        hd.inst = 0;
         CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(rec + rec_ids_off(), ids.data(), sizeof(int32_t) * t,
                            cudaMemcpyHostToDevice, s));
@@ -404,13 +418,19 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         int one = 1;
         CK(cudaMemcpyAsync(c->slot.p, &one, sizeof(one), cudaMemcpyHostToDevice, s));
 
+        Rules rule{};
+        rule.off = c->off.as<int64_t>();
+        rule.off2 = c->off2.as<int64_t>();
+        rule.md = c->md.as<int32_t>();
+        rule.ubt = c->ubt.as<int32_t>();
+        rule.mdlen = (int32_t)md.size();
+        rule.min_size = min_size;
+        rule.vbase = 0;
+        CK(c->rules.ensure(sizeof(Rules)));
+        CK(cudaMemcpyAsync(c->rules.p, &rule, sizeof(rule), cudaMemcpyHostToDevice, s));
         ExpandParams P{};
-        P.off = c->off.as<int64_t>();
-        P.off2 = c->off2.as<int64_t>();
-        P.md = c->md.as<int32_t>();
-        P.ubt = c->ubt.as<int32_t>();
-        P.mdlen = (int32_t)md.size();
-        P.min_size = min_size;
+        P.rules = c->rules.as<Rules>();
+        P.nrules = 1;
         P.ctl = c->ctl.as<Control>();
         P.arena = c->arena.as<char>();
         P.stack = c->stack.as<WorkItem>();
@@ -456,6 +476,10 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
             if (attempt < 6) continue;
             return fail(QC_ERR_RESULT_OVERFLOW, "result buffer exhausted after growing");
         }
+        if (ctl.status & ST_CHECK)
+            return fail(QC_ERR_CUDA, "device self-check failed at site " +
+                                         std::to_string(ctl.check_site) + " value " +
+                                         std::to_string(ctl.check_value));
         if (ctl.status & ST_TOO_LARGE) return fail(QC_ERR_TOO_LARGE, "task larger than workspace");
         if (ctl.status & ST_DEADLINE)
             return fail(QC_ERR_ITER_LIMIT,
@@ -549,6 +573,352 @@ extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, i
     return QC_OK;
 }
 
+// ------------------------------------------------------------------
+// batched mining: many independent instances in one persistent launch
+// ------------------------------------------------------------------
+
+struct RootMeta {
+    unsigned long long rec; // arena offset of the root record
+    int32_t t, W, cov, inst, cls, vbase;
+    int64_t id_at;          // first id in the concatenated root-id array
+    int64_t row_at;         // first row in the flattened row index
+};
+
+// headers and ids of every root record (one thread per root id)
+__global__ void batch_root_fill_kernel(const RootMeta* meta, int nroots, const int32_t* ids_all,
+                                       int64_t total_rows, char* arena, int32_t* pos)
+{
+    int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= total_rows) return;
+    int lo = 0, hi = nroots - 1; // root j with row_at <= r
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (meta[mid].row_at <= r) lo = mid;
+        else hi = mid - 1;
+    }
+    const RootMeta& M = meta[lo];
+    int i = (int)(r - M.row_at);
+    char* rec = arena + M.rec;
+    int32_t id = ids_all[M.id_at + i];
+    ((int32_t*)(rec + rec_ids_off()))[i] = id;
+    ((int32_t*)(rec + rec_l2_off(M.t)))[i] = 0;
+    pos[M.vbase + id] = i;
+    if (i == 0) {
+        TaskHdr* h = (TaskHdr*)rec;
+        h->t = M.t;
+        h->m = 0;
+        h->cov = M.cov;
+        h->W = M.W;
+        h->refs = 1;
+        h->cls = M.cls;
+        h->inst = M.inst;
+        h->pad = 0;
+    }
+}
+
+// one warp per root row: set the bits of its 1-hop and 2-hop neighbours
+__global__ void batch_root_rows_kernel(const RootMeta* meta, int nroots, const int32_t* ids_all,
+                                       int64_t total_rows, const Rules* rules,
+                                       const int32_t* adj_base, const int64_t* adj_at,
+                                       const int32_t* adj2_base, const int64_t* adj2_at,
+                                       char* arena, const int32_t* pos)
+{
+    int lane = threadIdx.x & 31;
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp; r < total_rows; r += nw) {
+        int lo = 0, hi = nroots - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (meta[mid].row_at <= r) lo = mid;
+            else hi = mid - 1;
+        }
+        const RootMeta& M = meta[lo];
+        int i = (int)(r - M.row_at);
+        const Rules& R = rules[M.inst];
+        const int32_t* adj = adj_base + adj_at[M.inst];
+        const int32_t* adj2 = adj2_base + adj2_at[M.inst];
+        int u = ids_all[M.id_at + i];
+        char* rec = arena + M.rec;
+        uint32_t* r1 = (uint32_t*)(rec + rec_a1_off(M.t)) + (int64_t)i * M.W;
+        uint32_t* r2 = (uint32_t*)(rec + rec_a2_off(M.t, M.W)) + (int64_t)i * M.W;
+        const int32_t* pv = pos + M.vbase;
+        for (int64_t e = R.off[u] + lane; e < R.off[u + 1]; e += 32) {
+            int p = pv[adj[e]];
+            if (p >= 0) atomicOr(&r1[p >> 5], 1u << (p & 31));
+        }
+        for (int64_t e = R.off2[u] + lane; e < R.off2[u + 1]; e += 32) {
+            int p = pv[adj2[e]];
+            if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
+        }
+    }
+}
+
+__global__ void batch_root_unpos_kernel(const RootMeta* meta, int nroots, const int32_t* ids_all,
+                                        int64_t total_rows, int32_t* pos)
+{
+    int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= total_rows) return;
+    int lo = 0, hi = nroots - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (meta[mid].row_at <= r) lo = mid;
+        else hi = mid - 1;
+    }
+    const RootMeta& M = meta[lo];
+    pos[M.vbase + ids_all[M.id_at + (r - M.row_at)]] = -1;
+}
+
+
+static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const double* gammas,
+                            const int32_t* min_sizes, int32_t count, std::vector<qc_result*>& res)
+{
+    auto t_all = clk::now();
+    cudaStream_t s = c->stream;
+    CK(cudaSetDevice(c->cfg.device));
+    BatchBufs& B = c->batch; // reused across calls on this context
+    // host side: tables, level 0, concatenation
+    std::vector<int64_t> h_off, h_off2, adj_at(count), adj2_at(count);
+    std::vector<int32_t> h_adj, h_adj2, h_md, h_ubt, h_ids;
+    std::vector<Rules> rules(count);
+    std::vector<int64_t> off_at(count), md_at_(count);
+    std::vector<RootMeta> meta;
+    int64_t vtotal = 0;
+    int max_t = 1;
+    auto t_load = clk::now();
+    for (int i = 0; i < count; i++) {
+        const HostGraph& h = graphs[i]->h;
+        off_at[i] = (int64_t)h_off.size();
+        h_off.insert(h_off.end(), h.off.begin(), h.off.end());
+        h_off2.insert(h_off2.end(), h.off2.begin(), h.off2.end());
+        adj_at[i] = (int64_t)h_adj.size();
+        h_adj.insert(h_adj.end(), h.adj.begin(), h.adj.end());
+        adj2_at[i] = (int64_t)h_adj2.size();
+        h_adj2.insert(h_adj2.end(), h.adj2.begin(), h.adj2.end());
+        rules[i].vbase = (int32_t)vtotal;
+        vtotal += h.n;
+    }
+    if (vtotal > INT32_MAX) return fail(QC_ERR_TOO_LARGE, "batch has more than 2^31 vertices");
+    CK(upload(B.off, h_off, s));
+    CK(upload(B.off2, h_off2, s));
+    CK(upload(B.adj, h_adj, s));
+    CK(upload(B.adj2, h_adj2, s));
+    CK(upload(B.adj_at, adj_at, s));
+    CK(upload(B.adj2_at, adj2_at, s));
+    double load_ms = ms_since(t_load);
+
+    auto t_enum = clk::now();
+    uint64_t arena_at = 0;
+    for (int i = 0; i < count; i++) {
+        const HostGraph& h = graphs[i]->h;
+        std::vector<int32_t> md, ubt, ids;
+        gamma_tables(gammas[i], h.n, min_sizes[i], md, ubt);
+        md_at_[i] = (int64_t)h_md.size();
+        rules[i].mdlen = (int32_t)md.size();
+        rules[i].min_size = min_sizes[i];
+        h_md.insert(h_md.end(), md.begin(), md.end());
+        h_ubt.insert(h_ubt.end(), ubt.begin(), ubt.end());
+        int cov = 0;
+        build_root(h, md.data(), min_sizes[i], ids, cov);
+        if (ids.empty()) continue;
+        RootMeta M{};
+        M.t = (int32_t)ids.size();
+        M.W = words_for(M.t);
+        M.cov = cov;
+        M.inst = i;
+        M.cls = arena_class(rec_bytes(M.t, M.W));
+        M.vbase = rules[i].vbase;
+        M.rec = arena_at;
+        M.id_at = (int64_t)h_ids.size();
+        M.row_at = M.id_at;
+        arena_at += arena_class_bytes(M.cls);
+        h_ids.insert(h_ids.end(), ids.begin(), ids.end());
+        max_t = std::max(max_t, M.t);
+        meta.push_back(M);
+    }
+    CK(upload(B.md, h_md, s));
+    CK(upload(B.ubt, h_ubt, s));
+    for (int i = 0; i < count; i++) {
+        rules[i].md = B.md.as<int32_t>() + md_at_[i];
+        rules[i].ubt = B.ubt.as<int32_t>() + md_at_[i];
+        rules[i].off = B.off.as<int64_t>() + off_at[i];
+        rules[i].off2 = B.off2.as<int64_t>() + off_at[i];
+    }
+    CK(upload(B.rules, rules, s));
+    const int nroots = (int)meta.size();
+    const int64_t total_rows = (int64_t)h_ids.size();
+
+    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 8;
+    int resident = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
+    if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
+    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : resident;
+    int blocks = c->sms * bps;
+    int nwarps = blocks * wpb;
+    WsLayout L = ws_layout(max_t);
+    CK(c->ws.ensure((size_t)L.total * nwarps));
+    CK(c->ctl.ensure(sizeof(Control)));
+    if (nroots > 0) {
+        CK(upload(B.meta, meta, s));
+        CK(upload(B.ids, h_ids, s));
+        if (B.pos.n < sizeof(int32_t) * (size_t)std::max<int64_t>(vtotal, 1)) {
+            CK(B.pos.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(vtotal, 1)));
+            CK(cudaMemsetAsync(B.pos.p, 0xff, B.pos.n, s));
+        }
+    }
+
+    Control ctl{};
+    float kms = 0;
+    for (int attempt = 0;; attempt++) {
+        if ((int64_t)arena_at * 2 > c->arena_bytes) c->arena_bytes = (int64_t)arena_at * 2;
+        c->stack_slots = std::max<int64_t>(c->stack_slots, (int64_t)nroots * 2);
+        CK(c->arena.ensure((size_t)c->arena_bytes));
+        CK(c->stack.ensure(sizeof(WorkItem) * (size_t)c->stack_slots));
+        CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
+        CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
+        const int64_t set_cap = std::max<int64_t>(c->result_ints / 4, 1024);
+        CK(c->starts.ensure(sizeof(unsigned long long) * (size_t)set_cap));
+        CK(cudaMemsetAsync(c->slot.p, 0, sizeof(int32_t) * (size_t)c->stack_slots, s));
+        if (nroots == 0) break;
+        CK(cudaEventRecord(c->ev[0], s));
+        CK(cudaMemsetAsync(c->arena.p, 0, arena_at, s));
+        int64_t rb = (total_rows + 255) / 256;
+        batch_root_fill_kernel<<<(unsigned)rb, 256, 0, s>>>(B.meta.as<RootMeta>(), nroots,
+                                                            B.ids.as<int32_t>(), total_rows,
+                                                            c->arena.as<char>(), B.pos.as<int32_t>());
+        batch_root_rows_kernel<<<std::max(1, blocks * 4), 256, 0, s>>>(
+            B.meta.as<RootMeta>(), nroots, B.ids.as<int32_t>(), total_rows, B.rules.as<Rules>(),
+            B.adj.as<int32_t>(), B.adj_at.as<int64_t>(), B.adj2.as<int32_t>(),
+            B.adj2_at.as<int64_t>(), c->arena.as<char>(), B.pos.as<int32_t>());
+        batch_root_unpos_kernel<<<(unsigned)rb, 256, 0, s>>>(B.meta.as<RootMeta>(), nroots,
+                                                             B.ids.as<int32_t>(), total_rows,
+                                                             B.pos.as<int32_t>());
+        CK(cudaGetLastError());
+        c->launches += 3;
+        ctl = Control{};
+        ctl.arena_top = arena_at;
+        ctl.arena_live = arena_at;
+        ctl.arena_cap = (unsigned long long)c->arena_bytes;
+        ctl.result_cap = (unsigned long long)c->result_ints;
+        ctl.set_cap = (unsigned long long)set_cap;
+        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots, INT32_MAX);
+        ctl.stack_top = nroots;
+        ctl.pending = nroots;
+        CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
+        std::vector<WorkItem> items((size_t)nroots);
+        for (int j = 0; j < nroots; j++) items[(size_t)j] = WorkItem{meta[(size_t)j].rec, -1, -1};
+        std::vector<int32_t> ones((size_t)nroots, 1);
+        CK(cudaMemcpyAsync(c->stack.p, items.data(), sizeof(WorkItem) * nroots,
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(c->slot.p, ones.data(), sizeof(int32_t) * nroots,
+                           cudaMemcpyHostToDevice, s));
+        ExpandParams P{};
+        P.rules = B.rules.as<Rules>();
+        P.nrules = count;
+        P.ctl = c->ctl.as<Control>();
+        P.arena = c->arena.as<char>();
+        P.stack = c->stack.as<WorkItem>();
+        P.slot = c->slot.as<int32_t>();
+        P.results = c->results.as<int32_t>();
+        P.set_starts = c->starts.as<unsigned long long>();
+        P.ws = c->ws.as<char>();
+        P.ws_stride = L.total;
+        P.max_t = max_t;
+        P.split = c->cfg.split > 0 ? c->cfg.split : 1;
+        P.small_path = 1;
+        P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
+        P.deadline_ns = 0;
+        if (c->cfg.time_limit_ms > 0) {
+            unsigned long long now = 0;
+            CK(read_globaltimer(s, c->ctl.as<Control>(), &now));
+            P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
+        }
+        CK(cudaEventRecord(c->ev[1], s));
+        expand_kernel<<<blocks, wpb * 32, 0, s>>>(P);
+        CK(cudaGetLastError());
+        c->launches += 1;
+        CK(cudaEventRecord(c->ev[2], s));
+        CK(cudaMemcpyAsync(&ctl, c->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
+        if (ctl.status & ST_TASK_OVERFLOW) {
+            if (ctl.arena_top > ctl.arena_cap) c->arena_bytes *= 4;
+            if (ctl.stack_top >= ctl.stack_cap) c->stack_slots *= 4;
+            if (ctl.arena_top <= ctl.arena_cap && ctl.stack_top < ctl.stack_cap) {
+                c->arena_bytes *= 2;
+                c->stack_slots *= 2;
+            }
+            if (attempt < 6) continue;
+            return fail(QC_ERR_TASK_OVERFLOW, "task arena/stack exhausted after growing");
+        }
+        if (ctl.status & ST_RESULT_OVERFLOW) {
+            c->result_ints = std::max<int64_t>({c->result_ints * 4, (int64_t)ctl.result_top * 2,
+                                                (int64_t)ctl.emitted * 8});
+            if (attempt < 6) continue;
+            return fail(QC_ERR_RESULT_OVERFLOW, "result buffer exhausted after growing");
+        }
+        if (ctl.status & ST_CHECK)
+            return fail(QC_ERR_CUDA, "device self-check failed at site " +
+                                         std::to_string(ctl.check_site) + " value " +
+                                         std::to_string(ctl.check_value));
+        if (ctl.status & ST_TOO_LARGE) return fail(QC_ERR_TOO_LARGE, "task larger than workspace");
+        if (ctl.status & ST_DEADLINE) return fail(QC_ERR_ITER_LIMIT, "time limit reached");
+        if (ctl.status & ST_ITER_LIMIT)
+            return fail(QC_ERR_ITER_LIMIT, "device wait gave up (site " +
+                                               std::to_string(ctl.wait_fail_where) + ")");
+        break;
+    }
+    double enum_ms = ms_since(t_enum);
+
+    // one filter over all instances: ids are global (vbase + id), so sets of
+    // different instances never contain one another
+    auto t_filter = clk::now();
+    std::vector<int32_t> flat;
+    int64_t nsets = 0;
+    std::string fe = filter_maximal(c->filt, c->results.as<int32_t>(), (int64_t)ctl.result_top,
+                                    c->starts.as<unsigned long long>(), (int64_t)ctl.emitted,
+                                    (int32_t)std::max<int64_t>(vtotal, 1), s, c->sms, flat, nsets,
+                                    &c->launches);
+    if (!fe.empty()) return fail(QC_ERR_CUDA, fe);
+    double filter_ms = ms_since(t_filter);
+    res.assign((size_t)count, nullptr);
+    for (int i = 0; i < count; i++) res[(size_t)i] = new qc_result();
+    std::vector<int32_t> vb(count);
+    for (int i = 0; i < count; i++) vb[i] = rules[i].vbase;
+    for (int64_t p = 0; p < (int64_t)flat.size();) {
+        int32_t k = flat[(size_t)p];
+        int32_t first = flat[(size_t)p + 1];
+        int i = (int)(std::upper_bound(vb.begin(), vb.end(), first) - vb.begin()) - 1;
+        qc_result* r = res[(size_t)i];
+        r->sets.push_back(k);
+        for (int32_t j = 0; j < k; j++) r->sets.push_back(flat[(size_t)(p + 1 + j)] - vb[i]);
+        r->nsets++;
+        p += 1 + k;
+    }
+    double total_ms = ms_since(t_all);
+    for (int i = 0; i < count; i++) {
+        qc_stats& st = res[(size_t)i]->st;
+        st.load_ms = load_ms;
+        st.enum_ms = enum_ms;
+        st.filter_ms = filter_ms;
+        st.total_ms = total_ms;
+        st.kernel_ms = kms;
+        st.tasks = (int64_t)ctl.tasks;
+        st.branches = (int64_t)ctl.branches;
+        st.children = (int64_t)ctl.children;
+        st.emitted = (int64_t)ctl.emitted;
+        st.emitted_ints = (int64_t)ctl.result_top;
+        st.maximal = res[(size_t)i]->nsets;
+        st.max_task = ctl.max_task;
+        st.arena_peak = (int64_t)ctl.arena_live_peak;
+        st.kernel_launches = c->launches;
+        st.parent_vertices = (int64_t)ctl.parent_vertices;
+        st.p_rows = (int64_t)ctl.p_rows;
+        st.child_vertices = (int64_t)ctl.child_vertices;
+    }
+    return QC_OK;
+}
+
 extern "C" qc_status qc_mine_batch(qc_context* ctx, const qc_graph* const* graphs,
                                    const double* gammas, const int32_t* min_sizes, int32_t count,
                                    qc_result** outs)
@@ -557,13 +927,21 @@ extern "C" qc_status qc_mine_batch(qc_context* ctx, const qc_graph* const* graph
         return fail(QC_ERR_ARGS, "NULL argument");
     for (int32_t i = 0; i < count; i++) outs[i] = nullptr;
     for (int32_t i = 0; i < count; i++) {
-        qc_status st = qc_mine(ctx, graphs[i], gammas[i], min_sizes[i], 0, &outs[i]);
-        if (st != QC_OK) {
-            for (int32_t j = 0; j < i; j++) qc_result_free(outs[j]);
-            for (int32_t j = 0; j < count; j++) outs[j] = nullptr;
-            return st;
-        }
+        if (!graphs[i]) return fail(QC_ERR_ARGS, "NULL graph in batch");
+        if (!(gammas[i] >= 0.5 && gammas[i] <= 1.0))
+            return fail(QC_ERR_ARGS, "minimum degree ratio must be between .5 and 1 inclusive");
+        if (min_sizes[i] <= 1) return fail(QC_ERR_ARGS, "minimum size must be greater than 1");
+        if (graphs[i]->h.off2.size() != graphs[i]->h.off.size())
+            return fail(QC_ERR_FORMAT, "graph has no 2-hop lists");
     }
+    if (count == 0) return QC_OK;
+    std::vector<qc_result*> res;
+    qc_status st = mine_batch(ctx, graphs, gammas, min_sizes, count, res);
+    if (st != QC_OK) {
+        for (auto* r : res) delete r;
+        return st;
+    }
+    for (int32_t i = 0; i < count; i++) outs[i] = res[(size_t)i];
     return QC_OK;
 }
 

@@ -27,6 +27,7 @@ __host__ __device__ inline int clz64(unsigned long long x)
 
 constexpr int kWarp = 32;
 constexpr int kArenaClasses = 4 * 40; // arena size classes (see arena_class)
+constexpr int kArenaShards = 32;       // free lists per class, selected by block
 
 // status bits written by the device
 enum : int {
@@ -35,7 +36,8 @@ enum : int {
     ST_RESULT_OVERFLOW = 2, // emitted-set buffer exhausted
     ST_ITER_LIMIT = 4,      // a bounded wait gave up
     ST_TOO_LARGE = 8,       // task larger than the workspace supports
-    ST_DEADLINE = 16        // the run's time budget ran out
+    ST_DEADLINE = 16,       // the run's time budget ran out
+    ST_CHECK = 32           // a self-check caught a bad record offset or header
 };
 
 struct Control {
@@ -56,7 +58,9 @@ struct Control {
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
     unsigned long long arena_live;      // bytes in blocks currently allocated
     unsigned long long arena_live_peak;
-    unsigned long long free_head[kArenaClasses]; // [tag:24 | offset/16:40], 0 = empty
+    unsigned long long check_site;      // first failed self-check: site id
+    unsigned long long check_value;     //   ... and the offending value
+    unsigned long long free_head[kArenaClasses * kArenaShards]; // [tag:24 | offset/16+1:40]
 };
 
 struct WorkItem {
@@ -77,7 +81,8 @@ struct TaskHdr {
     int32_t W;    // words per bit row
     int32_t refs; // work items that still reference this record
     int32_t cls;  // arena size class of the record's block
-    int32_t pad[2];
+    int32_t inst; // instance (batched runs) whose rules apply
+    int32_t pad;
 };
 
 // Arena blocks come in size classes: four steps per power of two from
@@ -111,13 +116,22 @@ __host__ __device__ inline uint64_t rec_bytes(int t, int W) {
     return rec_a2_off(t, W) + align16(4ull * t * W);
 }
 
-struct ExpandParams {
-    const int64_t* off;  // 1-hop offsets (degrees for the work counters)
-    const int64_t* off2; // 2-hop offsets
+// Per-instance rules: the gamma tables and CSR offsets of one mining
+// instance (a batched launch carries one entry per instance).
+struct Rules {
     const int32_t* md;   // md[0 .. mdlen)
     const int32_t* ubt;  // floor(d / gamma), d in [0 .. mdlen)
+    const int64_t* off;  // 1-hop offsets (degrees for the work counters)
+    const int64_t* off2; // 2-hop offsets
     int32_t mdlen;
     int32_t min_size;
+    int32_t vbase;       // added to vertex ids when sets are emitted
+    int32_t pad;
+};
+
+struct ExpandParams {
+    const Rules* rules;  // indexed by TaskHdr::inst
+    int32_t nrules;
     Control* ctl;
     char* arena;
     WorkItem* stack;

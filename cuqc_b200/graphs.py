@@ -175,7 +175,7 @@ def chung_lu_weights(n, beta, mean_degree):
         w = (idx + i0) ** (-e)
         return w[0] / w.mean() * mean_degree
 
-    lo, hi = 0.0, float(n)
+    lo, hi = 1e-9, float(n)
     if wmax_for(lo) <= cutoff:
         i0 = lo
     else:
@@ -218,3 +218,26 @@ def random_small(n, p, seed, planted=0, size=0, density=1.0):
         a, b = _plant(rng, members, density)
         ss.append(a); dd.append(b)
     return from_edges(n, np.concatenate(ss), np.concatenate(dd))
+
+
+# ---------------------------------------------------------------------------
+# multi-instance workload: independent instances of uneven size
+# ---------------------------------------------------------------------------
+
+GAMMAS_CFG3 = ("0.6", "0.7", "0.8", "0.9", "0.95")
+
+
+def batch_instance(i, base_seed=3000):
+    """Instance i of the batched workload: n log-uniform in [200, 5000],
+    Chung-Lu exponent 2.1 with mean degree uniform in [10, 50], 1-20 planted
+    groups of size 10-40 at density 0.8-1.0, gamma drawn from
+    {0.6, 0.7, 0.8, 0.9, 0.95} and min_size uniform in 5..30.
+    Returns (graph, gamma string, min_size)."""
+    rng = np.random.Generator(np.random.PCG64(base_seed + i))
+    n = int(math.floor(math.exp(rng.uniform(math.log(200), math.log(5000)))))
+    d = float(rng.uniform(10, 50))
+    k = int(rng.integers(1, 21))
+    gamma = GAMMAS_CFG3[int(rng.integers(0, len(GAMMAS_CFG3)))]
+    ms = int(rng.integers(5, 31))
+    g = chung_lu_planted(n, 2.1, d, k, (10, 40), (0.8, 1.0), seed=base_seed + 100000 + i)
+    return g, gamma, ms

@@ -67,3 +67,44 @@ def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20, small_path=
     keys = ["tasks", "branches", "children", "emitted", "lookahead_hits", "status", "max_task",
             "arena_bytes"]
     return flat, dict(zip(keys, (int(x) for x in cnt))), st
+
+
+def mine_batch(gs, gammas, min_sizes, warps=3, split=2):
+    """Emulated batched launch; returns per-instance emitted flat lists (local ids)."""
+    L = lib()
+    if not hasattr(L, "_batch_set"):
+        P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+        L.emu_mine_batch.argtypes = [C.c_int, P32, P64, P32, P64, P32, C.POINTER(C.c_double), P32,
+                                     C.c_int, C.c_int, P64, C.POINTER(P32), P64]
+        L.emu_mine_batch.restype = C.c_int
+        L._batch_set = True
+    ns = np.array([g.n for g in gs], np.int32)
+    off = np.concatenate([np.asarray(g.off, np.int64) for g in gs])
+    off2 = np.concatenate([np.asarray(g.off2, np.int64) for g in gs])
+    adj = np.concatenate([np.asarray(g.adj, np.int32) for g in gs])
+    adj2 = np.concatenate([np.asarray(g.adj2, np.int32) for g in gs])
+    gm = np.asarray(gammas, np.float64)
+    ms = np.asarray(min_sizes, np.int32)
+    ni = C.c_int64()
+    buf = C.POINTER(C.c_int32)()
+    cnt = np.zeros(3, np.int64)
+    P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+    st = L.emu_mine_batch(len(gs), ns.ctypes.data_as(P32), off.ctypes.data_as(P64),
+                          adj.ctypes.data_as(P32), off2.ctypes.data_as(P64), adj2.ctypes.data_as(P32),
+                          gm.ctypes.data_as(C.POINTER(C.c_double)), ms.ctypes.data_as(P32),
+                          int(warps), int(split), C.byref(ni), C.byref(buf), cnt.ctypes.data_as(P64))
+    flat = np.zeros(0, np.int32)
+    if ni.value:
+        flat = np.ctypeslib.as_array(buf, shape=(ni.value,)).copy()
+        L.emu_free(C.cast(buf, C.c_void_p))
+    vb = np.concatenate([[0], np.cumsum(ns)])[:-1]
+    per = [[] for _ in gs]
+    p = 0
+    while p < len(flat):
+        k = int(flat[p])
+        ids = flat[p + 1:p + 1 + k]
+        i = int(np.searchsorted(vb, ids[0], side="right") - 1)
+        per[i].append(k)
+        per[i].extend(int(x) - int(vb[i]) for x in ids)
+        p += 1 + k
+    return per, st

@@ -46,6 +46,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     h->W = W;
     h->refs = 1;
     h->cls = arena_class(rec_bytes(t, W));
+    h->inst = 0;
     int32_t* rid = (int32_t*)(arena.data() + rec_ids_off());
     uint32_t* A1 = (uint32_t*)(arena.data() + rec_a1_off(t));
     uint32_t* A2 = (uint32_t*)(arena.data() + rec_a2_off(t, W));
@@ -83,13 +84,17 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     WsLayout L = ws_layout(t);
     std::vector<char> ws((size_t)(L.total * warps));
 
+    Rules rule{};
+    rule.off = off;
+    rule.off2 = off2;
+    rule.md = md.data();
+    rule.ubt = ubt.data();
+    rule.mdlen = (int32_t)md.size();
+    rule.min_size = min_size;
+    rule.vbase = 0;
     ExpandParams P{};
-    P.off = off;
-    P.off2 = off2;
-    P.md = md.data();
-    P.ubt = ubt.data();
-    P.mdlen = (int32_t)md.size();
-    P.min_size = min_size;
+    P.rules = &rule;
+    P.nrules = 1;
     P.ctl = &ctl;
     P.arena = arena.data();
     P.stack = stack.data();
@@ -122,3 +127,112 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
 }
 
 extern "C" void emu_free(void* p) { free(p); }
+
+// Several instances in one emulated launch: graph i is given by its slices of
+// the concatenated arrays (offsets local to the instance).  Emitted ids are
+// global (instance vertex base + id).
+extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_all,
+                              const int32_t* adj_all, const int64_t* off2_all,
+                              const int32_t* adj2_all, const double* gammas,
+                              const int32_t* min_sizes, int warps, int split,
+                              int64_t* out_nints, int32_t** out_buf, int64_t* counters)
+{
+    std::vector<Rules> rules((size_t)count);
+    std::vector<std::vector<int32_t>> mds((size_t)count), ubts((size_t)count);
+    std::vector<int64_t> off_at((size_t)count), adj_at((size_t)count), adj2_at((size_t)count);
+    std::vector<char> arena((size_t)1 << 27, 0);
+    uint64_t arena_at = 0;
+    std::vector<WorkItem> items;
+    int64_t oa = 0, aa = 0, a2 = 0, vb = 0;
+    int max_t = 1;
+    for (int i = 0; i < count; i++) {
+        int n = ns[i];
+        const int64_t* off = off_all + oa;
+        const int64_t* off2 = off2_all + oa;
+        const int32_t* adj = adj_all + aa;
+        const int32_t* adj2 = adj2_all + a2;
+        HostGraph g;
+        g.n = n;
+        g.off.assign(off, off + n + 1);
+        g.adj.assign(adj, adj + off[n]);
+        g.off2.assign(off2, off2 + n + 1);
+        g.adj2.assign(adj2, adj2 + off2[n]);
+        gamma_tables(gammas[i], n, min_sizes[i], mds[(size_t)i], ubts[(size_t)i]);
+        rules[(size_t)i] = Rules{mds[(size_t)i].data(), ubts[(size_t)i].data(), off, off2,
+                                 (int32_t)mds[(size_t)i].size(), min_sizes[i], (int32_t)vb, 0};
+        std::vector<int32_t> ids;
+        int cov = 0;
+        build_root(g, mds[(size_t)i].data(), min_sizes[i], ids, cov);
+        if (!ids.empty()) {
+            int t = (int)ids.size(), W = words_for(t);
+            int cls = arena_class(rec_bytes(t, W));
+            char* rec = arena.data() + arena_at;
+            TaskHdr* h = (TaskHdr*)rec;
+            h->t = t; h->m = 0; h->cov = cov; h->W = W; h->refs = 1; h->cls = cls; h->inst = i;
+            int32_t* rid = (int32_t*)(rec + rec_ids_off());
+            uint32_t* A1 = (uint32_t*)(rec + rec_a1_off(t));
+            uint32_t* A2 = (uint32_t*)(rec + rec_a2_off(t, W));
+            std::vector<int32_t> pos((size_t)n, -1);
+            for (int k = 0; k < t; k++) { rid[k] = ids[(size_t)k]; pos[(size_t)ids[(size_t)k]] = k; }
+            for (int k = 0; k < t; k++) {
+                int u = ids[(size_t)k];
+                for (int64_t e = off[u]; e < off[u + 1]; e++) {
+                    int p = pos[(size_t)adj[e]];
+                    if (p >= 0) A1[(int64_t)k * W + (p >> 5)] |= 1u << (p & 31);
+                }
+                for (int64_t e = off2[u]; e < off2[u + 1]; e++) {
+                    int p = pos[(size_t)adj2[e]];
+                    if (p >= 0) A2[(int64_t)k * W + (p >> 5)] |= 1u << (p & 31);
+                }
+            }
+            items.push_back(WorkItem{arena_at, -1, -1});
+            arena_at += arena_class_bytes(cls);
+            max_t = std::max(max_t, t);
+        }
+        oa += n + 1;
+        aa += off[n];
+        a2 += off2[n];
+        vb += n;
+    }
+    Control ctl{};
+    ctl.arena_top = arena_at;
+    ctl.arena_live = arena_at;
+    ctl.arena_cap = arena.size();
+    ctl.result_cap = 1ull << 24;
+    ctl.set_cap = 1ull << 22;
+    ctl.stack_cap = 1 << 20;
+    ctl.stack_top = (int)items.size();
+    ctl.pending = (int)items.size();
+    std::vector<WorkItem> stack((size_t)ctl.stack_cap);
+    std::vector<int32_t> slot((size_t)ctl.stack_cap, 0);
+    for (size_t j = 0; j < items.size(); j++) { stack[j] = items[j]; slot[j] = 1; }
+    std::vector<int32_t> results((size_t)ctl.result_cap);
+    std::vector<unsigned long long> set_starts((size_t)ctl.set_cap);
+    WsLayout L = ws_layout(max_t);
+    std::vector<char> ws((size_t)(L.total * warps));
+    ExpandParams P{};
+    P.rules = rules.data();
+    P.nrules = count;
+    P.ctl = &ctl;
+    P.arena = arena.data();
+    P.stack = stack.data();
+    P.slot = slot.data();
+    P.results = results.data();
+    P.set_starts = set_starts.data();
+    P.ws = ws.data();
+    P.ws_stride = L.total;
+    P.max_t = max_t;
+    P.split = split;
+    P.small_path = 1;
+    P.wait_ns = 20000000000ll;
+    if (!items.empty()) emu_launch(1, warps * 32, [&] { expand_kernel(P); });
+    counters[0] = (int64_t)ctl.tasks;
+    counters[1] = (int64_t)ctl.branches;
+    counters[2] = ctl.status;
+    int64_t k = ctl.status ? 0 : (int64_t)ctl.result_top;
+    int32_t* out = (int32_t*)malloc(sizeof(int32_t) * (size_t)(k > 0 ? k : 1));
+    for (int64_t i = 0; i < k; i++) out[i] = results[(size_t)i];
+    *out_nints = k;
+    *out_buf = out;
+    return ctl.status;
+}

@@ -37,3 +37,18 @@ def test_emulated_kernel_matches_oracle(case, small_path):
     assert cnt["tasks"] == st["tasks"]
     assert cnt["branches"] == st["branches"]
     assert cnt["children"] == st["children"]
+
+
+def test_emulated_batch_matches_oracle_per_instance():
+    specs = [(22, 0.3, 11, 1, 7, 0.8, 4), (30, 0.25, 12, 2, 8, 0.9, 5), (18, 0.4, 13, 0, 0, 0.7, 4),
+             (26, 0.3, 14, 1, 9, 1.0, 4), (40, 0.2, 15, 1, 12, 0.85, 6)]
+    gs, gms, mss = [], [], []
+    for n, p, seed, pl, sz, gm, ms in specs:
+        gs.append(graphs.random_small(n, p, seed, planted=pl, size=sz, density=0.95))
+        gms.append(gm)
+        mss.append(ms)
+    per, st = emu.mine_batch(gs, gms, mss)
+    assert st == 0
+    for g, gm, ms, got in zip(gs, gms, mss, per):
+        want, _ = oracle.mine(g, gm, ms, "clean")
+        assert canon(got) == canon(want)

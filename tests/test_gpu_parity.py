@@ -104,3 +104,41 @@ def test_cli_matches_reference_binary_output():
     expect = open(refbin).read() if os.path.exists(refbin) else oracle.result_text(
         oracle.solve(g, float(gamma), ms, "clean")[0])
     assert got == expect
+
+
+def _batch_specs(seed0, count):
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng(seed0 + i)
+        n = int(rng.integers(12, 90))
+        g = graphs.random_small(n, float(rng.uniform(0.08, 0.4)), seed0 + i,
+                                planted=int(rng.integers(0, 4)), size=int(rng.integers(5, 15)),
+                                density=float(rng.uniform(0.85, 1.0)))
+        out.append((g, [0.7, 0.8, 0.85, 0.9, 0.95, 1.0][i % 6], int(rng.integers(3, 9))))
+    return out
+
+
+def test_batch_matches_per_instance_oracle(ctx):
+    specs = _batch_specs(500, 24)
+    res = ctx.mine_batch([s[0] for s in specs], [s[1] for s in specs], [s[2] for s in specs])
+    assert len(res) == len(specs)
+    for (g, gm, ms), r in zip(specs, res):
+        assert r.sets == oracle.solve(g, gm, ms)[0]
+
+
+def test_batch_equals_plain_calls(ctx):
+    specs = _batch_specs(700, 8)
+    batch = ctx.mine_batch([s[0] for s in specs], [s[1] for s in specs], [s[2] for s in specs])
+    for (g, gm, ms), r in zip(specs, batch):
+        assert r.sets == ctx.mine(g, gm, ms).sets
+
+
+def test_batch_with_golden_cases(ctx):
+    loaded = [load_case(c) for c in CASES]
+    res = ctx.mine_batch([x[0] for x in loaded], [float(x[2]) for x in loaded],
+                         [x[3] for x in loaded])
+    for case, (g, path, gamma, ms, _), r in zip(CASES, loaded, res):
+        refbin = os.path.join(GOLDEN, case["name"] + ".refbin.result")
+        want = open(refbin).read() if os.path.exists(refbin) else oracle.result_text(
+            oracle.solve(g, float(gamma), ms)[0])
+        assert r.text() == want, case["name"]
