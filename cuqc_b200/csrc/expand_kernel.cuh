@@ -153,6 +153,8 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
 }
 
 struct Ws {
+    WorkItem* kept;    // a child this warp runs next instead of pushing it
+    int32_t* kept_set; // 1 while kept holds an item
     int32_t* indeg;
     int32_t* exdeg;
     int32_t* aux;
@@ -170,6 +172,8 @@ __device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global)
     WsLayout L = ws_layout(P.max_t);
     char* b = P.ws + (int64_t)warp_global * P.ws_stride;
     Ws w;
+    w.kept = (WorkItem*)(b + L.kept);
+    w.kept_set = (int32_t*)(b + L.kept + sizeof(WorkItem));
     w.indeg = (int32_t*)(b + L.indeg);
     w.exdeg = (int32_t*)(b + L.exdeg);
     w.aux = (int32_t*)(b + L.aux);
@@ -594,7 +598,6 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
         }
         int top = *(volatile int*)&P.ctl->stack_top;
         if (top > 0) {
-            backoff = 64;
             if (atomicCAS(&P.ctl->stack_top, top, top - 1) == top) {
                 int idx = top - 1;
                 // a failed push (stack full) leaves stack_top above the
@@ -622,6 +625,11 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
                 atomicExch(&P.slot[idx], 0);
                 return 1;
             }
+            // lost the race for the top: wait a short, warp-dependent time so
+            // the losers do not retry in lock step
+            unsigned jitter = (unsigned)((blockIdx.x * 37u + (threadIdx.x >> 5) * 11u + spins) & 255u);
+            __nanosleep(32 + jitter);
+            spins++;
             continue;
         }
         int pend = *(volatile int*)&P.ctl->pending;
@@ -643,6 +651,21 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
 }
 
 
+
+// lane 0: hand a freshly written child to the scheduler.  The first child a
+// warp creates while it holds none is kept and run next by the same warp
+// (no trip through the shared stack); the others are pushed for any warp.
+__device__ void schedule_child(const ExpandParams& P, Ws& ws, const WorkItem& it)
+{
+    if (!*ws.kept_set) {
+        atomicAdd(&P.ctl->pending, 1);
+        *ws.kept = it;
+        *ws.kept_set = 1;
+        return;
+    }
+    push_item(P, it);
+}
+
 // ------------------------------------------------------------------
 // record arena: size classes with lock-free free lists (lane 0 only)
 // A list head packs a 24-bit tag (bumped on every change, against ABA) and
@@ -662,9 +685,19 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
         unsigned long long idx = h & kOffMask;
         if (idx == 0) break;
         unsigned long long off = (idx - 1) * 16;
+        // acquire: the block's link word must be read after the head that
+        // published it, or a stale link could be installed as the new head
+        __threadfence();
         unsigned long long next = *(volatile unsigned long long*)(P.arena + off) & kOffMask;
         unsigned long long nh = (((h >> 40) + 1) << 40) | next;
         if (atomicCAS(head, h, nh) == h) {
+            unsigned long long lim = *(volatile unsigned long long*)&P.ctl->arena_top;
+            if (off + size > lim || (next && (next - 1) * 16 + 16 > lim)) {
+                // a corrupted list: report it instead of writing through it
+                if (atomicCAS(&P.ctl->check_site, 0ull, 7ull) == 0ull) P.ctl->check_value = off;
+                set_status(P, ST_CHECK);
+                return ~0ull;
+            }
             __threadfence();
             unsigned long long live = atomicAdd(&P.ctl->arena_live, size) + size;
             atomicMax(&P.ctl->arena_live_peak, live);
@@ -838,7 +871,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
         it.rec = at;
         it.q_lo = -1;
         it.q_hi = -1;
-        push_item(P, it);
+        schedule_child(P, ws, it);
     }
     __syncwarp();
 }
@@ -1153,7 +1186,7 @@ __device__ __forceinline__ void clique_small(const ExpandParams& P, const Rules&
 }
 
 // child record of the vertices in M2 | R2, Q-sorted, matrices compacted
-__device__ void child_small(const ExpandParams& P, const Rules& R, const SmallTask& T, unsigned M2, int m2,
+__device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T, unsigned M2, int m2,
                             unsigned R2, int in, int ex)
 {
     int lane = lane_id();
@@ -1222,12 +1255,12 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, const SmallTa
         it.rec = at;
         it.q_lo = -1;
         it.q_hi = -1;
-        push_item(P, it);
+        schedule_child(P, ws, it);
     }
     __syncwarp();
 }
 
-__device__ void branch_small(const ExpandParams& P, const Rules& R, const SmallTask& T, int q)
+__device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T, int q)
 {
     int lane = lane_id();
     unsigned Mm = low_mask(T.m);
@@ -1276,11 +1309,11 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, const SmallT
     bool fail2 = prune_small(P, R, T.a1, M2, m2, C2, D2, R2, in, ex, b2);
     if (m2 >= R.min_size) clique_small(P, R, M2, m2, in, T.id);
     if (fail2) return;
-    if (R2) child_small(P, R, T, M2, m2, R2, in, ex);
+    if (R2) child_small(P, R, ws, T, M2, m2, R2, in, ex);
 }
 
 // a fresh task of at most 32 vertices, processed whole by one warp
-__device__ void process_small(const ExpandParams& P, const Rules& R, const TaskView& V)
+__device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V)
 {
     int lane = lane_id();
     SmallTask T;
@@ -1328,7 +1361,7 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, const TaskV
     if (qlo > t - 1) return;
     for (int q = t - 1; q >= qlo; q--) {
         if (*(volatile int*)&P.ctl->status) return;
-        branch_small(P, R, T, q);
+        branch_small(P, R, ws, T, q);
     }
 }
 
@@ -1348,7 +1381,7 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
     }
     int q_lo = it.q_lo, q_hi = it.q_hi;
     if (q_lo < 0 && t <= 32 && P.small_path) {
-        process_small(P, R, T);
+        process_small(P, R, ws, T);
         return;
     }
     if (q_lo < 0) {
@@ -1497,11 +1530,19 @@ __global__ void expand_kernel(ExpandParams P)
     int lane = lane_id();
     int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     Ws ws = ws_view(P, warp_global);
+    if (lane == 0) *ws.kept_set = 0;
+    __syncwarp();
     for (;;) {
         WorkItem it;
         int r = 0;
         if (lane == 0) {
-            r = pop_item(P, it);
+            if (*ws.kept_set) {
+                it = *ws.kept;
+                *ws.kept_set = 0;
+                r = *(volatile int*)&P.ctl->status ? -1 : 1;
+            } else {
+                r = pop_item(P, it);
+            }
             if (r > 0 && !item_ok(P, it)) r = -1;
         }
         r = __shfl_sync(QC_FULL, r, 0);

@@ -149,7 +149,7 @@ struct ExpandParams {
 
 // Per-warp workspace layout for tasks of up to max_t vertices.
 struct WsLayout {
-    int64_t indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
+    int64_t kept, indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
     int64_t total;
 };
 
@@ -162,6 +162,7 @@ __host__ __device__ inline WsLayout ws_layout(int max_t)
     tp += 64;
     int64_t W = words_for(max_t) + 2;
     int64_t o = 0;
+    L.kept = o;     o += 32;
     L.indeg = o;    o += align16(4 * t);
     L.exdeg = o;    o += align16(4 * t);
     L.aux = o;      o += align16(4 * t);
