@@ -51,6 +51,10 @@ WORKLOADS = {
                          density_range=(0.85, 1.0), seed=2),
                  gamma="0.8", min_size=15),
 }
+# Batched workload: independent instances of uneven size (graphs.batch_instance)
+BATCH_WORKLOADS = {"cfg3": dict(desc="independent instances: n log-uniform 200-5000, Chung-Lu "
+                                     "mean deg 10-50 + 1-20 planted groups 10-40 @0.8-1.0, "
+                                     "gamma in {0.6,0.7,0.8,0.9,0.95}, min_size 5-30")}
 DEFAULT_WORKLOAD = "cfg1"
 L2_FLUSH_BYTES = 256 << 20
 
@@ -193,6 +197,62 @@ def run_reference(args):
 # our arm
 # ---------------------------------------------------------------------------
 
+def run_batch(args):
+    """Batched vs plain on the multi-instance workload: one persistent launch
+    for all instances against one launch per instance."""
+    import torch
+
+    import cuqc_b200 as Q
+
+    n_inst = args.instances
+    inst = [graphs.batch_instance(i) for i in range(n_inst)]
+    gs = [x[0] for x in inst]
+    gms = [float(x[1]) for x in inst]
+    mss = [x[2] for x in inst]
+    ctx = Q.Context(device=0)
+    dgs = [Q.DeviceGraph.from_graph(g) for g in gs]
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        ref = ctx.mine_batch(dgs, gms, mss)
+    batched_ms, plain_ms = [], []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            res, ms = timed(lambda: ctx.mine_batch(dgs, gms, mss))
+            assert [r.sets for r in res] == [r.sets for r in ref]
+            batched_ms.append(ms)
+        for _ in range(max(1, args.steps // 2)):
+            res, ms = timed(lambda: [ctx.mine(d, gm, m) for d, gm, m in zip(dgs, gms, mss)])
+            assert [r.sets for r in res] == [r.sets for r in ref]
+            plain_ms.append(ms)
+    b = statistics.median(batched_ms)
+    p = statistics.median(plain_ms)
+    line = {
+        "metric": "instances/s (batched: all instances in one persistent launch)",
+        "value": n_inst / (b / 1000.0), "unit": "instances/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": b,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator: %s)" % BATCH_WORKLOADS["cfg3"]["desc"],
+        "config": {"workload": "cfg3", "instances": n_inst, "l2": "inputs resident; no flush",
+                   "parallelism": "one persistent launch"},
+        "plain": {"value": n_inst / (p / 1000.0), "unit": "instances/s", "ms_per_step": p,
+                  "form": "one qc_mine launch per instance"},
+        "batched_over_plain": p / b,
+        "maximal_total": sum(len(r.sets) for r in ref),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+    ctx.close()
+
+
 def run_ours(args):
     import torch
 
@@ -329,12 +389,16 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-instances", type=int, default=8)
+    ap.add_argument("--instances", type=int, default=256, help="batched workload size")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in BATCH_WORKLOADS:
+        run_batch(args)
     else:
         run_ours(args)
 

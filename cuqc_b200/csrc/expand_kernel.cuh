@@ -494,6 +494,14 @@ __device__ __forceinline__ void set_status(const ExpandParams& P, int bits)
     atomicOr(&P.ctl->status, bits);
 }
 
+// record the first failed self-check (site, value) and stop the run
+__device__ __forceinline__ void check_fail(const ExpandParams& P, unsigned long long site,
+                                           unsigned long long value)
+{
+    if (atomicCAS(&P.ctl->check_site, 0ull, site) == 0ull) P.ctl->check_value = value;
+    set_status(P, ST_CHECK);
+}
+
 // write the ids of the vertices in mask `mm` (count k) as one set
 __device__ void emit_mask(const ExpandParams& P, const Rules& R, const TaskView& T, const uint32_t* mm, int k)
 {
@@ -692,6 +700,12 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
         unsigned long long nh = (((h >> 40) + 1) << 40) | next;
         if (atomicCAS(head, h, nh) == h) {
             unsigned long long lim = *(volatile unsigned long long*)&P.ctl->arena_top;
+            int mark = ((volatile TaskHdr*)(P.arena + off))->refs;
+            if (mark != kFreeMagic) {
+                check_fail(P, 9, off); // handed out a block that is not free
+                return ~0ull;
+            }
+            ((volatile TaskHdr*)(P.arena + off))->refs = 0;
             if (off + size > lim || (next && (next - 1) * 16 + 16 > lim)) {
                 // a corrupted list: report it instead of writing through it
                 if (atomicCAS(&P.ctl->check_site, 0ull, 7ull) == 0ull) P.ctl->check_value = off;
@@ -721,6 +735,7 @@ __device__ void arena_free(const ExpandParams& P, unsigned long long off, int cl
     for (int tries = 0; tries < (1 << 20); tries++) {
         unsigned long long h = *(volatile unsigned long long*)head;
         *(volatile unsigned long long*)(P.arena + off) = h & kOffMask;
+        ((volatile TaskHdr*)(P.arena + off))->refs = kFreeMagic;
         __threadfence();
         unsigned long long nh = (((h >> 40) + 1) << 40) | (off / 16 + 1);
         if (atomicCAS(head, h, nh) == h) {
@@ -737,7 +752,9 @@ __device__ void release_record(const ExpandParams& P, unsigned long long rec)
     TaskHdr* h = (TaskHdr*)(P.arena + rec);
     int cls = *(volatile int32_t*)&h->cls;
     __threadfence();
-    if (atomicSub(&h->refs, 1) == 1) arena_free(P, rec, cls);
+    int before = atomicSub(&h->refs, 1);
+    if (before == 1) arena_free(P, rec, cls);
+    else if (before < 1 || before == kFreeMagic) check_fail(P, 10, rec); // released too often
 }
 
 // ------------------------------------------------------------------
@@ -1375,6 +1392,17 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
     const Rules R = P.rules[T.inst];
+    {
+        int bad = 0;
+        for (int v = lane; v < t; v += 32) {
+            int id = T.ids[v];
+            if (id < 0 || id >= R.n) bad = 1;
+        }
+        if (__any_sync(QC_FULL, bad)) {
+            if (lane == 0) check_fail(P, 8, it.rec);
+            return;
+        }
+    }
     if (t > P.max_t) {
         if (lane == 0) set_status(P, ST_TOO_LARGE);
         return;
@@ -1481,6 +1509,10 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
     }
     for (int q = q_hi; q >= q_lo; q--) {
         if (*(volatile int*)&P.ctl->status) return;
+        if (P.deadline_ns && now_ns() > P.deadline_ns) {
+            if (lane == 0) set_status(P, ST_DEADLINE);
+            return;
+        }
         expand_branch(P, R, T, ws, q);
     }
 }

@@ -347,14 +347,17 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     CK(upload(c->ubt, ubt, s));
     CK(upload(c->ids, ids, s));
 
-    // expand_kernel is compiled with __launch_bounds__(256, 2): at most 8 warps a block
-    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 8;
+    // expand_kernel is compiled with __launch_bounds__(256, 2): at most 8 warps a
+    // block.  The search tree offers limited parallelism and every idle warp
+    // polls the shared stack, so the default is one block of 4 warps per SM.
+    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
     int resident = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
     if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
     // a persistent launch: never more blocks than can be resident at once
-    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : resident;
+    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : 1;
     int blocks = c->sms * bps;
+    if (c->cfg.max_blocks > 0) blocks = std::min(blocks, c->cfg.max_blocks);
     int nwarps = blocks * wpb;
     WsLayout L = ws_layout(t);
     CK(c->ws.ensure((size_t)L.total * nwarps));
@@ -426,6 +429,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         rule.mdlen = (int32_t)md.size();
         rule.min_size = min_size;
         rule.vbase = 0;
+        rule.n = h.n;
         CK(c->rules.ensure(sizeof(Rules)));
         CK(cudaMemcpyAsync(c->rules.p, &rule, sizeof(rule), cudaMemcpyHostToDevice, s));
         ExpandParams P{};
@@ -696,6 +700,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         adj2_at[i] = (int64_t)h_adj2.size();
         h_adj2.insert(h_adj2.end(), h.adj2.begin(), h.adj2.end());
         rules[i].vbase = (int32_t)vtotal;
+        rules[i].n = h.n;
         vtotal += h.n;
     }
     if (vtotal > INT32_MAX) return fail(QC_ERR_TOO_LARGE, "batch has more than 2^31 vertices");
@@ -748,12 +753,13 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     const int nroots = (int)meta.size();
     const int64_t total_rows = (int64_t)h_ids.size();
 
-    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 8;
+    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
     int resident = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
     if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
-    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : resident;
+    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : 1;
     int blocks = c->sms * bps;
+    if (c->cfg.max_blocks > 0) blocks = std::min(blocks, c->cfg.max_blocks);
     int nwarps = blocks * wpb;
     WsLayout L = ws_layout(max_t);
     CK(c->ws.ensure((size_t)L.total * nwarps));

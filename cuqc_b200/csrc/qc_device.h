@@ -126,8 +126,10 @@ struct Rules {
     int32_t mdlen;
     int32_t min_size;
     int32_t vbase;       // added to vertex ids when sets are emitted
-    int32_t pad;
+    int32_t n;           // vertices of the instance (ids must be below it)
 };
+
+constexpr int32_t kFreeMagic = 0x7ee7f00d; // refs of a block on a free list
 
 struct ExpandParams {
     const Rules* rules;  // indexed by TaskHdr::inst

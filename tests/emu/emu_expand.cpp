@@ -14,6 +14,15 @@
 
 using namespace qcb;
 
+// optional stop time for the next emulated launches (0: none), to exercise the
+// kernel's deadline drain
+static long long g_emu_time_limit_ms = 0;
+extern "C" void emu_set_time_limit_ms(long long ms) { g_emu_time_limit_ms = ms; }
+static unsigned long long emu_deadline()
+{
+    return g_emu_time_limit_ms > 0 ? emu_globaltimer() + (unsigned long long)g_emu_time_limit_ms * 1000000ull : 0ull;
+}
+
 extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
                         const int32_t* adj2, double gamma, int min_size, int warps, int split,
                         int small_path,
@@ -92,6 +101,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     rule.mdlen = (int32_t)md.size();
     rule.min_size = min_size;
     rule.vbase = 0;
+    rule.n = n;
     ExpandParams P{};
     P.rules = &rule;
     P.nrules = 1;
@@ -107,6 +117,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     P.split = split;
     P.small_path = small_path;
     P.wait_ns = 20000000000ll;
+    P.deadline_ns = emu_deadline();
     emu_launch(1, warps * 32, [&] { expand_kernel(P); });
 
     counters[0] = (int64_t)ctl.tasks;
@@ -159,7 +170,7 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
         g.adj2.assign(adj2, adj2 + off2[n]);
         gamma_tables(gammas[i], n, min_sizes[i], mds[(size_t)i], ubts[(size_t)i]);
         rules[(size_t)i] = Rules{mds[(size_t)i].data(), ubts[(size_t)i].data(), off, off2,
-                                 (int32_t)mds[(size_t)i].size(), min_sizes[i], (int32_t)vb, 0};
+                                 (int32_t)mds[(size_t)i].size(), min_sizes[i], (int32_t)vb, n};
         std::vector<int32_t> ids;
         int cov = 0;
         build_root(g, mds[(size_t)i].data(), min_sizes[i], ids, cov);
@@ -225,6 +236,7 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     P.split = split;
     P.small_path = 1;
     P.wait_ns = 20000000000ll;
+    P.deadline_ns = emu_deadline();
     if (!items.empty()) emu_launch(1, warps * 32, [&] { expand_kernel(P); });
     counters[0] = (int64_t)ctl.tasks;
     counters[1] = (int64_t)ctl.branches;
