@@ -77,10 +77,19 @@ __device__ __forceinline__ long long wscan64(long long x)
 
 __device__ __forceinline__ bool bit(const uint32_t* a, int v) { return (a[v >> 5] >> (v & 31)) & 1u; }
 
+// Task records are written by one SM and read by another after a hand-off
+// through the work stack, and their blocks are recycled; every read of record
+// content goes through L2 (ld.global.cg) so no SM can see a stale L1 copy of a
+// block's previous contents.
+__device__ __forceinline__ uint32_t rec_ld(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ int32_t rec_ld(const int32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ bool rec_bit(const uint32_t* a, int v) { return (rec_ld(a + (v >> 5)) >> (v & 31)) & 1u; }
+
+// |record row & mask| over W words (row in a task record, mask in the workspace)
 __device__ __forceinline__ int popc_and(const uint32_t* row, const uint32_t* mask, int W)
 {
     int s = 0;
-    for (int w = 0; w < W; w++) s += __popc(row[w] & mask[w]);
+    for (int w = 0; w < W; w++) s += __popc(rec_ld(row + w) & mask[w]);
     return s;
 }
 
@@ -135,15 +144,16 @@ struct TaskView {
     unsigned long long rec;
 };
 
-__device__ __forceinline__ TaskView task_view(char* arena, unsigned long long rec)
+// view of a record whose header fields were read once (through L2) and
+// validated when the work item was dequeued
+__device__ __forceinline__ TaskView task_view(char* arena, unsigned long long rec, const TaskHdr& h)
 {
     TaskView T;
-    const TaskHdr* h = (const TaskHdr*)(arena + rec);
-    T.t = h->t;
-    T.m = h->m;
-    T.cov = h->cov;
-    T.W = h->W;
-    T.inst = h->inst;
+    T.t = h.t;
+    T.m = h.m;
+    T.cov = h.cov;
+    T.W = h.W;
+    T.inst = h.inst;
     T.ids = (const int32_t*)(arena + rec + rec_ids_off());
     T.l2 = (int32_t*)(arena + rec + rec_l2_off(T.t));
     T.A1 = (const uint32_t*)(arena + rec + rec_a1_off(T.t));
@@ -264,7 +274,7 @@ __device__ int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const u
         if (v < t && bit(cm, v)) {
             int in = ws.indeg[v];
             if (!filter_valid || cand_valid(R, in, ws.exdeg[v], m, b)) {
-                int j = vmax - (in > vmax ? vmax : in);
+                int j = vmax - (in > vmax ? vmax : (in < 0 ? 0 : in));
                 atomicAdd(&ws.hist[j], 1);
                 cnt++;
             }
@@ -528,7 +538,7 @@ __device__ void emit_mask(const ExpandParams& P, const Rules& R, const TaskView&
         unsigned bal = __ballot_sync(QC_FULL, in);
         if (in) {
             int r = __popc(bal & ((1u << lane) - 1u));
-            P.results[at + 1 + written + r] = T.ids[v] + R.vbase;
+            P.results[at + 1 + written + r] = rec_ld(T.ids + v) + R.vbase;
         }
         written += __popc(bal);
     }
@@ -686,6 +696,10 @@ constexpr unsigned long long kOffMask = (1ull << 40) - 1;
 __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long long bytes, int& cls)
 {
     cls = arena_class(bytes);
+    if (cls >= kArenaClasses) {
+        set_status(P, ST_TOO_LARGE);
+        return ~0ull;
+    }
     unsigned long long size = arena_class_bytes(cls);
     unsigned long long* head = &P.ctl->free_head[cls * kArenaShards + (blockIdx.x % kArenaShards)];
     for (int tries = 0; tries < 256; tries++) {
@@ -693,6 +707,14 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
         unsigned long long idx = h & kOffMask;
         if (idx == 0) break;
         unsigned long long off = (idx - 1) * 16;
+        {
+            unsigned long long lim0 = *(volatile unsigned long long*)&P.ctl->arena_top;
+            if (lim0 > P.ctl->arena_cap) lim0 = P.ctl->arena_cap;
+            if (off + size > lim0) {
+                check_fail(P, 12, off); // a list head outside the arena: never read through it
+                return ~0ull;
+            }
+        }
         // acquire: the block's link word must be read after the head that
         // published it, or a stale link could be installed as the new head
         __threadfence();
@@ -700,18 +722,17 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
         unsigned long long nh = (((h >> 40) + 1) << 40) | next;
         if (atomicCAS(head, h, nh) == h) {
             unsigned long long lim = *(volatile unsigned long long*)&P.ctl->arena_top;
+            if (lim > P.ctl->arena_cap) lim = P.ctl->arena_cap;
+            if ((off & 15ull) != 0 || off + size > lim || (next && (next - 1) * 16 + 16 > lim)) {
+                check_fail(P, 7, off); // a corrupted list: report it, never write through it
+                return ~0ull;
+            }
             int mark = ((volatile TaskHdr*)(P.arena + off))->refs;
             if (mark != kFreeMagic) {
                 check_fail(P, 9, off); // handed out a block that is not free
                 return ~0ull;
             }
             ((volatile TaskHdr*)(P.arena + off))->refs = 0;
-            if (off + size > lim || (next && (next - 1) * 16 + 16 > lim)) {
-                // a corrupted list: report it instead of writing through it
-                if (atomicCAS(&P.ctl->check_site, 0ull, 7ull) == 0ull) P.ctl->check_value = off;
-                set_status(P, ST_CHECK);
-                return ~0ull;
-            }
             __threadfence();
             unsigned long long live = atomicAdd(&P.ctl->arena_live, size) + size;
             atomicMax(&P.ctl->arena_live_peak, live);
@@ -751,6 +772,10 @@ __device__ void release_record(const ExpandParams& P, unsigned long long rec)
 {
     TaskHdr* h = (TaskHdr*)(P.arena + rec);
     int cls = *(volatile int32_t*)&h->cls;
+    if (cls < 0 || cls >= kArenaClasses) {
+        check_fail(P, 11, rec); // a header whose size class is out of range
+        return;
+    }
     __threadfence();
     int before = atomicSub(&h->refs, 1);
     if (before == 1) arena_free(P, rec, cls);
@@ -823,9 +848,9 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
             unsigned long long cls = isM ? 0ull : 1ull;
             unsigned long long in_k = 0xffffull - (unsigned long long)ws.indeg[v];
             unsigned long long ex_k = 0xffffull - (unsigned long long)ws.exdeg[v];
-            unsigned long long l2_k = 0xffffull - (unsigned long long)T.l2[v];
+            unsigned long long l2_k = 0xffffull - (unsigned long long)rec_ld(T.l2 + v);
             ws.khi[r] = (cls << 48) | (in_k << 32) | (ex_k << 16) | l2_k;
-            ws.klo[r] = 0xffffffffull - (unsigned long long)(unsigned)T.ids[v];
+            ws.klo[r] = 0xffffffffull - (unsigned long long)(unsigned)rec_ld(T.ids + v);
             ws.sel[r] = v;
         }
         written += __popc(bal);
@@ -855,7 +880,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     uint32_t* c1 = (uint32_t*)(rec + rec_a1_off(tc));
     uint32_t* c2 = (uint32_t*)(rec + rec_a2_off(tc, Wc));
     for (int i = lane; i < tc; i += 32) {
-        cid[i] = T.ids[ws.sel[i]];
+        cid[i] = rec_ld(T.ids + ws.sel[i]);
         cl2[i] = 0;
     }
     // compacted rows: child bit j of row i = parent bit sel[j] of row sel[i]
@@ -867,8 +892,8 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
             bool b1 = false, b2 = false;
             if (j < tc) {
                 int pj = ws.sel[j];
-                b1 = bit(r1, pj);
-                b2 = bit(r2, pj);
+                b1 = rec_bit(r1, pj);
+                b2 = rec_bit(r2, pj);
             }
             unsigned w1 = __ballot_sync(QC_FULL, b1);
             unsigned w2 = __ballot_sync(QC_FULL, b2);
@@ -907,7 +932,6 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     uint32_t* Rm = ws.mk[MK_R];
     uint32_t* CA = ws.mk[MK_CA];
     uint32_t* Kc = ws.mk[MK_K];
-    uint32_t* who = ws.mk[MK_U];
 
     // members M u {q}; candidates before q
     bs_range(M, W, 0, T.m);
@@ -926,14 +950,15 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     }
     // diameter pruning (main.cu:1709-1732): PRE & N2(q)
     const uint32_t* r2q = T.A2 + (int64_t)q * W;
-    for (int w = lane; w < W; w += 32) D[w] = PRE[w] & r2q[w];
+    for (int w = lane; w < W; w += 32) D[w] = PRE[w] & rec_ld(r2q + w);
     __syncwarp();
     if (lane == 0) {
         atomicAdd(&P.ctl->branches, 1ull);
         atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
-        int pid = T.ids[q];
-        atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
-                                                       (R.off2[pid + 1] - R.off2[pid])));
+        int pid = rec_ld(T.ids + q);
+        if (pid >= 0 && pid < R.n)
+            atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
+                                                           (R.off2[pid + 1] - R.off2[pid])));
     }
 
     Bounds b = {0, 0, 0};
@@ -960,7 +985,7 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
             while (kw) {
                 int v = base + __ffs(kw) - 1;
                 kw &= kw - 1;
-                acc |= T.A1[(int64_t)v * W + w];
+                acc |= rec_ld(T.A1 + (int64_t)v * W + w);
             }
         }
         CA[w] = acc & Rm[w];
@@ -1005,7 +1030,6 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
         bs_copy(C2, Rm, W);
         bs_copy(D2, Rm, W);
     }
-    (void)who;
     uint32_t* R2 = ws.mk[MK_R];
     Bounds b2 = {0, 0, 0};
     bool fail2 = degree_prune(P, R, T, ws, M, m2, C2, D2, R2, b2);
@@ -1292,7 +1316,7 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
         atomicAdd(&P.ctl->branches, 1ull);
         atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
     }
-    if (lane == q) {
+    if (lane == q && T.id >= 0 && T.id < R.n) {
         atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[T.id + 1] - R.off[T.id]) +
                                                        (R.off2[T.id + 1] - R.off2[T.id])));
     }
@@ -1339,10 +1363,10 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     T.cov = V.cov;
     T.inst = V.inst;
     bool act = lane < T.t;
-    T.id = act ? V.ids[lane] : -1;
-    T.a1 = act ? V.A1[lane] : 0u;
-    T.a2 = act ? V.A2[lane] : 0u;
-    T.l2 = act ? V.l2[lane] : 0;
+    T.id = act ? rec_ld(V.ids + lane) : -1;
+    T.a1 = act ? rec_ld(V.A1 + lane) : 0u;
+    T.a2 = act ? rec_ld(V.A2 + lane) : 0u;
+    T.l2 = act ? rec_ld(V.l2 + lane) : 0;
     const int t = T.t, m = T.m;
     unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
     int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
@@ -1386,16 +1410,16 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
 // a work item: fresh task (lookahead, branch range) or a branch range
 // ------------------------------------------------------------------
 
-__device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
+__device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, const TaskHdr& hv)
 {
-    TaskView T = task_view(P.arena, it.rec);
+    TaskView T = task_view(P.arena, it.rec, hv);
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
     const Rules R = P.rules[T.inst];
     {
         int bad = 0;
         for (int v = lane; v < t; v += 32) {
-            int id = T.ids[v];
+            int id = rec_ld(T.ids + v);
             if (id < 0 || id >= R.n) bad = 1;
         }
         if (__any_sync(QC_FULL, bad)) {
@@ -1522,7 +1546,9 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it)
 // offset must be 16-byte aligned and inside the written arena, and the
 // header must describe a record that fits there.  A failure records the
 // site and value and the item is skipped instead of being dereferenced.
-__device__ bool item_ok(const ExpandParams& P, const WorkItem& it)
+// The header is read once, through L2, into `hv`; the warp uses only those
+// validated values.
+__device__ bool item_ok(const ExpandParams& P, const WorkItem& it, TaskHdr& hv)
 {
     unsigned long long top = *(volatile unsigned long long*)&P.ctl->arena_top;
     unsigned long long cap = P.ctl->arena_cap;
@@ -1532,8 +1558,13 @@ __device__ bool item_ok(const ExpandParams& P, const WorkItem& it)
     else if (it.rec + sizeof(TaskHdr) > lim) site = 2;
     else {
         const volatile TaskHdr* h = (const volatile TaskHdr*)(P.arena + it.rec);
-        int t = h->t, W = h->W, m = h->m, inst = h->inst;
-        if (t < 1 || t > P.max_t || W != words_for(t) || m < 0 || m > t) {
+        int t = h->t, W = h->W, m = h->m, inst = h->inst, cov = h->cov;
+        hv.t = t;
+        hv.W = W;
+        hv.m = m;
+        hv.inst = inst;
+        hv.cov = cov;
+        if (t < 1 || t > P.max_t || W != words_for(t) || m < 0 || m > t || cov < 0 || m + cov > t) {
             site = 3;
             val = ((unsigned long long)(unsigned)t << 32) | (unsigned)W;
         } else if (it.rec + rec_bytes(t, W) > lim) site = 4;
@@ -1566,6 +1597,7 @@ __global__ void expand_kernel(ExpandParams P)
     __syncwarp();
     for (;;) {
         WorkItem it;
+        TaskHdr hv{};
         int r = 0;
         if (lane == 0) {
             if (*ws.kept_set) {
@@ -1575,15 +1607,20 @@ __global__ void expand_kernel(ExpandParams P)
             } else {
                 r = pop_item(P, it);
             }
-            if (r > 0 && !item_ok(P, it)) r = -1;
+            if (r > 0 && !item_ok(P, it, hv)) r = -1;
         }
         r = __shfl_sync(QC_FULL, r, 0);
         if (r <= 0) break;
         it.rec = __shfl_sync(QC_FULL, it.rec, 0);
         it.q_lo = __shfl_sync(QC_FULL, it.q_lo, 0);
         it.q_hi = __shfl_sync(QC_FULL, it.q_hi, 0);
+        hv.t = __shfl_sync(QC_FULL, hv.t, 0);
+        hv.m = __shfl_sync(QC_FULL, hv.m, 0);
+        hv.cov = __shfl_sync(QC_FULL, hv.cov, 0);
+        hv.W = __shfl_sync(QC_FULL, hv.W, 0);
+        hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
         __threadfence();
-        process_item(P, ws, it);
+        process_item(P, ws, it, hv);
         __syncwarp();
         __threadfence();
         if (lane == 0) {

@@ -85,6 +85,7 @@ inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0
 inline int __all_sync(unsigned m, int pred) { return __ballot_sync(m, pred) == 0xffffffffu; }
 inline void __syncwarp(unsigned = 0xffffffffu) { emu_w->bar.arrive_and_wait(); }
 inline int __popc(unsigned x) { return __builtin_popcount(x); }
+template <class T> inline T __ldcg(const T* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
 inline int __ffs(unsigned x) { return x ? __builtin_ctz(x) + 1 : 0; }
 inline int __clz(unsigned x) { return x ? __builtin_clz(x) : 32; }
