@@ -165,6 +165,9 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
 struct Ws {
     WorkItem* kept;    // a child this warp runs next instead of pushing it
     int32_t* kept_set; // 1 while kept holds an item
+    WarpCount* cnt;    // this warp's work counters (lane 0)
+    unsigned long long* fhead; // private free list per size class: offset/16+1, 0 = empty
+    int32_t* fcount;           // blocks on each private list
     int32_t* indeg;
     int32_t* exdeg;
     int32_t* aux;
@@ -184,6 +187,9 @@ __device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global)
     Ws w;
     w.kept = (WorkItem*)(b + L.kept);
     w.kept_set = (int32_t*)(b + L.kept + sizeof(WorkItem));
+    w.cnt = (WarpCount*)(b + L.count);
+    w.fhead = (unsigned long long*)(b + L.freel);
+    w.fcount = (int32_t*)(b + L.freel + 8 * (int64_t)kArenaClasses);
     w.indeg = (int32_t*)(b + L.indeg);
     w.exdeg = (int32_t*)(b + L.exdeg);
     w.aux = (int32_t*)(b + L.aux);
@@ -525,7 +531,6 @@ __device__ void emit_mask(const ExpandParams& P, const Rules& R, const TaskView&
             at = ~0ull;
         } else {
             P.set_starts[idx] = at;
-            atomicAdd(&P.ctl->emitted_ints, (unsigned long long)(k + 1));
         }
     }
     at = __shfl_sync(QC_FULL, at, 0);
@@ -673,10 +678,11 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
 // lane 0: hand a freshly written child to the scheduler.  The first child a
 // warp creates while it holds none is kept and run next by the same warp
 // (no trip through the shared stack); the others are pushed for any warp.
+// A kept child takes over the outstanding-work count of the item that made
+// it (the warp does not decrement `pending` when it finishes that item).
 __device__ void schedule_child(const ExpandParams& P, Ws& ws, const WorkItem& it)
 {
     if (!*ws.kept_set) {
-        atomicAdd(&P.ctl->pending, 1);
         *ws.kept = it;
         *ws.kept_set = 1;
         return;
@@ -693,7 +699,7 @@ __device__ void schedule_child(const ExpandParams& P, Ws& ws, const WorkItem& it
 
 constexpr unsigned long long kOffMask = (1ull << 40) - 1;
 
-__device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long long bytes, int& cls)
+__device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigned long long bytes, int& cls)
 {
     cls = arena_class(bytes);
     if (cls >= kArenaClasses) {
@@ -701,6 +707,24 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
         return ~0ull;
     }
     unsigned long long size = arena_class_bytes(cls);
+    // this warp's own free list: blocks it freed itself, no other warp touches it
+    if (ws.fcount[cls] > 0) {
+        unsigned long long off = (ws.fhead[cls] - 1) * 16;
+        unsigned long long lim = *(volatile unsigned long long*)&P.ctl->arena_top;
+        if (lim > P.ctl->arena_cap) lim = P.ctl->arena_cap;
+        if (ws.fhead[cls] == 0 || off + size > lim) {
+            check_fail(P, 13, off); // a private list that points outside the arena
+            return ~0ull;
+        }
+        if (((TaskHdr*)(P.arena + off))->refs != kFreeMagic) {
+            check_fail(P, 15, off); // a private-list block that is not free
+            return ~0ull;
+        }
+        ws.fhead[cls] = *(unsigned long long*)(P.arena + off) & kOffMask;
+        ws.fcount[cls]--;
+        ((TaskHdr*)(P.arena + off))->refs = 0;
+        return off;
+    }
     unsigned long long* head = &P.ctl->free_head[cls * kArenaShards + (blockIdx.x % kArenaShards)];
     for (int tries = 0; tries < 256; tries++) {
         unsigned long long h = *(volatile unsigned long long*)head;
@@ -734,8 +758,6 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
             }
             ((volatile TaskHdr*)(P.arena + off))->refs = 0;
             __threadfence();
-            unsigned long long live = atomicAdd(&P.ctl->arena_live, size) + size;
-            atomicMax(&P.ctl->arena_live_peak, live);
             return off;
         }
     }
@@ -744,14 +766,21 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, unsigned long l
         set_status(P, ST_TASK_OVERFLOW);
         return ~0ull;
     }
-    unsigned long long live = atomicAdd(&P.ctl->arena_live, size) + size;
-    atomicMax(&P.ctl->arena_live_peak, live);
     return at;
 }
 
-__device__ void arena_free(const ExpandParams& P, unsigned long long off, int cls)
+// lane 0: return a block.  It goes to this warp's private list (reused by the
+// warp's next allocation of the class, without atomics) until that list holds
+// kPrivateFreeCap blocks; beyond that, to the shared lock-free list.
+__device__ void arena_free(const ExpandParams& P, Ws& ws, unsigned long long off, int cls)
 {
-    unsigned long long size = arena_class_bytes(cls);
+    if (ws.fcount[cls] < kPrivateFreeCap) {
+        *(unsigned long long*)(P.arena + off) = ws.fhead[cls];
+        ((TaskHdr*)(P.arena + off))->refs = kFreeMagic;
+        ws.fhead[cls] = off / 16 + 1;
+        ws.fcount[cls]++;
+        return;
+    }
     unsigned long long* head = &P.ctl->free_head[cls * kArenaShards + (blockIdx.x % kArenaShards)];
     for (int tries = 0; tries < (1 << 20); tries++) {
         unsigned long long h = *(volatile unsigned long long*)head;
@@ -759,16 +788,15 @@ __device__ void arena_free(const ExpandParams& P, unsigned long long off, int cl
         ((volatile TaskHdr*)(P.arena + off))->refs = kFreeMagic;
         __threadfence();
         unsigned long long nh = (((h >> 40) + 1) << 40) | (off / 16 + 1);
-        if (atomicCAS(head, h, nh) == h) {
-            atomicAdd(&P.ctl->arena_live, 0ull - size);
-            return;
-        }
+        if (atomicCAS(head, h, nh) == h) return;
     }
     // contention beyond any plausible bound: keep the block (a leak, not a fault)
 }
 
-// a work item on this record is finished; the last one frees the block
-__device__ void release_record(const ExpandParams& P, unsigned long long rec)
+// a work item on this record is finished; the last one frees the block.
+// `sole`: no other work item ever referenced the record (a task processed
+// whole by one warp), so the reference count needs no atomic.
+__device__ void release_record(const ExpandParams& P, Ws& ws, unsigned long long rec, bool sole)
 {
     TaskHdr* h = (TaskHdr*)(P.arena + rec);
     int cls = *(volatile int32_t*)&h->cls;
@@ -776,9 +804,18 @@ __device__ void release_record(const ExpandParams& P, unsigned long long rec)
         check_fail(P, 11, rec); // a header whose size class is out of range
         return;
     }
+    if (sole) {
+        int before = *(volatile int32_t*)&h->refs;
+        if (before != 1) {
+            check_fail(P, 14, rec); // a record thought to be private has other users
+            return;
+        }
+        arena_free(P, ws, rec, cls);
+        return;
+    }
     __threadfence();
     int before = atomicSub(&h->refs, 1);
-    if (before == 1) arena_free(P, rec, cls);
+    if (before == 1) arena_free(P, ws, rec, cls);
     else if (before < 1 || before == kFreeMagic) check_fail(P, 10, rec); // released too often
 }
 
@@ -861,7 +898,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     unsigned long long bytes = rec_bytes(tc, Wc);
     unsigned long long at = 0;
     int cls = 0;
-    if (lane == 0) at = arena_alloc(P, bytes, cls);
+    if (lane == 0) at = arena_alloc(P, ws, bytes, cls);
     at = __shfl_sync(QC_FULL, at, 0);
     if (at == ~0ull) return;
     char* rec = P.arena + at;
@@ -905,9 +942,8 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     }
     __syncwarp();
     if (lane == 0) {
-        atomicAdd(&P.ctl->children, 1ull);
-        atomicAdd(&P.ctl->child_vertices, (unsigned long long)tc);
-        atomicMax(&P.ctl->max_task, tc);
+        ws.cnt->children++;
+        ws.cnt->child_vertices += (unsigned long long)tc;
         __threadfence();
         WorkItem it;
         it.rec = at;
@@ -953,12 +989,12 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     for (int w = lane; w < W; w += 32) D[w] = PRE[w] & rec_ld(r2q + w);
     __syncwarp();
     if (lane == 0) {
-        atomicAdd(&P.ctl->branches, 1ull);
-        atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
+        ws.cnt->branches++;
+        ws.cnt->parent_vertices += (unsigned long long)(q + 1);
         int pid = rec_ld(T.ids + q);
         if (pid >= 0 && pid < R.n)
-            atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
-                                                           (R.off2[pid + 1] - R.off2[pid])));
+            ws.cnt->p_rows += (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
+                                                   (R.off2[pid + 1] - R.off2[pid]));
     }
 
     Bounds b = {0, 0, 0};
@@ -1210,7 +1246,6 @@ __device__ void emit_small(const ExpandParams& P, const Rules& R, unsigned S, in
             at = ~0ull;
         } else {
             P.set_starts[idx] = at;
-            atomicAdd(&P.ctl->emitted_ints, (unsigned long long)(k + 1));
             P.results[at] = k;
         }
     }
@@ -1267,7 +1302,7 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
     unsigned long long bytes = rec_bytes(tc, 1);
     unsigned long long at = 0;
     int cls = 0;
-    if (lane == 0) at = arena_alloc(P, bytes, cls);
+    if (lane == 0) at = arena_alloc(P, ws, bytes, cls);
     at = __shfl_sync(QC_FULL, at, 0);
     if (at == ~0ull) return;
     char* rec = P.arena + at;
@@ -1289,8 +1324,8 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
     }
     __syncwarp();
     if (lane == 0) {
-        atomicAdd(&P.ctl->children, 1ull);
-        atomicAdd(&P.ctl->child_vertices, (unsigned long long)tc);
+        ws.cnt->children++;
+        ws.cnt->child_vertices += (unsigned long long)tc;
         __threadfence();
         WorkItem it;
         it.rec = at;
@@ -1312,13 +1347,16 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
     int ex = __popc(T.a1 & PRE);
     unsigned r2q = __shfl_sync(QC_FULL, T.a2, q);
     unsigned D = PRE & r2q;
-    if (lane == 0) {
-        atomicAdd(&P.ctl->branches, 1ull);
-        atomicAdd(&P.ctl->parent_vertices, (unsigned long long)(q + 1));
-    }
-    if (lane == q && T.id >= 0 && T.id < R.n) {
-        atomicAdd(&P.ctl->p_rows, (unsigned long long)((R.off[T.id + 1] - R.off[T.id]) +
-                                                       (R.off2[T.id + 1] - R.off2[T.id])));
+    {
+        long long rows = 0;
+        if (lane == q && T.id >= 0 && T.id < R.n)
+            rows = (R.off[T.id + 1] - R.off[T.id]) + (R.off2[T.id + 1] - R.off2[T.id]);
+        rows = __shfl_sync(QC_FULL, rows, q);
+        if (lane == 0) {
+            ws.cnt->branches++;
+            ws.cnt->parent_vertices += (unsigned long long)(q + 1);
+            ws.cnt->p_rows += (unsigned long long)rows;
+        }
     }
     Bounds b = {0, 0, 0};
     unsigned Rm = 0;
@@ -1371,8 +1409,8 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
     int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
     if (lane == 0) {
-        atomicAdd(&P.ctl->tasks, 1ull);
-        atomicMax(&P.ctl->max_task, t);
+        ws.cnt->tasks++;
+        if ((unsigned long long)t > ws.cnt->max_task) ws.cnt->max_task = t;
     }
     // lookahead (main.cu:1349-1405)
     int need_t = md_at(R, t);
@@ -1381,7 +1419,7 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
         if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
         bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
         if (!__any_sync(QC_FULL, bad)) {
-            if (lane == 0) atomicAdd(&P.ctl->lookahead_hits, 1ull);
+            if (lane == 0) ws.cnt->lookahead_hits++;
             emit_small(P, R, low_mask(t), T.id);
             return;
         }
@@ -1410,12 +1448,15 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
 // a work item: fresh task (lookahead, branch range) or a branch range
 // ------------------------------------------------------------------
 
-__device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, const TaskHdr& hv)
+// Returns true when other work items (branch ranges pushed here or earlier)
+// share the record, so its release must go through the reference count.
+__device__ bool process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, const TaskHdr& hv)
 {
     TaskView T = task_view(P.arena, it.rec, hv);
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
     const Rules R = P.rules[T.inst];
+    bool shared = it.q_lo >= 0;
     {
         int bad = 0;
         for (int v = lane; v < t; v += 32) {
@@ -1424,22 +1465,22 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
         }
         if (__any_sync(QC_FULL, bad)) {
             if (lane == 0) check_fail(P, 8, it.rec);
-            return;
+            return shared;
         }
     }
     if (t > P.max_t) {
         if (lane == 0) set_status(P, ST_TOO_LARGE);
-        return;
+        return shared;
     }
     int q_lo = it.q_lo, q_hi = it.q_hi;
     if (q_lo < 0 && t <= 32 && P.small_path) {
         process_small(P, R, ws, T);
-        return;
+        return shared;
     }
     if (q_lo < 0) {
         if (lane == 0) {
-            atomicAdd(&P.ctl->tasks, 1ull);
-            atomicMax(&P.ctl->max_task, t);
+            ws.cnt->tasks++;
+            if ((unsigned long long)t > ws.cnt->max_task) ws.cnt->max_task = t;
         }
         uint32_t* MM = ws.mk[MK_M];
         uint32_t* CC = ws.mk[MK_C];
@@ -1472,9 +1513,9 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
             if (!__any_sync(QC_FULL, bad2)) {
                 uint32_t* all = ws.mk[MK_T];
                 bs_range(all, W, 0, t);
-                if (lane == 0) atomicAdd(&P.ctl->lookahead_hits, 1ull);
+                if (lane == 0) ws.cnt->lookahead_hits++;
                 emit_mask(P, R, T, all, t);
-                return;
+                return shared;
             }
         }
         // branches executed before a member fails on removal (main.cu:1092-1099)
@@ -1489,7 +1530,7 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
             int seen = 0;
             for (int base = 0; base < W * 32; base += 32 * 32) {
                 int w = (base >> 5) + lane;
-                uint32_t x = (w < W) ? (row[w] & CC[w]) : 0u;
+                uint32_t x = (w < W) ? (rec_ld(row + w) & CC[w]) : 0u;
                 int c = __popc(x);
                 int inc = wscan(c);
                 int tot = __shfl_sync(QC_FULL, inc, 31);
@@ -1511,7 +1552,7 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
         }
         q_lo = qmax > t - 1 ? t - 1 : qmax;
         q_hi = t - 1;
-        if (m + T.cov >= t) return; // no branchable candidate
+        if (m + T.cov >= t) return shared; // no branchable candidate
         int nb = q_hi - q_lo + 1;
         if (nb > P.split) {
             __syncwarp();
@@ -1529,16 +1570,18 @@ __device__ void process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
             }
             __syncwarp();
             q_lo = q_hi - P.split + 1;
+            shared = true;
         }
     }
     for (int q = q_hi; q >= q_lo; q--) {
-        if (*(volatile int*)&P.ctl->status) return;
+        if (*(volatile int*)&P.ctl->status) return shared;
         if (P.deadline_ns && now_ns() > P.deadline_ns) {
             if (lane == 0) set_status(P, ST_DEADLINE);
-            return;
+            return shared;
         }
         expand_branch(P, R, T, ws, q);
     }
+    return shared;
 }
 
 
@@ -1593,7 +1636,14 @@ __global__ void expand_kernel(ExpandParams P)
     int lane = lane_id();
     int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     Ws ws = ws_view(P, warp_global);
-    if (lane == 0) *ws.kept_set = 0;
+    if (lane == 0) {
+        *ws.kept_set = 0;
+        *ws.cnt = WarpCount{};
+    }
+    for (int c = lane; c < kArenaClasses; c += 32) {
+        ws.fhead[c] = 0;
+        ws.fcount[c] = 0;
+    }
     __syncwarp();
     for (;;) {
         WorkItem it;
@@ -1620,13 +1670,25 @@ __global__ void expand_kernel(ExpandParams P)
         hv.W = __shfl_sync(QC_FULL, hv.W, 0);
         hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
         __threadfence();
-        process_item(P, ws, it, hv);
+        bool shared = process_item(P, ws, it, hv);
         __syncwarp();
         __threadfence();
         if (lane == 0) {
-            release_record(P, it.rec);
-            atomicSub(&P.ctl->pending, 1);
+            release_record(P, ws, it.rec, !shared);
+            // a kept child inherits this item's outstanding-work count
+            if (!*ws.kept_set) atomicSub(&P.ctl->pending, 1);
         }
+    }
+    if (lane == 0) {
+        const WarpCount& c = *ws.cnt;
+        if (c.tasks) atomicAdd(&P.ctl->tasks, c.tasks);
+        if (c.branches) atomicAdd(&P.ctl->branches, c.branches);
+        if (c.children) atomicAdd(&P.ctl->children, c.children);
+        if (c.lookahead_hits) atomicAdd(&P.ctl->lookahead_hits, c.lookahead_hits);
+        if (c.parent_vertices) atomicAdd(&P.ctl->parent_vertices, c.parent_vertices);
+        if (c.p_rows) atomicAdd(&P.ctl->p_rows, c.p_rows);
+        if (c.child_vertices) atomicAdd(&P.ctl->child_vertices, c.child_vertices);
+        if (c.max_task) atomicMax(&P.ctl->max_task, (int)c.max_task);
     }
 }
 

@@ -408,7 +408,6 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
 
         Control ctl{};
         ctl.arena_top = root_block;
-        ctl.arena_live = root_block;
         ctl.arena_cap = (unsigned long long)c->arena_bytes;
         ctl.result_cap = (unsigned long long)c->result_ints;
         ctl.set_cap = (unsigned long long)set_cap;
@@ -507,7 +506,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         r->st.p_rows = (int64_t)ctl.p_rows;
         r->st.child_vertices = (int64_t)ctl.child_vertices;
         r->st.kernel_ms = kms;
-        r->st.arena_peak = (int64_t)ctl.arena_live_peak;
+        r->st.arena_peak = (int64_t)std::min(ctl.arena_top, ctl.arena_cap);
         r->st.kernel_launches = c->launches;
         if (c->cfg.keep_emitted) {
             flat.resize((size_t)ctl.result_top);
@@ -803,7 +802,6 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         c->launches += 3;
         ctl = Control{};
         ctl.arena_top = arena_at;
-        ctl.arena_live = arena_at;
         ctl.arena_cap = (unsigned long long)c->arena_bytes;
         ctl.result_cap = (unsigned long long)c->result_ints;
         ctl.set_cap = (unsigned long long)set_cap;
@@ -916,7 +914,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         st.emitted_ints = (int64_t)ctl.result_top;
         st.maximal = res[(size_t)i]->nsets;
         st.max_task = ctl.max_task;
-        st.arena_peak = (int64_t)ctl.arena_live_peak;
+        st.arena_peak = (int64_t)std::min(ctl.arena_top, ctl.arena_cap);
         st.kernel_launches = c->launches;
         st.parent_vertices = (int64_t)ctl.parent_vertices;
         st.p_rows = (int64_t)ctl.p_rows;

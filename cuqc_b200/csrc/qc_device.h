@@ -50,14 +50,12 @@ struct Control {
     int stack_cap;
     int pending;                   // work items pushed and not yet finished
     int status;
-    unsigned long long tasks, branches, children, emitted, emitted_ints;
+    unsigned long long tasks, branches, children, emitted;
     unsigned long long lookahead_hits;
     unsigned long long parent_vertices, p_rows, child_vertices;
     int max_task;
     int active_warps;              // warps still inside the work loop
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
-    unsigned long long arena_live;      // bytes in blocks currently allocated
-    unsigned long long arena_live_peak;
     unsigned long long check_site;      // first failed self-check: site id
     unsigned long long check_value;     //   ... and the offending value
     unsigned long long free_head[kArenaClasses * kArenaShards]; // [tag:24 | offset/16+1:40]
@@ -149,9 +147,22 @@ struct ExpandParams {
     unsigned long long deadline_ns; // globaltimer value to stop at (0: none)
 };
 
+// Work counters a warp accumulates privately and adds to the control block
+// once, when it leaves the work loop.
+struct WarpCount {
+    unsigned long long tasks, branches, children, lookahead_hits;
+    unsigned long long parent_vertices, p_rows, child_vertices;
+    unsigned long long max_task;
+};
+
+// Blocks a warp keeps on its private free lists before it hands further
+// frees to the shared lists.
+constexpr int kPrivateFreeCap = 64;
+
 // Per-warp workspace layout for tasks of up to max_t vertices.
 struct WsLayout {
-    int64_t kept, indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
+    int64_t kept, count, freel, indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo,
+        masks;
     int64_t total;
 };
 
@@ -165,6 +176,8 @@ __host__ __device__ inline WsLayout ws_layout(int max_t)
     int64_t W = words_for(max_t) + 2;
     int64_t o = 0;
     L.kept = o;     o += 32;
+    L.count = o;    o += align16(sizeof(WarpCount));
+    L.freel = o;    o += align16((8 + 4) * (int64_t)kArenaClasses); // heads, then counts
     L.indeg = o;    o += align16(4 * t);
     L.exdeg = o;    o += align16(4 * t);
     L.aux = o;      o += align16(4 * t);

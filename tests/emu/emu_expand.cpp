@@ -77,7 +77,6 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     }
     Control ctl{};
     ctl.arena_top = arena_class_bytes(h->cls);
-    ctl.arena_live = ctl.arena_top;
     ctl.arena_cap = (unsigned long long)arena_bytes;
     ctl.result_cap = result_cap > 0 ? (unsigned long long)result_cap : (1ull << 24);
     ctl.set_cap = ctl.result_cap / 2 + 1;
@@ -127,7 +126,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     counters[4] = (int64_t)ctl.lookahead_hits;
     counters[5] = ctl.status;
     counters[6] = ctl.max_task;
-    counters[7] = (int64_t)ctl.arena_live_peak;
+    counters[7] = (int64_t)std::min(ctl.arena_top, ctl.arena_cap);
     int64_t k = std::min<int64_t>((int64_t)ctl.result_top, (int64_t)ctl.result_cap);
     if (ctl.status) k = 0;
     int32_t* out = (int32_t*)malloc(sizeof(int32_t) * (size_t)(k > 0 ? k : 1));
@@ -207,7 +206,6 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     }
     Control ctl{};
     ctl.arena_top = arena_at;
-    ctl.arena_live = arena_at;
     ctl.arena_cap = arena.size();
     ctl.result_cap = 1ull << 24;
     ctl.set_cap = 1ull << 22;
