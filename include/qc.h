@@ -131,7 +131,7 @@ typedef struct {
     int64_t maximal;       /* sets in the result                               */
     int64_t root_size;     /* vertices in the root task                        */
     int64_t max_task;      /* largest task                                     */
-    int64_t arena_peak;    /* bytes of task records written                    */
+    int64_t arena_peak;    /* high-water mark of the task-record arena (bytes) */
     int64_t kernel_launches;
     double kernel_ms;      /* expansion kernel alone (CUDA events)            */
     /* work counters for the algorithmic-byte model (per expanded branch:
