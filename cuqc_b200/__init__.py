@@ -38,6 +38,7 @@ EXPORTS = [
     "qc_graph_twohop_offsets", "qc_graph_twohop_neighbors", "qc_graph_free", "qc_config_default",
     "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
+    "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices",
 ]
 
 
@@ -120,6 +121,8 @@ def lib():
         L.qc_result_stats.restype = C.POINTER(Stats)
         L.qc_result_write.argtypes = [vp, C.c_char_p]
         L.qc_result_free.argtypes = [vp]
+        L.qc_twohop_noalloc.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int64, P64, vp]
+        L.qc_twohop_noalloc_max_vertices.restype = C.c_int32
         _lib = L
     return _lib
 

@@ -981,6 +981,28 @@ extern "C" void qc_result_free(qc_result* r) { delete r; }
 std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
                               std::vector<int32_t>& adj2);
 
+std::string qcb_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
+                               int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
+                               int64_t* total_out, cudaStream_t s, int* too_large, int* too_small);
+
+extern "C" qc_status qc_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
+                                       int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
+                                       int64_t* total_out, void* stream)
+{
+    if (n < 0 || !d_off2 || (n > 0 && !d_off)) return fail(QC_ERR_ARGS, "bad CSR arguments");
+    if (d_adj2 && adj2_cap < 0) return fail(QC_ERR_ARGS, "negative adj2 capacity");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(QC_ERR_NO_DEVICE, "no CUDA device visible");
+    int too_large = 0, too_small = 0;
+    std::string e = qcb_twohop_noalloc(n, d_off, d_adj, d_off2, d_adj2, adj2_cap, total_out,
+                                       (cudaStream_t)stream, &too_large, &too_small);
+    if (e.empty()) return QC_OK;
+    if (too_large) return fail(QC_ERR_TOO_LARGE, e);
+    if (too_small) return fail(QC_ERR_RESULT_OVERFLOW, e);
+    return fail(QC_ERR_CUDA, e);
+}
+
 extern "C" qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int32_t* adj,
                                        qc_graph** out)
 {

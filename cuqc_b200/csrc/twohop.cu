@@ -12,8 +12,10 @@
 // the touched words.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -191,4 +193,174 @@ done:
     cudaFree(d_off2);
     cudaFree(d_adj2);
     return g_th_err;
+}
+
+// ------------------------------------------------------------------
+// Two-hop lists without any device allocation (qc_twohop_noalloc).
+//
+// For callers that cannot call cudaMalloc: an application whose device
+// memory is owned by its own pool or fixed memory plan, or that must not
+// allocate while it is serving requests.  Inputs and outputs are the
+// caller's device buffers; the per-warp working memory (a bitmap of n bits
+// and a list of touched bitmap words per warp) lives in one file-scope
+// __device__ array that every GPU which loads this library holds until the
+// process exits.
+// ------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 16u << 20;  // 16 MiB per device
+constexpr int kNoAllocMinWarps = 32;                 // fewest warps a call may run on
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_twohop_scratch[kNoAllocScratchBytes];
+
+// Device address of g_twohop_scratch, looked up once per device (the host
+// symbol is only a stand-in: a kernel handed it would fault or read the
+// wrong memory).
+struct ScratchAddr {
+    std::mutex mu;
+    void* ptr[kNoAllocMaxDevices] = {};
+};
+ScratchAddr g_scratch_addr;
+
+cudaError_t scratch_for_device(int dev, unsigned char** out)
+{
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_scratch_addr.mu);
+    if (!g_scratch_addr.ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_twohop_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr.ptr[dev] = p;
+    }
+    *out = (unsigned char*)g_scratch_addr.ptr[dev];
+    return cudaSuccess;
+}
+
+// In-place scan of off2[1..n] (per-vertex counts) into CSR offsets, off2[0] = 0.
+// One block walks the array in chunks of its size, carrying the running total.
+__global__ void twohop_scan_kernel(int64_t* off2, int n)
+{
+    __shared__ int64_t warp_tot[32];
+    __shared__ int64_t carry;
+    int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) {
+        carry = 0;
+        off2[0] = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        int i = base + tid;
+        int64_t x = i < n ? off2[(int64_t)i + 1] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int nw = blockDim.x >> 5;
+            int64_t w = lane < nw ? warp_tot[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < nw) warp_tot[lane] = w;
+        }
+        __syncthreads();
+        int64_t before = (wid > 0 ? warp_tot[wid - 1] : 0) + carry;
+        if (i < n) off2[(int64_t)i + 1] = before + x;
+        __syncthreads();
+        if (tid == blockDim.x - 1) carry = before + x;
+        __syncthreads();
+    }
+}
+
+} // namespace
+
+std::string qcb_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
+                               int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
+                               int64_t* total_out, cudaStream_t s, int* too_large, int* too_small)
+{
+    *too_large = 0;
+    *too_small = 0;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+    unsigned char* scratch = nullptr;
+    e = scratch_for_device(dev, &scratch);
+    if (e != cudaSuccess) return std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+    if (n == 0) {
+        e = cudaMemsetAsync(d_off2, 0, sizeof(int64_t), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (total_out) *total_out = 0;
+        return e == cudaSuccess ? "" : std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+    }
+    // per-warp working memory: bitmap words, touched-word list (padded to a
+    // power of two for the warp sort), touched counter
+    const int64_t bm_words = ((int64_t)n + 31) / 32;
+    int64_t touched_cap = 1;
+    while (touched_cap < bm_words) touched_cap <<= 1;
+    const int64_t per_warp = 4 * bm_words + 4 * touched_cap + 4;
+    int64_t fit = (int64_t)kNoAllocScratchBytes / per_warp;
+    if (fit < kNoAllocMinWarps) {
+        *too_large = 1;
+        return "graph has " + std::to_string(n) + " vertices; qc_twohop_noalloc supports at most " +
+               std::to_string(qc_twohop_noalloc_max_vertices());
+    }
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e);
+    int64_t nwarps = std::min<int64_t>(fit, (int64_t)sms * 2 * kTwohopWarpsPerBlock);
+    nwarps -= nwarps % kTwohopWarpsPerBlock;
+    const int blocks = (int)(nwarps / kTwohopWarpsPerBlock);
+    uint32_t* bm = (uint32_t*)scratch;
+    int32_t* touched = (int32_t*)(scratch + 4 * bm_words * nwarps);
+    int* nt = (int*)(scratch + 4 * bm_words * nwarps + 4 * touched_cap * nwarps);
+    // the array keeps the last call's contents: the bitmaps must start empty
+    e = cudaMemsetAsync(bm, 0, sizeof(uint32_t) * bm_words * nwarps, s);
+    if (e != cudaSuccess) return std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+    // pass 1: per-vertex counts into off2[1..n], then the scan
+    twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32, 0, s>>>(
+        n, d_off, d_adj, bm, bm_words, touched, touched_cap, nt, d_off2 + 1, nullptr, nullptr);
+    twohop_scan_kernel<<<1, 1024, 0, s>>>(d_off2, n);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return std::string("launch: ") + cudaGetErrorString(e);
+    int64_t total = 0;
+    e = cudaMemcpyAsync(&total, d_off2 + n, sizeof(total), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return std::string("two-hop count: ") + cudaGetErrorString(e);
+    if (total_out) *total_out = total;
+    if (!d_adj2) return ""; // size query
+    if (total > adj2_cap) {
+        *too_small = 1;
+        return "adj2 holds " + std::to_string(adj2_cap) + " entries; the two-hop lists need " +
+               std::to_string(total);
+    }
+    // pass 2: sorted rows
+    twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32, 0, s>>>(
+        n, d_off, d_adj, bm, bm_words, touched, touched_cap, nt, nullptr, d_off2, d_adj2);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return std::string("two-hop rows: ") + cudaGetErrorString(e);
+    return "";
+}
+
+extern "C" int32_t qc_twohop_noalloc_max_vertices(void)
+{
+    // largest n (a multiple of 32) whose per-warp working memory still leaves
+    // room for kNoAllocMinWarps warps; the need grows with n
+    auto fits = [](int64_t n) {
+        int64_t w = (n + 31) / 32, tc = 1;
+        while (tc < w) tc <<= 1;
+        return (int64_t)kNoAllocScratchBytes / (4 * w + 4 * tc + 4) >= kNoAllocMinWarps;
+    };
+    int64_t lo = 32, hi = (int64_t)1 << 30; // fits(lo), !fits(hi)
+    while (hi - lo > 32) {
+        int64_t mid = ((lo + hi) / 2) & ~int64_t(31);
+        if (mid <= lo) mid = lo + 32;
+        if (fits(mid)) lo = mid;
+        else hi = mid;
+    }
+    return (int32_t)lo;
 }

@@ -63,6 +63,35 @@ qc_status qc_graph_from_csr2(int32_t n, const int64_t* off, const int32_t* adj,
  * adjToSer preprocessing (adjToSer.cpp:115-156). */
 qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int32_t* adj, qc_graph** out);
 
+/* Two-hop lists of a graph already in device memory, computed without any
+ * device allocation.  No counterpart in the reference (cuQC builds its
+ * two-hop lists offline, adjToSer.cpp:115-156, and allocates freely).
+ *
+ * For callers that cannot call cudaMalloc: applications whose device memory
+ * is owned by their own pool or a fixed memory plan, or that must not
+ * allocate while serving requests.  The caller passes device buffers:
+ * d_off (int64[n+1]) and d_adj (int32[d_off[n]]) hold a sorted, symmetric
+ * 1-hop CSR; d_off2 (int64[n+1]) receives the two-hop offsets and d_adj2
+ * (int32[adj2_cap]) the rows sorted(N(v) u N(N(v)) minus {v}).  With
+ * d_adj2 == NULL only d_off2 and *total_out are filled (a size query); if
+ * the rows need more than adj2_cap entries the call returns
+ * QC_ERR_RESULT_OVERFLOW with *total_out set to the size needed.
+ *
+ * Working memory is one 16 MiB array in device memory that every GPU which
+ * loads the library holds until the process exits; graphs above
+ * qc_twohop_noalloc_max_vertices() vertices are rejected with
+ * QC_ERR_TOO_LARGE.  The first call on a device looks up that array's device
+ * address, so make it before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU (other threads, other streams) race
+ * and must be serialised by the caller.  The call runs on `stream` (a
+ * cudaStream_t; NULL = the default stream) and returns when the lists are
+ * written. */
+qc_status qc_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
+                            int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
+                            int64_t* total_out, void* stream);
+/* Largest vertex count qc_twohop_noalloc accepts. */
+int32_t qc_twohop_noalloc_max_vertices(void);
+
 /* Write the graph in the serialized format (adjToSer.cpp:159-204). */
 qc_status qc_graph_write_serialized(const qc_graph* g, const char* path);
 
