@@ -163,8 +163,7 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
 }
 
 struct Ws {
-    WorkItem* kept;    // a child this warp runs next instead of pushing it
-    int32_t* kept_set; // 1 while kept holds an item
+    WarpSmem* sm;      // per-warp state in shared memory
     WarpCount* cnt;    // this warp's work counters (lane 0)
     unsigned long long* fhead; // private free list per size class: offset/16+1, 0 = empty
     int32_t* fcount;           // blocks on each private list
@@ -180,16 +179,15 @@ struct Ws {
     uint32_t* mk[12];
 };
 
-__device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global)
+__device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global, WarpSmem* sm)
 {
     WsLayout L = ws_layout(P.max_t);
     char* b = P.ws + (int64_t)warp_global * P.ws_stride;
     Ws w;
-    w.kept = (WorkItem*)(b + L.kept);
-    w.kept_set = (int32_t*)(b + L.kept + sizeof(WorkItem));
-    w.cnt = (WarpCount*)(b + L.count);
-    w.fhead = (unsigned long long*)(b + L.freel);
-    w.fcount = (int32_t*)(b + L.freel + 8 * (int64_t)kArenaClasses);
+    w.sm = sm;
+    w.cnt = &sm->cnt;
+    w.fhead = sm->fhead;
+    w.fcount = sm->fcount;
     w.indeg = (int32_t*)(b + L.indeg);
     w.exdeg = (int32_t*)(b + L.exdeg);
     w.aux = (int32_t*)(b + L.aux);
@@ -221,7 +219,7 @@ __device__ __forceinline__ int md_at(const Rules& R, int k)
 {
     k = k < 0 ? 0 : k;
     k = k >= R.mdlen ? R.mdlen - 1 : k;
-    return R.md[k];
+    return k < kTabCache ? R.md_s[k] : __ldg(R.md + k);
 }
 __device__ __forceinline__ int mindeg(const Rules& R, int k)
 {
@@ -231,7 +229,7 @@ __device__ __forceinline__ int ubt_at(const Rules& R, int d)
 {
     d = d < 0 ? 0 : d;
     d = d >= R.mdlen ? R.mdlen - 1 : d;
-    return R.ubt[d];
+    return d < kTabCache ? R.ubt_s[d] : __ldg(R.ubt + d);
 }
 
 // main.cu:2167-2178
@@ -682,9 +680,9 @@ __device__ int pop_item(const ExpandParams& P, WorkItem& out)
 // it (the warp does not decrement `pending` when it finishes that item).
 __device__ void schedule_child(const ExpandParams& P, Ws& ws, const WorkItem& it)
 {
-    if (!*ws.kept_set) {
-        *ws.kept = it;
-        *ws.kept_set = 1;
+    if (!ws.sm->kept_set) {
+        ws.sm->kept_rec = it.rec;
+        ws.sm->kept_set = 1;
         return;
     }
     push_item(P, it);
@@ -710,14 +708,8 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigne
     // this warp's own free list: blocks it freed itself, no other warp touches it
     if (ws.fcount[cls] > 0) {
         unsigned long long off = (ws.fhead[cls] - 1) * 16;
-        unsigned long long lim = *(volatile unsigned long long*)&P.ctl->arena_top;
-        if (lim > P.ctl->arena_cap) lim = P.ctl->arena_cap;
-        if (ws.fhead[cls] == 0 || off + size > lim) {
+        if (ws.fhead[cls] == 0 || off + size > P.arena_cap) {
             check_fail(P, 13, off); // a private list that points outside the arena
-            return ~0ull;
-        }
-        if (((TaskHdr*)(P.arena + off))->refs != kFreeMagic) {
-            check_fail(P, 15, off); // a private-list block that is not free
             return ~0ull;
         }
         ws.fhead[cls] = *(unsigned long long*)(P.arena + off) & kOffMask;
@@ -796,17 +788,14 @@ __device__ void arena_free(const ExpandParams& P, Ws& ws, unsigned long long off
 // a work item on this record is finished; the last one frees the block.
 // `sole`: no other work item ever referenced the record (a task processed
 // whole by one warp), so the reference count needs no atomic.
-__device__ void release_record(const ExpandParams& P, Ws& ws, unsigned long long rec, bool sole)
+// `hv` is the record's header as validated when the item was dequeued.
+__device__ void release_record(const ExpandParams& P, Ws& ws, unsigned long long rec, bool sole,
+                               const TaskHdr& hv)
 {
     TaskHdr* h = (TaskHdr*)(P.arena + rec);
-    int cls = *(volatile int32_t*)&h->cls;
-    if (cls < 0 || cls >= kArenaClasses) {
-        check_fail(P, 11, rec); // a header whose size class is out of range
-        return;
-    }
+    int cls = hv.cls;
     if (sole) {
-        int before = *(volatile int32_t*)&h->refs;
-        if (before != 1) {
+        if (hv.refs != 1) {
             check_fail(P, 14, rec); // a record thought to be private has other users
             return;
         }
@@ -1438,10 +1427,8 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     int qlo = rmax(pos);
     qlo = qlo > m + T.cov ? qlo : m + T.cov;
     if (qlo > t - 1) return;
-    for (int q = t - 1; q >= qlo; q--) {
-        if (*(volatile int*)&P.ctl->status) return;
-        branch_small(P, R, ws, T, q);
-    }
+    if (*(volatile int*)&P.ctl->status) return;
+    for (int q = t - 1; q >= qlo; q--) branch_small(P, R, ws, T, q);
 }
 
 // ------------------------------------------------------------------
@@ -1455,7 +1442,20 @@ __device__ bool process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
     TaskView T = task_view(P.arena, it.rec, hv);
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
-    const Rules R = P.rules[T.inst];
+    Rules R = P.rules[T.inst];
+    if (ws.sm->tab_inst != T.inst) {
+        // refresh this warp's shared copy of the instance's gamma tables
+        for (int k = lane; k < kTabCache; k += 32) {
+            int kk = k < R.mdlen ? k : R.mdlen - 1;
+            ws.sm->md[k] = __ldg(R.md + kk);
+            ws.sm->ubt[k] = __ldg(R.ubt + kk);
+        }
+        __syncwarp();
+        if (lane == 0) ws.sm->tab_inst = T.inst;
+        __syncwarp();
+    }
+    R.md_s = ws.sm->md;
+    R.ubt_s = ws.sm->ubt;
     bool shared = it.q_lo >= 0;
     {
         int bad = 0;
@@ -1593,21 +1593,23 @@ __device__ bool process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
 // validated values.
 __device__ bool item_ok(const ExpandParams& P, const WorkItem& it, TaskHdr& hv)
 {
-    unsigned long long top = *(volatile unsigned long long*)&P.ctl->arena_top;
-    unsigned long long cap = P.ctl->arena_cap;
-    unsigned long long lim = top < cap ? top : cap;
+    const unsigned long long lim = P.arena_cap;
     unsigned long long site = 0, val = it.rec;
     if ((it.rec & 15ull) != 0) site = 1;
     else if (it.rec + sizeof(TaskHdr) > lim) site = 2;
     else {
         const volatile TaskHdr* h = (const volatile TaskHdr*)(P.arena + it.rec);
-        int t = h->t, W = h->W, m = h->m, inst = h->inst, cov = h->cov;
+        int t = h->t, W = h->W, m = h->m, inst = h->inst, cov = h->cov, cls = h->cls,
+            refs = h->refs;
         hv.t = t;
         hv.W = W;
         hv.m = m;
         hv.inst = inst;
         hv.cov = cov;
-        if (t < 1 || t > P.max_t || W != words_for(t) || m < 0 || m > t || cov < 0 || m + cov > t) {
+        hv.cls = cls;
+        hv.refs = refs;
+        if (t < 1 || t > P.max_t || W != words_for(t) || m < 0 || m > t || cov < 0 || m + cov > t ||
+            cls < 0 || cls >= kArenaClasses || refs < 1 || refs == kFreeMagic) {
             site = 3;
             val = ((unsigned long long)(unsigned)t << 32) | (unsigned)W;
         } else if (it.rec + rec_bytes(t, W) > lim) site = 4;
@@ -1628,6 +1630,16 @@ __device__ bool item_ok(const ExpandParams& P, const WorkItem& it, TaskHdr& hv)
 // ------------------------------------------------------------------
 
 #ifndef QC_EMULATION
+extern __shared__ __align__(16) unsigned char qc_dyn_smem[];
+__device__ __forceinline__ unsigned char* dyn_smem() { return qc_dyn_smem; }
+#else
+__device__ __forceinline__ unsigned char* dyn_smem() { return emu_dyn_smem(); }
+#endif
+
+// dynamic shared memory the kernel needs per block of `warps` warps
+__host__ __device__ inline size_t expand_smem_bytes(int warps) { return sizeof(WarpSmem) * (size_t)warps; }
+
+#ifndef QC_EMULATION
 __global__ void __launch_bounds__(256, 2) expand_kernel(ExpandParams P)
 #else
 __global__ void expand_kernel(ExpandParams P)
@@ -1635,14 +1647,16 @@ __global__ void expand_kernel(ExpandParams P)
 {
     int lane = lane_id();
     int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    Ws ws = ws_view(P, warp_global);
+    WarpSmem* sm = (WarpSmem*)dyn_smem() + (threadIdx.x >> 5);
+    Ws ws = ws_view(P, warp_global, sm);
     if (lane == 0) {
-        *ws.kept_set = 0;
-        *ws.cnt = WarpCount{};
+        sm->kept_set = 0;
+        sm->tab_inst = -1;
+        sm->cnt = WarpCount{};
     }
     for (int c = lane; c < kArenaClasses; c += 32) {
-        ws.fhead[c] = 0;
-        ws.fcount[c] = 0;
+        sm->fhead[c] = 0;
+        sm->fcount[c] = 0;
     }
     __syncwarp();
     for (;;) {
@@ -1650,10 +1664,12 @@ __global__ void expand_kernel(ExpandParams P)
         TaskHdr hv{};
         int r = 0;
         if (lane == 0) {
-            if (*ws.kept_set) {
-                it = *ws.kept;
-                *ws.kept_set = 0;
-                r = *(volatile int*)&P.ctl->status ? -1 : 1;
+            if (sm->kept_set) {
+                it.rec = sm->kept_rec;
+                it.q_lo = -1;
+                it.q_hi = -1;
+                sm->kept_set = 0;
+                r = 1;
             } else {
                 r = pop_item(P, it);
             }
@@ -1674,13 +1690,13 @@ __global__ void expand_kernel(ExpandParams P)
         __syncwarp();
         __threadfence();
         if (lane == 0) {
-            release_record(P, ws, it.rec, !shared);
+            release_record(P, ws, it.rec, !shared, hv);
             // a kept child inherits this item's outstanding-work count
-            if (!*ws.kept_set) atomicSub(&P.ctl->pending, 1);
+            if (!sm->kept_set) atomicSub(&P.ctl->pending, 1);
         }
     }
     if (lane == 0) {
-        const WarpCount& c = *ws.cnt;
+        const WarpCount& c = sm->cnt;
         if (c.tasks) atomicAdd(&P.ctl->tasks, c.tasks);
         if (c.branches) atomicAdd(&P.ctl->branches, c.branches);
         if (c.children) atomicAdd(&P.ctl->children, c.children);

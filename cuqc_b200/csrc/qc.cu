@@ -352,7 +352,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     // polls the shared stack, so the default is one block of 4 warps per SM.
     int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
     int resident = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32,
+                                                     expand_smem_bytes(wpb)));
     if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
     // a persistent launch: never more blocks than can be resident at once
     int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : 1;
@@ -442,6 +443,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.set_starts = c->starts.as<unsigned long long>();
         P.ws = c->ws.as<char>();
         P.ws_stride = L.total;
+        P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 1;
         P.small_path = 1;
@@ -454,7 +456,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
             P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
         }
         CK(cudaEventRecord(c->ev[1], s));
-        expand_kernel<<<blocks, wpb * 32, 0, s>>>(P);
+        expand_kernel<<<blocks, wpb * 32, expand_smem_bytes(wpb), s>>>(P);
         CK(cudaGetLastError());
         c->launches += 1;
         CK(cudaEventRecord(c->ev[2], s));
@@ -754,7 +756,8 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
 
     int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
     int resident = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32,
+                                                     expand_smem_bytes(wpb)));
     if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
     int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : 1;
     int blocks = c->sms * bps;
@@ -827,6 +830,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         P.set_starts = c->starts.as<unsigned long long>();
         P.ws = c->ws.as<char>();
         P.ws_stride = L.total;
+        P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = max_t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 1;
         P.small_path = 1;
@@ -838,7 +842,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
             P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
         }
         CK(cudaEventRecord(c->ev[1], s));
-        expand_kernel<<<blocks, wpb * 32, 0, s>>>(P);
+        expand_kernel<<<blocks, wpb * 32, expand_smem_bytes(wpb), s>>>(P);
         CK(cudaGetLastError());
         c->launches += 1;
         CK(cudaEventRecord(c->ev[2], s));

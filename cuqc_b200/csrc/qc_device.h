@@ -125,6 +125,8 @@ struct Rules {
     int32_t min_size;
     int32_t vbase;       // added to vertex ids when sets are emitted
     int32_t n;           // vertices of the instance (ids must be below it)
+    const int32_t* md_s;  // shared-memory copies of md / ubt [0, kTabCache) (set on the
+    const int32_t* ubt_s; //   device per warp; null in the table uploaded by the host)
 };
 
 constexpr int32_t kFreeMagic = 0x7ee7f00d; // refs of a block on a free list
@@ -140,6 +142,7 @@ struct ExpandParams {
     unsigned long long* set_starts; // start offset (in results) of every emitted set
     char* ws;            // per-warp workspace
     int64_t ws_stride;   // bytes per warp
+    unsigned long long arena_cap; // bytes of the record arena
     int32_t max_t;       // largest task the workspace holds
     int32_t split;       // branches per work item before splitting
     int32_t small_path;  // 1: tasks of <= 32 vertices use the register path
@@ -159,10 +162,26 @@ struct WarpCount {
 // frees to the shared lists.
 constexpr int kPrivateFreeCap = 64;
 
-// Per-warp workspace layout for tasks of up to max_t vertices.
+// Entries of the gamma tables (md, ubt) a warp keeps in shared memory; the
+// tests of tasks up to this size never look further.
+constexpr int kTabCache = 128;
+
+// Per-warp state in shared memory: everything a warp touches on every task.
+struct WarpSmem {
+    WarpCount cnt;
+    unsigned long long kept_rec; // a child this warp runs next instead of pushing it
+    int32_t kept_set;            // 1 while kept_rec holds one
+    int32_t tab_inst;            // instance whose gamma tables are cached (-1: none)
+    unsigned long long fhead[kArenaClasses]; // private free lists: offset/16+1, 0 = empty
+    int32_t fcount[kArenaClasses];
+    int32_t md[kTabCache];
+    int32_t ubt[kTabCache];
+};
+
+// Per-warp workspace (global memory) for the bit-matrix path, tasks of up
+// to max_t vertices.
 struct WsLayout {
-    int64_t kept, count, freel, indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo,
-        masks;
+    int64_t indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
     int64_t total;
 };
 
@@ -175,9 +194,6 @@ __host__ __device__ inline WsLayout ws_layout(int max_t)
     tp += 64;
     int64_t W = words_for(max_t) + 2;
     int64_t o = 0;
-    L.kept = o;     o += 32;
-    L.count = o;    o += align16(sizeof(WarpCount));
-    L.freel = o;    o += align16((8 + 4) * (int64_t)kArenaClasses); // heads, then counts
     L.indeg = o;    o += align16(4 * t);
     L.exdeg = o;    o += align16(4 * t);
     L.aux = o;      o += align16(4 * t);

@@ -34,6 +34,8 @@ struct EmuWarp {
 };
 inline thread_local EmuWarp* emu_w = nullptr;
 inline thread_local int emu_lane = 0;
+inline thread_local unsigned char* emu_smem = nullptr; // this block's dynamic shared memory
+inline unsigned char* emu_dyn_smem() { return emu_smem; }
 
 inline uint64_t emu_xchg(uint64_t v, int src)
 {
@@ -86,6 +88,7 @@ inline int __all_sync(unsigned m, int pred) { return __ballot_sync(m, pred) == 0
 inline void __syncwarp(unsigned = 0xffffffffu) { emu_w->bar.arrive_and_wait(); }
 inline int __popc(unsigned x) { return __builtin_popcount(x); }
 template <class T> inline T __ldcg(const T* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+template <class T> inline T __ldg(const T* p) { return *p; }
 inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
 inline int __ffs(unsigned x) { return x ? __builtin_ctz(x) + 1 : 0; }
 inline int __clz(unsigned x) { return x ? __builtin_clz(x) : 32; }
@@ -136,20 +139,26 @@ inline unsigned long long emu_globaltimer()
         .count();
 }
 
-// Run `fn` as a grid of `blocks` x `threads` (threads a multiple of 32).
-inline void emu_launch(int blocks, int threads, const std::function<void()>& fn)
+// Run `fn` as a grid of `blocks` x `threads` (threads a multiple of 32) with
+// `smem_bytes` of dynamic shared memory per block.
+inline void emu_launch(int blocks, int threads, const std::function<void()>& fn,
+                       size_t smem_bytes = 0)
 {
     int nwarps_per_block = threads / 32;
     std::vector<EmuWarp*> warps;
     std::vector<std::thread> th;
+    std::vector<std::vector<unsigned char>> smem((size_t)blocks,
+                                                 std::vector<unsigned char>(smem_bytes + 16));
     for (int b = 0; b < blocks; b++)
         for (int w = 0; w < nwarps_per_block; w++) {
             EmuWarp* ew = new EmuWarp();
             warps.push_back(ew);
+            unsigned char* sb = smem[(size_t)b].data();
             for (int l = 0; l < 32; l++) {
                 th.emplace_back([=, &fn] {
                     emu_w = ew;
                     emu_lane = l;
+                    emu_smem = sb;
                     threadIdx.x = w * 32 + l;
                     blockIdx.x = b;
                     blockDim.x = threads;

@@ -112,12 +112,13 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     P.set_starts = set_starts.data();
     P.ws = ws.data();
     P.ws_stride = L.total;
+    P.arena_cap = ctl.arena_cap;
     P.max_t = t;
     P.split = split;
     P.small_path = small_path;
     P.wait_ns = 20000000000ll;
     P.deadline_ns = emu_deadline();
-    emu_launch(1, warps * 32, [&] { expand_kernel(P); });
+    emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps));
 
     counters[0] = (int64_t)ctl.tasks;
     counters[1] = (int64_t)ctl.branches;
@@ -230,12 +231,13 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     P.set_starts = set_starts.data();
     P.ws = ws.data();
     P.ws_stride = L.total;
+    P.arena_cap = ctl.arena_cap;
     P.max_t = max_t;
     P.split = split;
     P.small_path = 1;
     P.wait_ns = 20000000000ll;
     P.deadline_ns = emu_deadline();
-    if (!items.empty()) emu_launch(1, warps * 32, [&] { expand_kernel(P); });
+    if (!items.empty()) emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps));
     counters[0] = (int64_t)ctl.tasks;
     counters[1] = (int64_t)ctl.branches;
     counters[2] = ctl.status;
