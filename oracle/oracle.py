@@ -69,6 +69,7 @@ def lib():
         L.qo_brute.argtypes = [C.c_int, P64, P32, C.c_double, C.c_int, P64, P64, C.POINTER(P32)]
         L.qo_brute.restype = C.c_int
         L.qo_free.argtypes = [C.c_void_p]
+        L.qo_set_task_budget.argtypes = [C.c_int64]
         _lib = L
     return _lib
 
@@ -101,9 +102,16 @@ def unpack(flat):
     return out
 
 
-def mine(g, gamma, min_size, mode="clean"):
-    """Run the oracle enumeration. Returns (flat emitted sets, stats dict)."""
+class BudgetExceeded(RuntimeError):
+    """The search tree has more tasks than the budget given to ``mine``."""
+
+
+def mine(g, gamma, min_size, mode="clean", max_tasks=0):
+    """Run the oracle enumeration. Returns (flat emitted sets, stats dict).
+    With ``max_tasks`` > 0, raises BudgetExceeded once more tasks than that
+    would be expanded."""
     L = lib()
+    L.qo_set_task_budget(C.c_int64(int(max_tasks)))
     off, adj = np.ascontiguousarray(g.off, np.int64), np.ascontiguousarray(g.adj, np.int32)
     off2, adj2 = np.ascontiguousarray(g.off2, np.int64), np.ascontiguousarray(g.adj2, np.int32)
     ns, ni = C.c_int64(), C.c_int64()
@@ -112,6 +120,10 @@ def mine(g, gamma, min_size, mode="clean"):
     rc = L.qo_mine(int(g.n), _p64(off), _p32(adj), _p64(off2), _p32(adj2), float(gamma),
                    int(min_size), _MODES[mode], C.byref(ns), C.byref(ni), C.byref(buf),
                    C.byref(st))
+    L.qo_set_task_budget(C.c_int64(0))
+    if rc == -2:
+        _take(buf, ni.value)
+        raise BudgetExceeded("more than %d tasks" % max_tasks)
     if rc != 0:
         raise RuntimeError("oracle enumeration failed")
     return _take(buf, ni.value), st.as_dict()
@@ -138,8 +150,8 @@ def result_text(sets):
     return "".join("%d " % len(s) + "".join("%d " % v for v in s) + "\n" for s in sets)
 
 
-def solve(g, gamma, min_size, mode="clean"):
-    flat, st = mine(g, gamma, min_size, mode)
+def solve(g, gamma, min_size, mode="clean", max_tasks=0):
+    flat, st = mine(g, gamma, min_size, mode, max_tasks)
     return maximal(flat), st
 
 

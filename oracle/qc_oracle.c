@@ -828,6 +828,12 @@ static void ctx_free(qo_ctx* c)
     free(c->tmpv);
 }
 
+/* Optional bound on the tasks one qo_mine call may expand (0: none).  A call
+ * that would exceed it stops and returns -2; used to screen generated
+ * instances by search-tree size. */
+static int64_t g_task_budget = 0;
+void qo_set_task_budget(int64_t tasks) { g_task_budget = tasks > 0 ? tasks : 0; }
+
 /* Enumerate every quasi-clique the reference's rules emit (maximal or not).
  * Output: out_buf = [k, id_1..id_k, k, ...] (caller frees with qo_free). */
 int qo_mine(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
@@ -891,6 +897,10 @@ int qo_mine(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
         c.lane0_quirk = (mode == QO_BINARY);
         if (!c.host_rules) map_clear_all(&c);
         while (s.nt > 0 && !c.err) {
+            if (g_task_budget && c.st.tasks > g_task_budget) {
+                c.err = 2;
+                break;
+            }
             int64_t a = s.toff[--s.nt];
             int k = (int)(s.n - a);
             memcpy(cur, s.v + a, sizeof(qo_vtx) * (size_t)k);
@@ -915,7 +925,7 @@ int qo_mine(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
     free(vs); free(cur); free(w);
     free(s.v);
     free(s.toff);
-    return err ? -1 : 0;
+    return err == 2 ? -2 : (err ? -1 : 0);
 }
 
 void qo_free(void* p) { free(p); }
