@@ -576,19 +576,23 @@ __device__ __forceinline__ unsigned long long now_ns()
     return t;
 }
 
-// lane-0 only
-__device__ bool push_item(const ExpandParams& P, WorkItem it)
+// the shard a warp pushes to and starts its scans from
+__device__ __forceinline__ int home_shard() { return (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % kStackShards); }
+
+// lane-0 only: one entry onto shard `shard` of the shared stack
+__device__ bool push_entry(const ExpandParams& P, const StackEntry& e, int shard)
 {
     atomicAdd(&P.ctl->pending, 1);
-    int idx = atomicAdd(&P.ctl->stack_top, 1);
+    int idx = atomicAdd(&P.ctl->stack_top[shard], 1);
     if (idx >= P.ctl->stack_cap) {
         set_status(P, ST_TASK_OVERFLOW);
         atomicSub(&P.ctl->pending, 1);
         return false;
     }
+    long long at = (long long)shard * P.ctl->stack_cap + idx;
     unsigned long long t0 = now_ns();
     unsigned spins = 0;
-    while (atomicCAS(&P.slot[idx], 0, 2) != 0) {
+    while (atomicCAS(&P.slot[at], 0, 2) != 0) {
         if ((++spins & 255u) == 0) {
             if (now_ns() - t0 > (unsigned long long)P.wait_ns || P.ctl->status) {
                 set_status(P, ST_ITER_LIMIT);
@@ -598,94 +602,191 @@ __device__ bool push_item(const ExpandParams& P, WorkItem it)
         }
         __nanosleep(64);
     }
-    P.stack[idx] = it;
+    P.stack[at] = e;
     __threadfence();
-    atomicExch(&P.slot[idx], 1);
+    atomicExch(&P.slot[at], 1);
     return true;
 }
 
-// lane-0 only; returns 1 item, 0 empty-and-done, -1 error/abort
-__device__ int pop_item(const ExpandParams& P, WorkItem& out)
+__device__ bool push_item(const ExpandParams& P, const WorkItem& it)
 {
+    StackEntry e;
+    for (int i = 0; i < kBundle; i++) e.rec[i] = 0;
+    e.rec[0] = it.rec;
+    e.n = 1;
+    e.q_lo = it.q_lo;
+    e.q_hi = it.q_hi;
+    e.pad = 0;
+    return push_entry(P, e, home_shard());
+}
+
+// lane 0: read the entry at position idx of shard s once its writer is done
+__device__ int take_slot(const ExpandParams& P, int s, int idx, StackEntry& out)
+{
+    // a failed push (shard full) leaves the top above the capacity; such an
+    // index has no slot behind it
+    if (idx >= P.ctl->stack_cap) {
+        set_status(P, ST_TASK_OVERFLOW);
+        return -1;
+    }
+    long long at = (long long)s * P.ctl->stack_cap + idx;
+    unsigned long long t1 = now_ns();
+    unsigned s2 = 0;
+    while (atomicCAS(&P.slot[at], 1, 3) != 1) {
+        if ((++s2 & 255u) == 0 && now_ns() - t1 > (unsigned long long)P.wait_ns) {
+            set_status(P, ST_ITER_LIMIT);
+            P.ctl->wait_fail_where = 2;
+            return -1;
+        }
+        __nanosleep(32);
+    }
+    __threadfence();
+    const volatile StackEntry* src = &P.stack[at];
+    out.n = src->n;
+    out.q_lo = src->q_lo;
+    out.q_hi = src->q_hi;
+    for (int i = 0; i < kBundle; i++) out.rec[i] = src->rec[i];
+    __threadfence();
+    atomicExch(&P.slot[at], 0);
+    return 1;
+}
+
+// Whole warp: take one entry from the shared stack.  The lanes read all
+// shard tops in one coalesced load and lane 0 claims the first non-empty
+// shard at or after the warp's home shard.  Returns (in every lane) 1 with
+// the entry in lane 0's `out`, 0 when the stack is empty and no warp holds
+// work, -1 on error or abort.
+__device__ int pop_shared(const ExpandParams& P, StackEntry& out)
+{
+    const int lane = lane_id();
+    const int home = home_shard();
     unsigned long long t0 = now_ns();
     unsigned spins = 0;
     unsigned backoff = 64;
     int last_pending = -1;
     for (;;) {
-        if (*(volatile int*)&P.ctl->status) return -1;
-        if (P.deadline_ns && now_ns() > P.deadline_ns) {
-            set_status(P, ST_DEADLINE);
-            return -1;
-        }
-        int top = *(volatile int*)&P.ctl->stack_top;
-        if (top > 0) {
-            if (atomicCAS(&P.ctl->stack_top, top, top - 1) == top) {
-                int idx = top - 1;
-                // a failed push (stack full) leaves stack_top above the
-                // capacity; such an index has no slot behind it
-                if (idx >= P.ctl->stack_cap) {
-                    set_status(P, ST_TASK_OVERFLOW);
-                    return -1;
-                }
-                unsigned long long t1 = now_ns();
-                unsigned s2 = 0;
-                while (atomicCAS(&P.slot[idx], 1, 3) != 1) {
-                    if ((++s2 & 255u) == 0 && now_ns() - t1 > (unsigned long long)P.wait_ns) {
-                        set_status(P, ST_ITER_LIMIT);
-                        P.ctl->wait_fail_where = 2;
-                        return -1;
-                    }
-                    __nanosleep(32);
-                }
-                __threadfence();
-                const volatile WorkItem* src = &P.stack[idx];
-                out.rec = src->rec;
-                out.q_lo = src->q_lo;
-                out.q_hi = src->q_hi;
-                __threadfence();
-                atomicExch(&P.slot[idx], 0);
-                return 1;
+        int act = 0;
+        if (lane == 0) {
+            if (*(volatile int*)&P.ctl->status) act = -1;
+            else if (P.deadline_ns && now_ns() > P.deadline_ns) {
+                set_status(P, ST_DEADLINE);
+                act = -1;
             }
-            // lost the race for the top: wait a short, warp-dependent time so
+        }
+        if (__shfl_sync(QC_FULL, act, 0) < 0) return -1;
+        int top = *(volatile int*)&P.ctl->stack_top[lane];
+        unsigned ne = __ballot_sync(QC_FULL, top > 0);
+        if (ne) {
+            unsigned rot = home ? ((ne >> home) | (ne << (32 - home))) : ne;
+            int s = (home + __ffs(rot) - 1) & 31;
+            int ts = __shfl_sync(QC_FULL, top, s);
+            int got = 0;
+            if (lane == 0 && atomicCAS(&P.ctl->stack_top[s], ts, ts - 1) == ts)
+                got = take_slot(P, s, ts - 1, out);
+            got = __shfl_sync(QC_FULL, got, 0);
+            if (got != 0) return got;
+            // lost the race for that top: wait a short, warp-dependent time so
             // the losers do not retry in lock step
             unsigned jitter = (unsigned)((blockIdx.x * 37u + (threadIdx.x >> 5) * 11u + spins) & 255u);
             __nanosleep(32 + jitter);
             spins++;
             continue;
         }
-        int pend = *(volatile int*)&P.ctl->pending;
-        if (pend == 0) return 0;
-        if (pend != last_pending) {
-            last_pending = pend;
-            t0 = now_ns();
+        int done = 0;
+        if (lane == 0) {
+            int pend = *(volatile int*)&P.ctl->pending;
+            if (pend == 0) done = 1;
+            else {
+                if (pend != last_pending) {
+                    last_pending = pend;
+                    t0 = now_ns();
+                }
+                if ((++spins & 15u) == 0 && now_ns() - t0 > (unsigned long long)P.wait_ns) {
+                    set_status(P, ST_ITER_LIMIT);
+                    P.ctl->wait_fail_where = 3;
+                    done = -1;
+                }
+            }
         }
-        if ((++spins & 15u) == 0 && now_ns() - t0 > (unsigned long long)P.wait_ns) {
-            set_status(P, ST_ITER_LIMIT);
-            P.ctl->wait_fail_where = 3;
-            return -1;
-        }
+        done = __shfl_sync(QC_FULL, done, 0);
+        if (done == 1) return 0;
+        if (done < 0) return -1;
         // idle: back off (64 ns doubling to ~4 us) so waiting warps leave the
-        // issue slots and the stack's cache line to the working ones
+        // issue slots and the tops' cache line to the working ones
         __nanosleep(backoff);
         backoff = backoff < 4096 ? backoff * 2 : 4096;
     }
 }
 
+// Whole warp.  While it waits the warp is counted in `idle_warps`, which
+// busy warps read to decide whether to donate.  The first task of a popped
+// bundle becomes the warp's item (in lane 0), the others go on its own stack
+// (it holds no work when it pops, so they fit).
+__device__ int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out)
+{
+    const int lane = lane_id();
+    if (lane == 0) atomicAdd(&P.ctl->idle_warps, 1);
+    StackEntry e;
+    int r = pop_shared(P, e);
+    if (lane == 0) {
+        atomicSub(&P.ctl->idle_warps, 1);
+        if (r > 0) {
+            if (e.n < 1 || e.n > kBundle || (e.n > 1 && e.q_lo >= 0)) {
+                check_fail(P, 16, (unsigned long long)e.n); // a malformed stack entry
+                r = -1;
+            } else {
+                out.rec = e.rec[0];
+                out.q_lo = e.q_lo;
+                out.q_hi = e.q_hi;
+                for (int i = e.n - 1; i >= 1 && ws.sm->lcount < kLocalStack; i--)
+                    ws.sm->lstack[ws.sm->lcount++] = e.rec[i];
+            }
+        }
+    }
+    return __shfl_sync(QC_FULL, r, 0);
+}
 
-
-// lane 0: hand a freshly written child to the scheduler.  The first child a
-// warp creates while it holds none is kept and run next by the same warp
-// (no trip through the shared stack); the others are pushed for any warp.
-// A kept child takes over the outstanding-work count of the item that made
-// it (the warp does not decrement `pending` when it finishes that item).
+// lane 0: hand a freshly written child to the scheduler.  Children go to the
+// warp's own stack in shared memory (run depth first by this warp, no
+// atomics); only when that stack is full does a child go to the shared one.
+// `pending` counts shared-stack items plus warps that hold work, so local
+// children change it only when they are donated (push_item).
 __device__ void schedule_child(const ExpandParams& P, Ws& ws, const WorkItem& it)
 {
-    if (!ws.sm->kept_set) {
-        ws.sm->kept_rec = it.rec;
-        ws.sm->kept_set = 1;
+    if (ws.sm->lcount < kLocalStack) {
+        ws.sm->lstack[ws.sm->lcount++] = it.rec;
         return;
     }
     push_item(P, it);
+}
+
+// lane 0: while other warps wait for work, hand them all but the newest task
+// of this warp's own stack, oldest (shallowest, usually largest) first, in
+// bundles sized so each waiting warp can take one.
+__device__ void donate(const ExpandParams& P, Ws& ws)
+{
+    int n = ws.sm->lcount;
+    if (n < 2) return;
+    int hungry = *(volatile int*)&P.ctl->idle_warps;
+    if (hungry <= 0) return;
+    int give = n - 1;
+    int per = (give + hungry - 1) / hungry;
+    per = per < 1 ? 1 : (per > kBundle ? kBundle : per);
+    int given = 0;
+    const int home = home_shard();
+    for (int pushes = 0; given < give && pushes < 8; pushes++) {
+        int k = give - given < per ? give - given : per;
+        StackEntry e;
+        for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[given + i] : 0ull;
+        e.n = k;
+        e.q_lo = -1;
+        e.q_hi = -1;
+        e.pad = 0;
+        if (!push_entry(P, e, home)) break;
+        given += k;
+    }
+    for (int i = given; i < n; i++) ws.sm->lstack[i - given] = ws.sm->lstack[i];
+    ws.sm->lcount = n - given;
 }
 
 // ------------------------------------------------------------------
@@ -1650,7 +1751,7 @@ __global__ void expand_kernel(ExpandParams P)
     WarpSmem* sm = (WarpSmem*)dyn_smem() + (threadIdx.x >> 5);
     Ws ws = ws_view(P, warp_global, sm);
     if (lane == 0) {
-        sm->kept_set = 0;
+        sm->lcount = 0;
         sm->tab_inst = -1;
         sm->cnt = WarpCount{};
     }
@@ -1663,18 +1764,20 @@ __global__ void expand_kernel(ExpandParams P)
         WorkItem it;
         TaskHdr hv{};
         int r = 0;
-        if (lane == 0) {
-            if (sm->kept_set) {
-                it.rec = sm->kept_rec;
+        int local = 0;
+        if (lane == 0) local = sm->lcount > 0;
+        if (__shfl_sync(QC_FULL, local, 0)) {
+            if (lane == 0) {
+                donate(P, ws);
+                it.rec = sm->lstack[--sm->lcount];
                 it.q_lo = -1;
                 it.q_hi = -1;
-                sm->kept_set = 0;
                 r = 1;
-            } else {
-                r = pop_item(P, it);
             }
-            if (r > 0 && !item_ok(P, it, hv)) r = -1;
+        } else {
+            r = pop_item(P, ws, it);
         }
+        if (lane == 0 && r > 0 && !item_ok(P, it, hv)) r = -1;
         r = __shfl_sync(QC_FULL, r, 0);
         if (r <= 0) break;
         it.rec = __shfl_sync(QC_FULL, it.rec, 0);
@@ -1691,8 +1794,8 @@ __global__ void expand_kernel(ExpandParams P)
         __threadfence();
         if (lane == 0) {
             release_record(P, ws, it.rec, !shared, hv);
-            // a kept child inherits this item's outstanding-work count
-            if (!sm->kept_set) atomicSub(&P.ctl->pending, 1);
+            // the warp stays counted in `pending` while its own stack holds work
+            if (sm->lcount == 0) atomicSub(&P.ctl->pending, 1);
         }
     }
     if (lane == 0) {

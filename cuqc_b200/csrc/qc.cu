@@ -312,6 +312,14 @@ template <class T> cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaSt
 
 } // namespace
 
+// entries on the fullest shard of the shared stack
+static int max_top(const Control& ctl)
+{
+    int m = 0;
+    for (int i = 0; i < kStackShards; i++) m = std::max(m, ctl.stack_top[i]);
+    return m;
+}
+
 static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
                           qc_result* r)
 {
@@ -367,7 +375,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     std::vector<int32_t> flat;
     for (int attempt = 0;; attempt++) {
         CK(c->arena.ensure((size_t)c->arena_bytes));
-        CK(c->stack.ensure(sizeof(WorkItem) * (size_t)c->stack_slots));
+        c->stack_slots = std::max<int64_t>(c->stack_slots, 2 * kStackShards);
+        CK(c->stack.ensure(sizeof(StackEntry) * (size_t)c->stack_slots));
         CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
         CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
         const int64_t set_cap = std::max<int64_t>(c->result_ints / 4, 1024);
@@ -412,11 +421,15 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         ctl.arena_cap = (unsigned long long)c->arena_bytes;
         ctl.result_cap = (unsigned long long)c->result_ints;
         ctl.set_cap = (unsigned long long)set_cap;
-        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots, INT32_MAX);
-        ctl.stack_top = 1;
+        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots / kStackShards, INT32_MAX);
+        ctl.stack_top[0] = 1;
         ctl.pending = 1;
         CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
-        WorkItem root{0, -1, -1};
+        StackEntry root{};
+        root.rec[0] = 0;
+        root.n = 1;
+        root.q_lo = -1;
+        root.q_hi = -1;
         CK(cudaMemcpyAsync(c->stack.p, &root, sizeof(root), cudaMemcpyHostToDevice, s));
         int one = 1;
         CK(cudaMemcpyAsync(c->slot.p, &one, sizeof(one), cudaMemcpyHostToDevice, s));
@@ -437,7 +450,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.nrules = 1;
         P.ctl = c->ctl.as<Control>();
         P.arena = c->arena.as<char>();
-        P.stack = c->stack.as<WorkItem>();
+        P.stack = c->stack.as<StackEntry>();
         P.slot = c->slot.as<int32_t>();
         P.results = c->results.as<int32_t>();
         P.set_starts = c->starts.as<unsigned long long>();
@@ -467,8 +480,9 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
 
         if (ctl.status & ST_TASK_OVERFLOW) {
             if (ctl.arena_top > ctl.arena_cap) c->arena_bytes *= 4;
-            if (ctl.stack_top >= ctl.stack_cap) c->stack_slots *= 4;
-            if (ctl.arena_top <= ctl.arena_cap && ctl.stack_top < ctl.stack_cap) {
+            const bool stack_full = max_top(ctl) >= ctl.stack_cap;
+            if (stack_full) c->stack_slots *= 4;
+            if (ctl.arena_top <= ctl.arena_cap && !stack_full) {
                 c->arena_bytes *= 2;
                 c->stack_slots *= 2;
             }
@@ -493,7 +507,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
                             std::to_string(ctl.emitted) + " emitted sets, " +
                             std::to_string(ctl.result_top) + " result ints, " +
                             std::to_string(ctl.arena_top) + " arena bytes, stack " +
-                            std::to_string(ctl.stack_top) + ", max task " +
+                            std::to_string(max_top(ctl)) + " on the fullest stack shard, max task " +
                             std::to_string(ctl.max_task));
         if (ctl.status & ST_ITER_LIMIT)
             return fail(QC_ERR_ITER_LIMIT, "device wait gave up (site " +
@@ -779,9 +793,10 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     float kms = 0;
     for (int attempt = 0;; attempt++) {
         if ((int64_t)arena_at * 2 > c->arena_bytes) c->arena_bytes = (int64_t)arena_at * 2;
-        c->stack_slots = std::max<int64_t>(c->stack_slots, (int64_t)nroots * 2);
+        c->stack_slots = std::max<int64_t>(c->stack_slots, (int64_t)nroots * 2 + 64 * kStackShards);
         CK(c->arena.ensure((size_t)c->arena_bytes));
-        CK(c->stack.ensure(sizeof(WorkItem) * (size_t)c->stack_slots));
+        c->stack_slots = std::max<int64_t>(c->stack_slots, 2 * kStackShards);
+        CK(c->stack.ensure(sizeof(StackEntry) * (size_t)c->stack_slots));
         CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
         CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
         const int64_t set_cap = std::max<int64_t>(c->result_ints / 4, 1024);
@@ -808,23 +823,42 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         ctl.arena_cap = (unsigned long long)c->arena_bytes;
         ctl.result_cap = (unsigned long long)c->result_ints;
         ctl.set_cap = (unsigned long long)set_cap;
-        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots, INT32_MAX);
-        ctl.stack_top = nroots;
+        // roots dealt round-robin over the stack shards: root j is entry j / S
+        // of shard j % S, so every shard's entries are contiguous
+        const int64_t per_shard = c->stack_slots / kStackShards;
+        ctl.stack_cap = (int)std::min<int64_t>(per_shard, INT32_MAX);
         ctl.pending = nroots;
-        CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
-        std::vector<WorkItem> items((size_t)nroots);
-        for (int j = 0; j < nroots; j++) items[(size_t)j] = WorkItem{meta[(size_t)j].rec, -1, -1};
+        std::vector<StackEntry> items((size_t)nroots);
         std::vector<int32_t> ones((size_t)nroots, 1);
-        CK(cudaMemcpyAsync(c->stack.p, items.data(), sizeof(WorkItem) * nroots,
-                           cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(c->slot.p, ones.data(), sizeof(int32_t) * nroots,
-                           cudaMemcpyHostToDevice, s));
+        int64_t filled = 0;
+        for (int sh = 0; sh < kStackShards; sh++) {
+            int cnt = 0;
+            for (int j = sh; j < nroots; j += kStackShards) {
+                StackEntry e{};
+                e.rec[0] = meta[(size_t)j].rec;
+                e.n = 1;
+                e.q_lo = -1;
+                e.q_hi = -1;
+                items[(size_t)(filled + cnt)] = e;
+                cnt++;
+            }
+            ctl.stack_top[sh] = cnt;
+            if (cnt > 0) {
+                CK(cudaMemcpyAsync(c->stack.as<StackEntry>() + (size_t)sh * per_shard,
+                                   items.data() + filled, sizeof(StackEntry) * cnt,
+                                   cudaMemcpyHostToDevice, s));
+                CK(cudaMemcpyAsync(c->slot.as<int32_t>() + (size_t)sh * per_shard, ones.data(),
+                                   sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, s));
+            }
+            filled += cnt;
+        }
+        CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
         ExpandParams P{};
         P.rules = B.rules.as<Rules>();
         P.nrules = count;
         P.ctl = c->ctl.as<Control>();
         P.arena = c->arena.as<char>();
-        P.stack = c->stack.as<WorkItem>();
+        P.stack = c->stack.as<StackEntry>();
         P.slot = c->slot.as<int32_t>();
         P.results = c->results.as<int32_t>();
         P.set_starts = c->starts.as<unsigned long long>();
@@ -851,8 +885,9 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
         if (ctl.status & ST_TASK_OVERFLOW) {
             if (ctl.arena_top > ctl.arena_cap) c->arena_bytes *= 4;
-            if (ctl.stack_top >= ctl.stack_cap) c->stack_slots *= 4;
-            if (ctl.arena_top <= ctl.arena_cap && ctl.stack_top < ctl.stack_cap) {
+            const bool stack_full = max_top(ctl) >= ctl.stack_cap;
+            if (stack_full) c->stack_slots *= 4;
+            if (ctl.arena_top <= ctl.arena_cap && !stack_full) {
                 c->arena_bytes *= 2;
                 c->stack_slots *= 2;
             }

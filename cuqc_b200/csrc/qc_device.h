@@ -26,6 +26,7 @@ __host__ __device__ inline int clz64(unsigned long long x)
 }
 
 constexpr int kWarp = 32;
+constexpr int kStackShards = 32;       // shared-stack shards (one per lane of a scanning warp)
 constexpr int kArenaClasses = 4 * 40; // arena size classes (see arena_class)
 constexpr int kArenaShards = 32;       // free lists per class, selected by block
 
@@ -46,9 +47,10 @@ struct Control {
     unsigned long long result_top; // ints of emitted sets written
     unsigned long long result_cap;
     unsigned long long set_cap;    // capacity of the set-start array
-    int stack_top;
-    int stack_cap;
-    int pending;                   // work items pushed and not yet finished
+    int stack_top[kStackShards];   // entries on each shard of the shared stack
+    int stack_cap;                 // slots per shard; shard s owns slots [s*cap, (s+1)*cap)
+    int pending;                   // items on the shared stack + warps holding work
+    int idle_warps;                // warps looking for work on the shared stack
     int status;
     unsigned long long tasks, branches, children, emitted;
     unsigned long long lookahead_hits;
@@ -65,6 +67,18 @@ struct WorkItem {
     unsigned long long rec; // byte offset of the task record in the arena
     int q_lo;               // first branch position, -1: fresh task
     int q_hi;               // last branch position (inclusive)
+};
+
+// One slot of the shared stack: a branch range of one task, or a bundle of
+// up to kBundle fresh tasks that a busy warp donated at once (a warp that
+// takes it runs the first and keeps the rest on its own stack).
+constexpr int kBundle = 6;
+struct StackEntry {
+    unsigned long long rec[kBundle];
+    int32_t n;    // records in the entry, 1..kBundle
+    int32_t q_lo; // with n == 1: branch range, q_lo = -1 for a fresh task
+    int32_t q_hi;
+    int32_t pad;
 };
 
 // Task record header; the record continues with
@@ -136,7 +150,7 @@ struct ExpandParams {
     int32_t nrules;
     Control* ctl;
     char* arena;
-    WorkItem* stack;
+    StackEntry* stack;
     int32_t* slot;       // 0 free, 1 full, 2 being written, 3 being read
     int32_t* results;
     unsigned long long* set_starts; // start offset (in results) of every emitted set
@@ -166,11 +180,15 @@ constexpr int kPrivateFreeCap = 64;
 // tests of tasks up to this size never look further.
 constexpr int kTabCache = 128;
 
+// Fresh child tasks a warp keeps on its own stack (run depth first by the
+// warp itself) before it pushes further children to the shared stack.
+constexpr int kLocalStack = 48;
+
 // Per-warp state in shared memory: everything a warp touches on every task.
 struct WarpSmem {
     WarpCount cnt;
-    unsigned long long kept_rec; // a child this warp runs next instead of pushing it
-    int32_t kept_set;            // 1 while kept_rec holds one
+    unsigned long long lstack[kLocalStack]; // this warp's own fresh child tasks (record offsets)
+    int32_t lcount;                          // entries on lstack
     int32_t tab_inst;            // instance whose gamma tables are cached (-1: none)
     unsigned long long fhead[kArenaClasses]; // private free lists: offset/16+1, 0 = empty
     int32_t fcount[kArenaClasses];

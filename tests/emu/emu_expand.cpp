@@ -18,6 +18,15 @@ using namespace qcb;
 // kernel's deadline drain
 static long long g_emu_time_limit_ms = 0;
 extern "C" void emu_set_time_limit_ms(long long ms) { g_emu_time_limit_ms = ms; }
+static StackEntry one_entry(unsigned long long rec)
+{
+    StackEntry e{};
+    e.rec[0] = rec;
+    e.n = 1;
+    e.q_lo = -1;
+    e.q_hi = -1;
+    return e;
+}
 static unsigned long long emu_deadline()
 {
     return g_emu_time_limit_ms > 0 ? emu_globaltimer() + (unsigned long long)g_emu_time_limit_ms * 1000000ull : 0ull;
@@ -80,12 +89,13 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     ctl.arena_cap = (unsigned long long)arena_bytes;
     ctl.result_cap = result_cap > 0 ? (unsigned long long)result_cap : (1ull << 24);
     ctl.set_cap = ctl.result_cap / 2 + 1;
-    ctl.stack_cap = stack_cap > 0 ? stack_cap : (1 << 20);
-    ctl.stack_top = 1;
+    const int total_slots = std::max(stack_cap > 0 ? stack_cap : (1 << 20), 2 * kStackShards);
+    ctl.stack_cap = total_slots / kStackShards;
+    ctl.stack_top[0] = 1;
     ctl.pending = 1;
-    std::vector<WorkItem> stack((size_t)ctl.stack_cap);
-    std::vector<int32_t> slot((size_t)ctl.stack_cap, 0);
-    stack[0] = WorkItem{0, -1, -1};
+    std::vector<StackEntry> stack((size_t)total_slots);
+    std::vector<int32_t> slot((size_t)total_slots, 0);
+    stack[0] = one_entry(0);
     slot[0] = 1;
     std::vector<int32_t> results((size_t)ctl.result_cap);
     std::vector<unsigned long long> set_starts((size_t)ctl.set_cap);
@@ -153,7 +163,7 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     std::vector<int64_t> off_at((size_t)count), adj_at((size_t)count), adj2_at((size_t)count);
     std::vector<char> arena((size_t)1 << 27, 0);
     uint64_t arena_at = 0;
-    std::vector<WorkItem> items;
+    std::vector<StackEntry> items;
     int64_t oa = 0, aa = 0, a2 = 0, vb = 0;
     int max_t = 1;
     for (int i = 0; i < count; i++) {
@@ -196,7 +206,7 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
                     if (p >= 0) A2[(int64_t)k * W + (p >> 5)] |= 1u << (p & 31);
                 }
             }
-            items.push_back(WorkItem{arena_at, -1, -1});
+            items.push_back(one_entry(arena_at));
             arena_at += arena_class_bytes(cls);
             max_t = std::max(max_t, t);
         }
@@ -210,12 +220,17 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     ctl.arena_cap = arena.size();
     ctl.result_cap = 1ull << 24;
     ctl.set_cap = 1ull << 22;
-    ctl.stack_cap = 1 << 20;
-    ctl.stack_top = (int)items.size();
+    ctl.stack_cap = (1 << 20) / kStackShards;
     ctl.pending = (int)items.size();
-    std::vector<WorkItem> stack((size_t)ctl.stack_cap);
-    std::vector<int32_t> slot((size_t)ctl.stack_cap, 0);
-    for (size_t j = 0; j < items.size(); j++) { stack[j] = items[j]; slot[j] = 1; }
+    std::vector<StackEntry> stack((size_t)ctl.stack_cap * kStackShards);
+    std::vector<int32_t> slot(stack.size(), 0);
+    // item j is entry j / S of shard j % S, as the library seeds a batch
+    for (size_t j = 0; j < items.size(); j++) {
+        size_t at = (j % kStackShards) * (size_t)ctl.stack_cap + j / kStackShards;
+        stack[at] = items[j];
+        slot[at] = 1;
+        ctl.stack_top[j % kStackShards]++;
+    }
     std::vector<int32_t> results((size_t)ctl.result_cap);
     std::vector<unsigned long long> set_starts((size_t)ctl.set_cap);
     WsLayout L = ws_layout(max_t);
