@@ -13,7 +13,6 @@ from __future__ import annotations
 import ctypes as C
 import os
 import subprocess
-from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -192,21 +191,33 @@ class DeviceGraph:
             pass
 
 
-@dataclass
 class Result:
-    sets: list
-    stats: dict
-    emitted: np.ndarray = field(default=None)
+    """A mining result: the maximal sets (flat [k, ids..] as returned by the
+    library; `sets` converts them to sorted tuples on first use), the run's
+    counters and, with keep_emitted, the raw emitted multiset."""
+
+    def __init__(self, flat, stats, emitted=None):
+        self.flat = flat
+        self.stats = stats
+        self.emitted = emitted
+        self._sets = None
+
+    @property
+    def sets(self):
+        if self._sets is None:
+            self._sets = _flat_to_sets(self.flat)
+        return self._sets
 
     def text(self):
         return "".join("%d " % len(s) + "".join("%d " % v for v in s) + "\n" for s in self.sets)
 
 
 def _flat_to_sets(flat):
+    vals = flat.tolist()
     out, p = [], 0
-    while p < len(flat):
-        k = int(flat[p])
-        out.append(tuple(int(x) for x in flat[p + 1:p + 1 + k]))
+    while p < len(vals):
+        k = vals[p]
+        out.append(tuple(vals[p + 1:p + 1 + k]))
         p += 1 + k
     return out
 
@@ -238,7 +249,7 @@ class Context:
                 pe = L.qc_result_emitted(r, C.byref(ns), C.byref(ni))
                 emitted = (np.ctypeslib.as_array(pe, shape=(ni.value,)).copy() if ni.value
                            else np.zeros(0, np.int32))
-            return Result(sets=_flat_to_sets(flat), stats=st, emitted=emitted)
+            return Result(flat, st, emitted)
         finally:
             L.qc_result_free(r)
 
