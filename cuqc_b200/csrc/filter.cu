@@ -7,11 +7,13 @@
 //      hash the set (sum of per-id 64-bit mixes, plus its size);
 //   2. radix-sort (hash, set) and drop exact duplicates (equal hash and equal
 //      contents; a hash collision with different contents keeps both);
-//   3. inverted index over the distinct sets: a counting sort of
-//      (vertex, set) incidences gives every vertex its posting list;
+//   3. inverted index over the distinct sets: the (vertex, set) incidences,
+//      radix-sorted by vertex and, within a vertex, by set size descending,
+//      give every vertex its posting list with the largest sets first;
 //   4. one warp per distinct set S: scan the posting list of S's rarest
-//      vertex and test S against every longer set T in it by a sorted merge;
-//      S is maximal iff no such T contains it;
+//      vertex while its sets are larger than S and test S against each by a
+//      sorted merge (largest first, so a non-maximal S usually stops early);
+//      S is maximal iff no such set contains it;
 //   5. the maximal sets are compacted and copied back; the host orders them
 //      lexicographically (the order the reference's prefix tree writes).
 #include <cuda_runtime.h>
@@ -111,9 +113,26 @@ __global__ void dedupe_kernel(const int32_t* srt, const unsigned long long* star
     keep[osorted[i]] = dup ? 0 : 1;
 }
 
-// 3a. incidence counts per vertex over kept sets
-__global__ void count_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
-                             const uint8_t* keep, int32_t* cnt)
+// incidence key: vertex in the high bits, then the set's size descending
+__device__ __forceinline__ unsigned long long inc_key(int v, int k)
+{
+    return ((unsigned long long)(unsigned)v << 16) | (unsigned long long)(0xffff - (k < 0xffff ? k : 0xffff));
+}
+__device__ __forceinline__ int inc_size(unsigned long long key) { return 0xffff - (int)(key & 0xffffull); }
+
+// 3a. incidences per kept set
+__global__ void inc_len_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
+                               const uint8_t* keep, int64_t* len)
+{
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsets) return;
+    len[s] = keep[s] ? (int64_t)srt[starts[s]] : 0;
+}
+
+// 3b. (vertex, size) keys and set ids of every incidence, one warp per set
+__global__ void inc_emit_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
+                                const uint8_t* keep, const int64_t* pos,
+                                unsigned long long* key, int32_t* val)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -122,26 +141,28 @@ __global__ void count_kernel(const int32_t* srt, const unsigned long long* start
         if (!keep[s]) continue;
         unsigned long long a = starts[s];
         int k = srt[a];
-        for (int i = lane; i < k; i += 32) atomicAdd(&cnt[srt[a + 1 + i]], 1);
+        int64_t at = pos[s];
+        for (int i = lane; i < k; i += 32) {
+            key[at + i] = inc_key(srt[a + 1 + i], k);
+            val[at + i] = (int32_t)s;
+        }
     }
 }
 
-// 3b. scatter set ids into posting lists
-__global__ void scatter_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
-                               const uint8_t* keep, int64_t* cursor, int32_t* post)
+// 3c. start of every vertex's posting list in the sorted incidences
+__global__ void inc_offsets_kernel(const unsigned long long* key, int64_t total, int64_t nv,
+                                   int64_t* poff)
 {
-    int lane = threadIdx.x & 31;
-    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t s = warp; s < nsets; s += nw) {
-        if (!keep[s]) continue;
-        unsigned long long a = starts[s];
-        int k = srt[a];
-        for (int i = lane; i < k; i += 32) {
-            unsigned long long at = atomicAdd((unsigned long long*)&cursor[srt[a + 1 + i]], 1ull);
-            post[at] = (int32_t)s;
-        }
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v > nv) return;
+    unsigned long long want = (unsigned long long)v << 16;
+    int64_t lo = 0, hi = total; // first index with key >= want
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (key[mid] < want) lo = mid + 1;
+        else hi = mid;
     }
+    poff[v] = lo;
 }
 
 // is sorted set S (at a) a subset of sorted set T (at b)?  |T| > |S|
@@ -164,7 +185,7 @@ __device__ bool subset_of(const int32_t* srt, unsigned long long a, unsigned lon
 // 4. superset test, one warp per kept set
 __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
                                const uint8_t* keep, const int64_t* poff, const int32_t* post,
-                               uint8_t* maximal)
+                               const unsigned long long* pkey, uint8_t* maximal)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -200,11 +221,12 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
             int64_t lo = poff[best_v], hi = poff[best_v + 1];
             for (int64_t base = lo; base < hi; base += 32) {
                 int64_t e = base + lane;
-                if (e < hi) {
-                    unsigned long long b = starts[post[e]];
-                    if (srt[b] > k && subset_of(srt, a, b)) covered = true;
-                }
-                if (__any_sync(0xffffffffu, covered)) break;
+                bool larger = e < hi && inc_size(pkey[e]) > k;
+                if (larger && subset_of(srt, a, starts[post[e]])) covered = true;
+                // the list is ordered by size, largest first: past the sets
+                // larger than S nothing can contain it
+                unsigned more = __ballot_sync(0xffffffffu, larger);
+                if (__any_sync(0xffffffffu, covered) || more != 0xffffffffu) break;
             }
         }
         covered = __any_sync(0xffffffffu, covered);
@@ -262,12 +284,12 @@ std::string FilterScratch::ensure(void** p, size_t* have, size_t need)
 void FilterScratch::release()
 {
     for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &sizes, &keep, &maximal, &cnt,
-                     &poff, &cursor, &post, &len, &pos, &out, &temp}) {
+                     &poff, &cursor, &post, &len, &pos, &out, &temp, &ikey, &ikey2, &ival}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
     sorted_n = hash_n = hash2_n = order_n = order2_n = sizes_n = keep_n = maximal_n = cnt_n =
-        poff_n = cursor_n = post_n = len_n = pos_n = out_n = temp_n = 0;
+        poff_n = cursor_n = post_n = len_n = pos_n = out_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -278,6 +300,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     host_out.clear();
     host_nsets = 0;
     if (nsets == 0) return "";
+    if (nsets > INT32_MAX) return "filter: more than 2^31 emitted sets";
     std::string e;
     const int64_t nv = std::max<int64_t>(n_vertices, 1);
 #define ENS(ptr, n, bytes)                                              \
@@ -291,9 +314,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(sizes, sizes_n, sizeof(int32_t) * nsets);
     ENS(keep, keep_n, nsets);
     ENS(maximal, maximal_n, nsets);
-    ENS(cnt, cnt_n, sizeof(int32_t) * (nv + 1));
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
-    ENS(cursor, cursor_n, sizeof(int64_t) * (nv + 1));
     ENS(len, len_n, sizeof(int64_t) * nsets);
     ENS(pos, pos_n, sizeof(int64_t) * (nsets + 1));
     const int blocks = sms * 8;
@@ -305,13 +326,10 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)F.hash,
                                         (unsigned long long*)F.hash2, (int32_t*)F.order,
                                         (int32_t*)F.order2, (int)nsets, 0, 64, s));
-    size_t tb2 = 0;
-    FCK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, (int32_t*)F.cnt, (int64_t*)F.poff,
-                                      (int)(nv + 1), s));
     size_t tb3 = 0;
     FCK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, (int64_t*)F.len, (int64_t*)F.pos,
                                       (int)nsets, s));
-    ENS(temp, temp_n, std::max(tb, std::max(tb2, tb3)) + 256);
+    ENS(temp, temp_n, std::max(tb, tb3) + 256);
     tb = F.temp_n;
     FCK(cub::DeviceRadixSort::SortPairs(F.temp, tb, (unsigned long long*)F.hash,
                                         (unsigned long long*)F.hash2, (int32_t*)F.order,
@@ -319,21 +337,42 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     dedupe_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
         (int32_t*)F.sorted, d_starts, (unsigned long long*)F.hash2, (int32_t*)F.order2, nsets,
         (uint8_t*)F.keep);
-    FCK(cudaMemsetAsync(F.cnt, 0, sizeof(int32_t) * (nv + 1), s));
-    count_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
-                                        (int32_t*)F.cnt);
+    // inverted index: incidences sorted by (vertex, size descending)
+    inc_len_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
+        (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep, (int64_t*)F.len);
     tb = F.temp_n;
-    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int32_t*)F.cnt, (int64_t*)F.poff, (int)(nv + 1),
-                                      s));
-    int64_t total = 0;
-    FCK(cudaMemcpyAsync(&total, (int64_t*)F.poff + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos, (int)nsets, s));
+    int64_t ilast_pos = 0, ilast_len = 0;
+    FCK(cudaMemcpyAsync(&ilast_pos, (int64_t*)F.pos + nsets - 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s));
+    FCK(cudaMemcpyAsync(&ilast_len, (int64_t*)F.len + nsets - 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s));
     FCK(cudaStreamSynchronize(s));
+    const int64_t total = ilast_pos + ilast_len;
+    if (total > INT32_MAX) return "filter: more than 2^31 vertex incidences in the emitted sets";
+    ENS(ikey, ikey_n, sizeof(unsigned long long) * std::max<int64_t>(total, 1));
+    ENS(ikey2, ikey2_n, sizeof(unsigned long long) * std::max<int64_t>(total, 1));
+    ENS(ival, ival_n, sizeof(int32_t) * std::max<int64_t>(total, 1));
     ENS(post, post_n, sizeof(int32_t) * std::max<int64_t>(total, 1));
-    FCK(cudaMemcpyAsync(F.cursor, F.poff, sizeof(int64_t) * (nv + 1), cudaMemcpyDeviceToDevice, s));
-    scatter_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
-                                          (int64_t*)F.cursor, (int32_t*)F.post);
+    inc_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
+                                           (int64_t*)F.pos, (unsigned long long*)F.ikey,
+                                           (int32_t*)F.ival);
+    int vbits = 1;
+    while (vbits < 47 && ((int64_t)1 << vbits) <= nv) vbits++;
+    size_t tb4 = 0;
+    FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb4, (unsigned long long*)F.ikey,
+                                        (unsigned long long*)F.ikey2, (int32_t*)F.ival,
+                                        (int32_t*)F.post, (int)total, 0, 16 + vbits, s));
+    ENS(temp, temp_n, tb4 + 256);
+    tb4 = F.temp_n;
+    FCK(cub::DeviceRadixSort::SortPairs(F.temp, tb4, (unsigned long long*)F.ikey,
+                                        (unsigned long long*)F.ikey2, (int32_t*)F.ival,
+                                        (int32_t*)F.post, (int)total, 0, 16 + vbits, s));
+    inc_offsets_kernel<<<(unsigned)((nv + 1 + 255) / 256), 256, 0, s>>>(
+        (unsigned long long*)F.ikey2, total, nv, (int64_t*)F.poff);
     maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
-                                          (int64_t*)F.poff, (int32_t*)F.post, (uint8_t*)F.maximal);
+                                          (int64_t*)F.poff, (int32_t*)F.post,
+                                          (unsigned long long*)F.ikey2, (uint8_t*)F.maximal);
     survivor_len_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
         (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.maximal, (int64_t*)F.len);
     tb = F.temp_n;
@@ -350,7 +389,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
                                                 (uint8_t*)F.maximal, (int64_t*)F.pos,
                                                 (int32_t*)F.out);
     FCK(cudaGetLastError());
-    if (launches) *launches += 9;
+    if (launches) *launches += 8;
     std::vector<int32_t> flat((size_t)out_ints);
     if (out_ints)
         FCK(cudaMemcpyAsync(flat.data(), F.out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
