@@ -41,18 +41,23 @@ enum : int {
     ST_CHECK = 32           // a self-check caught a bad record offset or header
 };
 
+// Control block of a launch.  Words that many warps touch at once sit on
+// their own 128-byte lines, so reads of one do not queue behind atomics on
+// another.
 struct Control {
-    unsigned long long arena_top;  // bytes of records written
+    // capacities (written by the host, read-only on the device)
     unsigned long long arena_cap;
-    unsigned long long result_top; // ints of emitted sets written
     unsigned long long result_cap;
     unsigned long long set_cap;    // capacity of the set-start array
-    int stack_top[kStackShards];   // entries on each shard of the shared stack
     int stack_cap;                 // slots per shard; shard s owns slots [s*cap, (s+1)*cap)
-    int pending;                   // items on the shared stack + warps holding work
-    int idle_warps;                // warps looking for work on the shared stack
-    int status;
-    unsigned long long tasks, branches, children, emitted;
+    alignas(128) int stack_top[kStackShards]; // entries on each shard of the shared stack
+    alignas(128) int pending;      // items on the shared stack + warps holding work
+    alignas(128) int idle_warps;   // warps looking for work on the shared stack
+    alignas(128) int status;
+    alignas(128) unsigned long long arena_top; // bytes of record blocks handed out
+    alignas(128) unsigned long long result_top; // ints of emitted sets written
+    unsigned long long emitted;
+    alignas(128) unsigned long long tasks, branches, children;
     unsigned long long lookahead_hits;
     unsigned long long parent_vertices, p_rows, child_vertices;
     int max_task;
@@ -60,7 +65,7 @@ struct Control {
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
     unsigned long long check_site;      // first failed self-check: site id
     unsigned long long check_value;     //   ... and the offending value
-    unsigned long long free_head[kArenaClasses * kArenaShards]; // [tag:24 | offset/16+1:40]
+    alignas(128) unsigned long long free_head[kArenaClasses * kArenaShards]; // [tag:24 | offset/16+1:40]
 };
 
 struct WorkItem {
