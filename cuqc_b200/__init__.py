@@ -37,7 +37,7 @@ EXPORTS = [
     "qc_graph_twohop_offsets", "qc_graph_twohop_neighbors", "qc_graph_free", "qc_config_default",
     "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
-    "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices",
+    "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune",
 ]
 
 
@@ -120,6 +120,7 @@ def lib():
         L.qc_result_stats.restype = C.POINTER(Stats)
         L.qc_result_write.argtypes = [vp, C.c_char_p]
         L.qc_result_free.argtypes = [vp]
+        L.qc_tune.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.POINTER(Config)]
         L.qc_twohop_noalloc.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int64, P64, vp]
         L.qc_twohop_noalloc_max_vertices.restype = C.c_int32
         _lib = L
@@ -269,6 +270,17 @@ class Context:
         r = C.c_void_p()
         _check(lib().qc_mine(self.h, dg.h, float(gamma), int(min_size), int(sched), C.byref(r)))
         return self._result(r)
+
+    def tune(self, g, gamma, min_size, repeats=2):
+        """Pick the fastest launch shape for this device on (g, gamma,
+        min_size) and keep it for later calls; returns it as a dict."""
+        dg = g if isinstance(g, DeviceGraph) else DeviceGraph.from_graph(g)
+        best = Config()
+        _check(lib().qc_tune(self.h, dg.h, float(gamma), int(min_size), int(repeats),
+                             C.byref(best)))
+        self.cfg = best
+        return {"warps_per_block": best.warps_per_block, "blocks_per_sm": best.blocks_per_sm,
+                "split": best.split}
 
     def mine_batch(self, gs, gammas, min_sizes):
         L = lib()

@@ -458,7 +458,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.ws_stride = L.total;
         P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = t;
-        P.split = c->cfg.split > 0 ? c->cfg.split : 1;
+        P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
         P.deadline_ns = 0;
@@ -589,6 +589,60 @@ extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, i
     qc_status st = mine_one(ctx, g, gamma, min_size, r.get());
     if (st != QC_OK) return st;
     *out = r.release();
+    return QC_OK;
+}
+
+// ------------------------------------------------------------------
+// autotuning of the launch shape (in place of the reference's compile-time
+// BLOCK_SIZE / NUM_OF_BLOCKS / TASKS_PER_WARP / EXPAND_THRESHOLD #defines,
+// main.cu:21-55)
+// ------------------------------------------------------------------
+
+extern "C" qc_status qc_tune(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                             int32_t repeats, qc_config* best)
+{
+    if (!ctx || !g) return fail(QC_ERR_ARGS, "NULL argument");
+    if (!(gamma >= 0.5 && gamma <= 1.0))
+        return fail(QC_ERR_ARGS, "minimum degree ratio must be between .5 and 1 inclusive");
+    if (min_size <= 1) return fail(QC_ERR_ARGS, "minimum size must be greater than 1");
+    if (g->h.off2.size() != g->h.off.size()) return fail(QC_ERR_FORMAT, "graph has no 2-hop lists");
+    if (repeats < 1) repeats = 2;
+    static const int32_t kWpb[] = {2, 4, 8};
+    static const int32_t kBps[] = {1, 2};
+    static const int32_t kSplit[] = {1, 2, 4};
+    const qc_config keep = ctx->cfg;
+    qc_config chosen = keep;
+    double best_ms = 1e300;
+    int64_t want_sets = -1;
+    for (int32_t wpb : kWpb)
+        for (int32_t bps : kBps)
+            for (int32_t split : kSplit) {
+                ctx->cfg = keep;
+                ctx->cfg.warps_per_block = wpb;
+                ctx->cfg.blocks_per_sm = bps;
+                ctx->cfg.split = split;
+                double t = 1e300;
+                for (int32_t rep = 0; rep <= repeats; rep++) { // first run warms up
+                    qc_result r;
+                    qc_status st = mine_one(ctx, g, gamma, min_size, &r);
+                    if (st != QC_OK) {
+                        ctx->cfg = keep;
+                        return st;
+                    }
+                    if (want_sets < 0) want_sets = r.nsets;
+                    if (r.nsets != want_sets) {
+                        ctx->cfg = keep;
+                        return fail(QC_ERR_CUDA, "tuning runs disagree on the result");
+                    }
+                    if (rep > 0) t = std::min(t, r.st.kernel_ms);
+                }
+                if (t < best_ms) {
+                    best_ms = t;
+                    chosen = ctx->cfg;
+                }
+            }
+    ctx->cfg = chosen;
+    if (best) *best = chosen;
     return QC_OK;
 }
 
@@ -866,7 +920,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         P.ws_stride = L.total;
         P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = max_t;
-        P.split = c->cfg.split > 0 ? c->cfg.split : 1;
+        P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
         P.deadline_ns = 0;

@@ -119,7 +119,7 @@ typedef struct {
     int32_t keep_emitted;        /* 1: keep the raw emitted multiset in the result    */
     int32_t wait_limit_ms;       /* bound on any device wait without progress; 0: 10000 */
     int32_t time_limit_ms;       /* stop a run after this long (QC_ERR_ITER_LIMIT); 0: none */
-    int32_t split;               /* branches per work item of a task over 32 vertices; 0: 1 */
+    int32_t split;               /* branches per work item of a task over 32 vertices; 0: 2 */
     int32_t max_blocks;          /* cap on the persistent grid (share the GPU between
                                     contexts running at once); 0: every resident block */
 } qc_config;
@@ -180,6 +180,16 @@ typedef struct qc_result qc_result;
  * (main.cu:535-692, 4939-4960). */
 qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
                   int32_t sched, qc_result** out);
+
+/* Pick the launch shape (warps per block, blocks per SM, branches per work
+ * item) for this device and workload: mines (g, gamma, min_size) with every
+ * candidate shape, `repeats` timed runs each after one warm-up, keeps the
+ * fastest expansion kernel, stores it in the context's configuration and, if
+ * `best` is not NULL, copies it there.  Every run must give the same result.
+ * Replaces the reference's compile-time launch constants (BLOCK_SIZE,
+ * NUM_OF_BLOCKS, TASKS_PER_WARP, EXPAND_THRESHOLD, main.cu:21-55). */
+qc_status qc_tune(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                  int32_t repeats, qc_config* best);
 
 /* Mine `count` independent instances in one persistent launch (each with
  * its own graph, gamma and min_size).  outs[i] receives instance i's result. */

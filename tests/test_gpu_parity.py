@@ -142,3 +142,55 @@ def test_batch_with_golden_cases(ctx):
         want = open(refbin).read() if os.path.exists(refbin) else oracle.result_text(
             oracle.solve(g, float(gamma), ms)[0])
         assert r.text() == want, case["name"]
+
+
+def _digest(sets):
+    import hashlib
+    text = "".join("%d %s \n" % (len(s), " ".join(map(str, s))) for s in sets)
+    return hashlib.sha1(text.encode()).hexdigest()
+
+
+def test_batched_workload_matches_oracle_digests(ctx):
+    """The first 64 instances of the batched workload, in one launch, against
+    the oracle's result digests recorded in the manifest."""
+    import json
+    man = json.load(open(os.path.join(GOLDEN, "cfg3_batch.json")))
+    rows = man["instances"][:64]
+    inst = [graphs.batch_instance(r["i"]) for r in rows]
+    res = ctx.mine_batch([x[0] for x in inst], [float(x[1]) for x in inst], [x[2] for x in inst])
+    for r, x in zip(rows, res):
+        assert len(x.sets) == r["maximal"], r["i"]
+        assert _digest(x.sets) == r["digest"], r["i"]
+
+
+@pytest.mark.parametrize("wpb,bps,split", [(1, 1, 1), (2, 2, 3), (4, 2, 2), (8, 1, 1)])
+def test_launch_shapes_agree(wpb, bps, split):
+    """Every grid shape and work split gives the same sets and the same tree."""
+    g = graphs.erdos_renyi_planted(1000, 0.02, 5, 30, 0.95, seed=1)
+    with Q.Context(device=0, warps_per_block=wpb, blocks_per_sm=bps, split=split) as c:
+        res = c.mine(g, 0.9, 20)
+    assert len(res.sets) == 1365
+    assert res.stats["tasks"] == 36601 and res.stats["branches"] == 68682
+    assert res.sets == oracle.maximal(oracle.mine(g, 0.9, 20, "clean")[0])
+
+
+def test_time_limit_stops_cleanly_and_context_stays_usable():
+    """A run over its time limit stops with QC_ERR_ITER_LIMIT (every wait in
+    the kernel is bounded); the same context then mines normally."""
+    g, gm, ms = graphs.batch_instance(3)   # tens of millions of tasks
+    small = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
+    with Q.Context(device=0, time_limit_ms=300) as c:
+        with pytest.raises(Q.QCError) as e:
+            c.mine(g, float(gm), ms)
+        assert e.value.status == 8
+        assert c.mine(small, 0.8, 10).sets == oracle.solve(small, 0.8, 10)[0]
+
+
+def test_tune_picks_a_shape_and_keeps_results():
+    g = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
+    want = oracle.solve(g, 0.8, 10)[0]
+    with Q.Context(device=0) as c:
+        best = c.tune(g, 0.8, 10, repeats=1)
+        assert best["warps_per_block"] in (2, 4, 8) and best["blocks_per_sm"] in (1, 2)
+        assert best["split"] in (1, 2, 4)
+        assert c.mine(g, 0.8, 10).sets == want
