@@ -294,6 +294,60 @@ def run_batch(args, standalone=True):
     return out
 
 
+def run_serving(args):
+    """Serving: Poisson arrivals of mining queries, 90% drawn from the batched
+    workload's instances and 10% config-1-sized graphs (ER n=1000 + 5 planted
+    groups of 30, reseeded per query); latency p50/p99 and instances/s per rate,
+    against serial one-at-a-time launches of the same queries."""
+    import random
+
+    import cuqc_b200 as Q
+    from cuqc_b200.serve import Request, Server, run_poisson
+
+    with open(BATCH_MANIFEST) as f:
+        man = json.load(f)
+    rows = man["instances"]
+    rng = random.Random(5)
+    pool = [graphs.batch_instance(r["i"]) for r in rows[:64]]
+    big = [(graphs.erdos_renyi_planted(1000, 0.02, 5, 30, 0.95, seed=100 + j), "0.9", 20)
+           for j in range(4)]
+    n_req = args.serve_requests
+    specs = [big[rng.randrange(len(big))] if rng.random() < 0.1 else pool[rng.randrange(len(pool))]
+             for _ in range(n_req)]
+    # serial reference: one plain launch at a time, back to back
+    with Q.Context(device=0) as ctx:
+        for g, gm, ms in specs[:8]:
+            ctx.mine(g, float(gm), ms)
+        t0 = time.perf_counter()
+        alone = [ctx.mine(g, float(gm), ms).flat.tobytes() for g, gm, ms in specs]
+        serial_s = time.perf_counter() - t0
+    rates_out = []
+    srv = Server(slots=args.serve_slots)
+    try:
+        for rate in args.serve_rates:
+            reqs = [Request(graph=g, gamma=float(gm), min_size=ms, rid=i)
+                    for i, (g, gm, ms) in enumerate(specs)]
+            st = run_poisson(srv, reqs, rate=rate, seed=int(rate))
+            same = all(r.error is None and r.result.flat.tobytes() == a
+                       for r, a in zip(reqs, alone))
+            st["same_as_alone"] = same
+            rates_out.append(st)
+    finally:
+        srv.close()
+    line = {
+        "metric": "serving latency p50/p99 (ms) and instances/s under Poisson arrivals",
+        "value": rates_out[-1]["instances_per_s"], "unit": "instances/s", "n_gpus": 1,
+        "steps": len(args.serve_rates), "warmup": 8, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "cfg5", "requests_per_rate": n_req, "slots": args.serve_slots,
+                   "mix": "90% batched-workload instances (first 64 of the manifest), 10% "
+                          "config-1-sized graphs"},
+        "rates": rates_out,
+        "serial": {"instances_per_s": n_req / serial_s, "form": "one qc_mine at a time"},
+    }
+    print(json.dumps(line))
+
+
 def run_ours(args):
     import torch
 
@@ -438,15 +492,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
-                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
+                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + ["cfg5"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-instances", type=int, default=8)
     ap.add_argument("--instances", type=int, default=256, help="batched workload size")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the batched-vs-plain comparison in the default run")
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[10, 30, 100, 300, 1000])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "cfg5":
+        run_serving(args)
     elif args.workload in BATCH_WORKLOADS:
         run_batch(args)
     else:
