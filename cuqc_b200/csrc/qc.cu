@@ -18,6 +18,8 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/qc.h"
@@ -114,12 +116,21 @@ struct DevBuf {
 } // namespace
 
 struct BatchBufs {
-    DevBuf off, adj, off2, adj2, md, ubt, rules, meta, ids, pos, adj_at, adj2_at;
+    DevBuf md, ubt, rules, meta, ids, pos;
     void release()
     {
-        for (DevBuf* b : {&off, &adj, &off2, &adj2, &md, &ubt, &rules, &meta, &ids, &pos, &adj_at,
-                          &adj2_at})
-            b->release();
+        for (DevBuf* b : {&md, &ubt, &rules, &meta, &ids, &pos}) b->release();
+    }
+};
+
+// A graph's CSR and two-hop CSR on the device.
+struct ResidentGraph {
+    DevBuf off, adj, off2, adj2;
+    size_t bytes = 0;
+    uint64_t last_use = 0;
+    void release()
+    {
+        for (DevBuf* b : {&off, &adj, &off2, &adj2}) b->release();
     }
 };
 
@@ -129,10 +140,14 @@ struct qc_context {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    DevBuf off, adj, off2, adj2, pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts, rules;
+    DevBuf pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts, rules;
     FilterScratch filt;
     int32_t pos_n = 0;
-    unsigned long long resident = 0; // serial of the graph whose CSR is on the device
+    // graphs kept on the device, by graph serial; least recently used ones are
+    // dropped when their bytes exceed res_budget
+    std::unordered_map<unsigned long long, std::unique_ptr<ResidentGraph>> res;
+    size_t res_bytes = 0, res_budget = 0;
+    uint64_t use_clock = 0;
     int64_t arena_bytes = 0, stack_slots = 0, result_ints = 0;
     int64_t launches = 0;
 };
@@ -163,6 +178,9 @@ extern "C" qc_status qc_context_create(const qc_config* cfg, qc_context** out)
     c->stack_slots = c->cfg.stack_slots > 0 ? c->cfg.stack_slots : (1ll << 20);
     c->result_ints = c->cfg.result_ints > 0 ? c->cfg.result_ints : (16ll << 20);
     if (c->cfg.wait_limit_ms <= 0) c->cfg.wait_limit_ms = 10000;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    c->res_budget = total_b / 4;
     *out = c.release();
     return QC_OK;
 }
@@ -171,8 +189,9 @@ extern "C" void qc_context_free(qc_context* c)
 {
     if (!c) return;
     cudaSetDevice(c->cfg.device);
-    for (DevBuf* b : {&c->off, &c->adj, &c->off2, &c->adj2, &c->pos, &c->ids, &c->md, &c->ubt,
-                      &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts,
+    for (auto& kv : c->res) kv.second->release();
+    c->res.clear();
+    for (DevBuf* b : {&c->pos, &c->ids, &c->md, &c->ubt, &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts,
                       &c->rules})
         b->release();
     c->filt.release();
@@ -320,6 +339,50 @@ static int max_top(const Control& ctl)
     return m;
 }
 
+// Device copy of graph g, uploaded on first use and kept for later calls.
+// When the resident graphs exceed the context's budget, the least recently
+// used ones (other than g and those in `keep`) are dropped.  Also sizes the
+// vertex-position scratch for g.
+static qc_status make_resident(qc_context* c, const qc_graph* g,
+                               const std::unordered_set<unsigned long long>* keep,
+                               ResidentGraph** out)
+{
+    const HostGraph& h = g->h;
+    cudaStream_t s = c->stream;
+    auto it = c->res.find(g->serial);
+    if (it == c->res.end()) {
+        std::unique_ptr<ResidentGraph> rg(new ResidentGraph());
+        CK(upload(rg->off, h.off, s));
+        CK(upload(rg->adj, h.adj, s));
+        CK(upload(rg->off2, h.off2, s));
+        CK(upload(rg->adj2, h.adj2, s));
+        rg->bytes = rg->off.n + rg->adj.n + rg->off2.n + rg->adj2.n;
+        c->res_bytes += rg->bytes;
+        it = c->res.emplace(g->serial, std::move(rg)).first;
+        while (c->res_bytes > c->res_budget && c->res.size() > 1) {
+            auto victim = c->res.end();
+            for (auto j = c->res.begin(); j != c->res.end(); ++j) {
+                if (j->first == g->serial || (keep && keep->count(j->first))) continue;
+                if (victim == c->res.end() || j->second->last_use < victim->second->last_use)
+                    victim = j;
+            }
+            if (victim == c->res.end()) break;
+            CK(cudaStreamSynchronize(s)); // its buffers may still be read by queued work
+            c->res_bytes -= victim->second->bytes;
+            victim->second->release();
+            c->res.erase(victim);
+        }
+    }
+    it->second->last_use = ++c->use_clock;
+    if (c->pos_n < h.n || !c->pos.p) {
+        CK(c->pos.ensure(sizeof(int32_t) * (size_t)std::max(h.n, 1)));
+        CK(cudaMemsetAsync(c->pos.p, 0xff, sizeof(int32_t) * (size_t)std::max(h.n, 1), s));
+        c->pos_n = h.n;
+    }
+    *out = it->second.get();
+    return QC_OK;
+}
+
 static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
                           qc_result* r)
 {
@@ -330,8 +393,9 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
 
     // graph -> device (timed as load; skipped when already resident)
     auto t_load = clk::now();
-    if (c->resident != g->serial) {
-        qc_status us = qc_context_upload(c, g);
+    ResidentGraph* rg = nullptr;
+    {
+        qc_status us = make_resident(c, g, nullptr, &rg);
         if (us != QC_OK) return us;
     }
     r->st.load_ms = ms_since(t_load);
@@ -408,8 +472,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         root_pos_kernel<<<(t + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), t,
                                                         c->pos.as<int32_t>(), 1);
         root_rows_kernel<<<std::min(blocks * 4, (t + 7) / 8), 256, 0, s>>>(
-            c->off.as<int64_t>(), c->adj.as<int32_t>(), c->off2.as<int64_t>(),
-            c->adj2.as<int32_t>(), c->ids.as<int32_t>(), t, W, c->pos.as<int32_t>(),
+            rg->off.as<int64_t>(), rg->adj.as<int32_t>(), rg->off2.as<int64_t>(),
+            rg->adj2.as<int32_t>(), c->ids.as<int32_t>(), t, W, c->pos.as<int32_t>(),
             (uint32_t*)(rec + rec_a1_off(t)), (uint32_t*)(rec + rec_a2_off(t, W)));
         root_pos_kernel<<<(t + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), t,
                                                         c->pos.as<int32_t>(), 0);
@@ -435,8 +499,10 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaMemcpyAsync(c->slot.p, &one, sizeof(one), cudaMemcpyHostToDevice, s));
 
         Rules rule{};
-        rule.off = c->off.as<int64_t>();
-        rule.off2 = c->off2.as<int64_t>();
+        rule.off = rg->off.as<int64_t>();
+        rule.off2 = rg->off2.as<int64_t>();
+        rule.adj = rg->adj.as<int32_t>();
+        rule.adj2 = rg->adj2.as<int32_t>();
         rule.md = c->md.as<int32_t>();
         rule.ubt = c->ubt.as<int32_t>();
         rule.mdlen = (int32_t)md.size();
@@ -555,22 +621,9 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
 extern "C" qc_status qc_context_upload(qc_context* c, const qc_graph* g)
 {
     if (!c || !g) return fail(QC_ERR_ARGS, "NULL argument");
-    const HostGraph& h = g->h;
-    cudaStream_t s = c->stream;
     CK(cudaSetDevice(c->cfg.device));
-    c->resident = 0;
-    CK(upload(c->off, h.off, s));
-    CK(upload(c->adj, h.adj, s));
-    CK(upload(c->off2, h.off2, s));
-    CK(upload(c->adj2, h.adj2, s));
-    if (c->pos_n < h.n || !c->pos.p) {
-        CK(c->pos.ensure(sizeof(int32_t) * (size_t)std::max(h.n, 1)));
-        CK(cudaMemsetAsync(c->pos.p, 0xff, sizeof(int32_t) * (size_t)std::max(h.n, 1), s));
-        c->pos_n = h.n;
-    }
-    CK(cudaStreamSynchronize(s));
-    c->resident = g->serial;
-    return QC_OK;
+    ResidentGraph* rg = nullptr;
+    return make_resident(c, g, nullptr, &rg);
 }
 
 extern "C" void* qc_context_stream(qc_context* c) { return c ? (void*)c->stream : nullptr; }
@@ -692,8 +745,6 @@ __global__ void batch_root_fill_kernel(const RootMeta* meta, int nroots, const i
 // one warp per root row: set the bits of its 1-hop and 2-hop neighbours
 __global__ void batch_root_rows_kernel(const RootMeta* meta, int nroots, const int32_t* ids_all,
                                        int64_t total_rows, const Rules* rules,
-                                       const int32_t* adj_base, const int64_t* adj_at,
-                                       const int32_t* adj2_base, const int64_t* adj2_at,
                                        char* arena, const int32_t* pos)
 {
     int lane = threadIdx.x & 31;
@@ -709,8 +760,8 @@ __global__ void batch_root_rows_kernel(const RootMeta* meta, int nroots, const i
         const RootMeta& M = meta[lo];
         int i = (int)(r - M.row_at);
         const Rules& R = rules[M.inst];
-        const int32_t* adj = adj_base + adj_at[M.inst];
-        const int32_t* adj2 = adj2_base + adj2_at[M.inst];
+        const int32_t* adj = R.adj;
+        const int32_t* adj2 = R.adj2;
         int u = ids_all[M.id_at + i];
         char* rec = arena + M.rec;
         uint32_t* r1 = (uint32_t*)(rec + rec_a1_off(M.t)) + (int64_t)i * M.W;
@@ -750,35 +801,31 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     cudaStream_t s = c->stream;
     CK(cudaSetDevice(c->cfg.device));
     BatchBufs& B = c->batch; // reused across calls on this context
-    // host side: tables, level 0, concatenation
-    std::vector<int64_t> h_off, h_off2, adj_at(count), adj2_at(count);
-    std::vector<int32_t> h_adj, h_adj2, h_md, h_ubt, h_ids;
+    // every instance's graph resident on the device (uploaded on first use);
+    // the rules of instance i point at its own arrays, nothing is concatenated
+    std::vector<int32_t> h_md, h_ubt, h_ids;
     std::vector<Rules> rules(count);
-    std::vector<int64_t> off_at(count), md_at_(count);
+    std::vector<int64_t> md_at_(count);
     std::vector<RootMeta> meta;
     int64_t vtotal = 0;
     int max_t = 1;
     auto t_load = clk::now();
+    std::unordered_set<unsigned long long> batch_serials;
+    for (int i = 0; i < count; i++) batch_serials.insert(graphs[i]->serial);
     for (int i = 0; i < count; i++) {
         const HostGraph& h = graphs[i]->h;
-        off_at[i] = (int64_t)h_off.size();
-        h_off.insert(h_off.end(), h.off.begin(), h.off.end());
-        h_off2.insert(h_off2.end(), h.off2.begin(), h.off2.end());
-        adj_at[i] = (int64_t)h_adj.size();
-        h_adj.insert(h_adj.end(), h.adj.begin(), h.adj.end());
-        adj2_at[i] = (int64_t)h_adj2.size();
-        h_adj2.insert(h_adj2.end(), h.adj2.begin(), h.adj2.end());
+        ResidentGraph* rg = nullptr;
+        qc_status us = make_resident(c, graphs[i], &batch_serials, &rg);
+        if (us != QC_OK) return us;
+        rules[i].off = rg->off.as<int64_t>();
+        rules[i].off2 = rg->off2.as<int64_t>();
+        rules[i].adj = rg->adj.as<int32_t>();
+        rules[i].adj2 = rg->adj2.as<int32_t>();
         rules[i].vbase = (int32_t)vtotal;
         rules[i].n = h.n;
         vtotal += h.n;
     }
     if (vtotal > INT32_MAX) return fail(QC_ERR_TOO_LARGE, "batch has more than 2^31 vertices");
-    CK(upload(B.off, h_off, s));
-    CK(upload(B.off2, h_off2, s));
-    CK(upload(B.adj, h_adj, s));
-    CK(upload(B.adj2, h_adj2, s));
-    CK(upload(B.adj_at, adj_at, s));
-    CK(upload(B.adj2_at, adj2_at, s));
     double load_ms = ms_since(t_load);
 
     auto t_enum = clk::now();
@@ -815,8 +862,6 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     for (int i = 0; i < count; i++) {
         rules[i].md = B.md.as<int32_t>() + md_at_[i];
         rules[i].ubt = B.ubt.as<int32_t>() + md_at_[i];
-        rules[i].off = B.off.as<int64_t>() + off_at[i];
-        rules[i].off2 = B.off2.as<int64_t>() + off_at[i];
     }
     CK(upload(B.rules, rules, s));
     const int nroots = (int)meta.size();
@@ -865,8 +910,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
                                                             c->arena.as<char>(), B.pos.as<int32_t>());
         batch_root_rows_kernel<<<std::max(1, blocks * 4), 256, 0, s>>>(
             B.meta.as<RootMeta>(), nroots, B.ids.as<int32_t>(), total_rows, B.rules.as<Rules>(),
-            B.adj.as<int32_t>(), B.adj_at.as<int64_t>(), B.adj2.as<int32_t>(),
-            B.adj2_at.as<int64_t>(), c->arena.as<char>(), B.pos.as<int32_t>());
+            c->arena.as<char>(), B.pos.as<int32_t>());
         batch_root_unpos_kernel<<<(unsigned)rb, 256, 0, s>>>(B.meta.as<RootMeta>(), nroots,
                                                              B.ids.as<int32_t>(), total_rows,
                                                              B.pos.as<int32_t>());

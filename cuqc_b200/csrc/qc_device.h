@@ -140,6 +140,8 @@ struct Rules {
     const int32_t* ubt;  // floor(d / gamma), d in [0 .. mdlen)
     const int64_t* off;  // 1-hop offsets (degrees for the work counters)
     const int64_t* off2; // 2-hop offsets
+    const int32_t* adj;  // 1-hop rows (read when the root record is built)
+    const int32_t* adj2; // 2-hop rows
     int32_t mdlen;
     int32_t min_size;
     int32_t vbase;       // added to vertex ids when sets are emitted

@@ -179,8 +179,18 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
         g.off2.assign(off2, off2 + n + 1);
         g.adj2.assign(adj2, adj2 + off2[n]);
         gamma_tables(gammas[i], n, min_sizes[i], mds[(size_t)i], ubts[(size_t)i]);
-        rules[(size_t)i] = Rules{mds[(size_t)i].data(), ubts[(size_t)i].data(), off, off2,
-                                 (int32_t)mds[(size_t)i].size(), min_sizes[i], (int32_t)vb, n};
+        Rules ru{};
+        ru.md = mds[(size_t)i].data();
+        ru.ubt = ubts[(size_t)i].data();
+        ru.off = off;
+        ru.off2 = off2;
+        ru.adj = adj;
+        ru.adj2 = adj2;
+        ru.mdlen = (int32_t)mds[(size_t)i].size();
+        ru.min_size = min_sizes[i];
+        ru.vbase = (int32_t)vb;
+        ru.n = n;
+        rules[(size_t)i] = ru;
         std::vector<int32_t> ids;
         int cov = 0;
         build_root(g, mds[(size_t)i].data(), min_sizes[i], ids, cov);
