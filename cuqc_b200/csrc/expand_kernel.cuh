@@ -79,10 +79,11 @@ __device__ __forceinline__ bool bit(const uint32_t* a, int v) { return (a[v >> 5
 
 // Task records are written by one SM and read by another after a hand-off
 // through the work stack, and their blocks are recycled; every read of record
-// content goes through L2 (ld.global.cg) so no SM can see a stale L1 copy of a
-// block's previous contents.
-__device__ __forceinline__ uint32_t rec_ld(const uint32_t* p) { return __ldcg(p); }
-__device__ __forceinline__ int32_t rec_ld(const int32_t* p) { return __ldcg(p); }
+// content in global memory goes through L2 (ld.global.cg) so no SM can see a
+// stale L1 copy of a block's previous contents.  A record staged in shared
+// memory is read there.
+__device__ __forceinline__ uint32_t rec_ld(const uint32_t* p) { return __isGlobal(p) ? __ldcg(p) : *p; }
+__device__ __forceinline__ int32_t rec_ld(const int32_t* p) { return __isGlobal(p) ? __ldcg(p) : *p; }
 __device__ __forceinline__ bool rec_bit(const uint32_t* a, int v) { return (rec_ld(a + (v >> 5)) >> (v & 31)) & 1u; }
 
 // |record row & mask| over W words (row in a task record, mask in the workspace)
@@ -141,6 +142,7 @@ struct TaskView {
     int32_t* l2;
     const uint32_t* A1;
     const uint32_t* A2;
+    int32_t* l2g;      // the record's l2 array in the arena (== l2 unless staged)
     unsigned long long rec;
 };
 
@@ -158,8 +160,26 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
     T.l2 = (int32_t*)(arena + rec + rec_l2_off(T.t));
     T.A1 = (const uint32_t*)(arena + rec + rec_a1_off(T.t));
     T.A2 = (const uint32_t*)(arena + rec + rec_a2_off(T.t, T.W));
+    T.l2g = T.l2;
     T.rec = rec;
     return T;
+}
+
+// Copy a record's body (ids, l2, A1, A2) into this warp's shared-memory
+// buffer with 16-byte loads through L2 and point the view there.
+__device__ void stage_record(const ExpandParams& P, TaskView& T, char* buf)
+{
+    const char* src = P.arena + T.rec + rec_ids_off();
+    const uint64_t body = rec_bytes(T.t, T.W) - rec_ids_off(); // multiple of 16
+    const uint4* s4 = (const uint4*)src;
+    uint4* d4 = (uint4*)buf;
+    for (uint64_t i = lane_id(); i < body / 16; i += 32) d4[i] = __ldcg(s4 + i);
+    __syncwarp();
+    char* b = buf - rec_ids_off(); // same offsets as in the record
+    T.ids = (const int32_t*)(b + rec_ids_off());
+    T.l2 = (int32_t*)(b + rec_l2_off(T.t));
+    T.A1 = (const uint32_t*)(b + rec_a1_off(T.t));
+    T.A2 = (const uint32_t*)(b + rec_a2_off(T.t, T.W));
 }
 
 struct Ws {
@@ -179,10 +199,10 @@ struct Ws {
     uint32_t* mk[12];
 };
 
-__device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global, WarpSmem* sm)
+// workspace arrays laid out by ws_layout(max_t) from base b (global or shared)
+__device__ __forceinline__ Ws ws_view(char* b, int max_t, WarpSmem* sm)
 {
-    WsLayout L = ws_layout(P.max_t);
-    char* b = P.ws + (int64_t)warp_global * P.ws_stride;
+    WsLayout L = ws_layout(max_t);
     Ws w;
     w.sm = sm;
     w.cnt = &sm->cnt;
@@ -197,7 +217,7 @@ __device__ __forceinline__ Ws ws_view(const ExpandParams& P, int warp_global, Wa
     w.sel = (int32_t*)(b + L.sel);
     w.khi = (unsigned long long*)(b + L.key_hi);
     w.klo = (unsigned long long*)(b + L.key_lo);
-    int Wm = words_for(P.max_t) + 2;
+    int Wm = words_for(max_t) + 2;
     uint32_t* m0 = (uint32_t*)(b + L.masks);
     for (int i = 0; i < 12; i++) w.mk[i] = m0 + (int64_t)i * Wm;
     return w;
@@ -1538,11 +1558,19 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
 
 // Returns true when other work items (branch ranges pushed here or earlier)
 // share the record, so its release must go through the reference count.
-__device__ bool process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, const TaskHdr& hv)
+//
+// Tasks of 33..P.smem_t vertices run with their record and workspace in this
+// warp's shared memory (`wss`, `stage`); larger ones use the global
+// workspace `wsg` and read the record through L2.
+__device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stage, const WorkItem& it,
+                             const TaskHdr& hv)
 {
     TaskView T = task_view(P.arena, it.rec, hv);
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
+    const bool staged = stage != nullptr && t > 32 && t <= P.smem_t && t <= P.max_t;
+    if (staged) stage_record(P, T, stage);
+    Ws& ws = staged ? wss : wsg;
     Rules R = P.rules[T.inst];
     if (ws.sm->tab_inst != T.inst) {
         // refresh this warp's shared copy of the instance's gamma tables
@@ -1608,6 +1636,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& ws, const WorkItem& it, 
             for (int v = m + lane; v < t; v += 32) {
                 int l2 = popc_and(T.A2 + (int64_t)v * W, CC, W);
                 T.l2[v] = l2;
+                if (T.l2g != T.l2) T.l2g[v] = l2; // branch items on other warps read the arena
                 if (l2 < nc - 1 || ws.indeg[v] + ws.exdeg[v] < need_t) bad2 = 1;
             }
             __syncwarp();
@@ -1737,8 +1766,12 @@ __device__ __forceinline__ unsigned char* dyn_smem() { return qc_dyn_smem; }
 __device__ __forceinline__ unsigned char* dyn_smem() { return emu_dyn_smem(); }
 #endif
 
-// dynamic shared memory the kernel needs per block of `warps` warps
-__host__ __device__ inline size_t expand_smem_bytes(int warps) { return sizeof(WarpSmem) * (size_t)warps; }
+// dynamic shared memory the kernel needs per block of `warps` warps when
+// tasks of up to smem_t vertices are staged in shared memory
+__host__ __device__ inline size_t expand_smem_bytes(int warps, int smem_t)
+{
+    return warp_smem_bytes(smem_t) * (size_t)warps;
+}
 
 #ifndef QC_EMULATION
 __global__ void __launch_bounds__(256, 2) expand_kernel(ExpandParams P)
@@ -1748,8 +1781,16 @@ __global__ void expand_kernel(ExpandParams P)
 {
     int lane = lane_id();
     int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    WarpSmem* sm = (WarpSmem*)dyn_smem() + (threadIdx.x >> 5);
-    Ws ws = ws_view(P, warp_global, sm);
+    char* base = (char*)dyn_smem() + (size_t)(threadIdx.x >> 5) * warp_smem_bytes(P.smem_t);
+    WarpSmem* sm = (WarpSmem*)base;
+    Ws ws = ws_view(P.ws + (int64_t)warp_global * P.ws_stride, P.max_t, sm);
+    Ws wss = ws;
+    char* stage = nullptr;
+    if (P.smem_t > 0) {
+        char* sb = base + align16(sizeof(WarpSmem));
+        wss = ws_view(sb, P.smem_t, sm);
+        stage = sb + ws_layout(P.smem_t).total;
+    }
     if (lane == 0) {
         sm->lcount = 0;
         sm->tab_inst = -1;
@@ -1789,7 +1830,7 @@ __global__ void expand_kernel(ExpandParams P)
         hv.W = __shfl_sync(QC_FULL, hv.W, 0);
         hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
         __threadfence();
-        bool shared = process_item(P, ws, it, hv);
+        bool shared = process_item(P, ws, wss, stage, it, hv);
         __syncwarp();
         __threadfence();
         if (lane == 0) {

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
@@ -339,6 +340,59 @@ static int max_top(const Control& ctl)
     return m;
 }
 
+// Launch shape of expand_kernel for tasks of up to max_t vertices: warps per
+// block, blocks, and the largest task staged in shared memory (the biggest
+// candidate whose per-warp buffers fit the blocks resident on one SM).
+struct Shape {
+    int wpb = 4, blocks = 0, smem_t = 0;
+    size_t smem_bytes = 0;
+};
+
+static qc_status launch_shape(qc_context* c, int max_t, Shape& sh)
+{
+    // expand_kernel is compiled with __launch_bounds__(256, 2): at most 8 warps a
+    // block.  The default is one block of 4 warps per SM.
+    sh.wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
+    const int want_bps = c->cfg.blocks_per_sm > 0 ? c->cfg.blocks_per_sm : 1;
+    const size_t sm_budget = 220u << 10; // of the 228 KB of shared memory per SM
+    sh.smem_t = 0;
+    if (max_t > 32) {
+        for (int cand : {256, 192, 128, 96, 64}) {
+            int tt = std::min(cand, max_t);
+            if (warp_smem_bytes(tt) * sh.wpb * want_bps <= sm_budget) {
+                sh.smem_t = tt;
+                break;
+            }
+        }
+    }
+    sh.smem_bytes = expand_smem_bytes(sh.wpb, sh.smem_t);
+    {
+        // raised once per device to the opt-in maximum and never lowered:
+        // contexts on other threads launch with their own sizes meanwhile
+        static std::mutex mu;
+        static bool raised[64] = {};
+        std::lock_guard<std::mutex> lk(mu);
+        int dev = c->cfg.device;
+        if (dev < 0 || dev >= 64) return fail(QC_ERR_ARGS, "device ordinal above 63");
+        if (!raised[dev]) {
+            int optin = 0;
+            CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            CK(cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    optin));
+            raised[dev] = true;
+        }
+    }
+    int resident = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, sh.wpb * 32,
+                                                     sh.smem_bytes));
+    if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
+    // a persistent launch: never more blocks than can be resident at once
+    const int bps = std::min(want_bps, resident);
+    sh.blocks = c->sms * bps;
+    if (c->cfg.max_blocks > 0) sh.blocks = std::min(sh.blocks, c->cfg.max_blocks);
+    return QC_OK;
+}
+
 // Device copy of graph g, uploaded on first use and kept for later calls.
 // When the resident graphs exceed the context's budget, the least recently
 // used ones (other than g and those in `keep`) are dropped.  Also sizes the
@@ -419,18 +473,12 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     CK(upload(c->ubt, ubt, s));
     CK(upload(c->ids, ids, s));
 
-    // expand_kernel is compiled with __launch_bounds__(256, 2): at most 8 warps a
-    // block.  The search tree offers limited parallelism and every idle warp
-    // polls the shared stack, so the default is one block of 4 warps per SM.
-    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
-    int resident = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32,
-                                                     expand_smem_bytes(wpb)));
-    if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
-    // a persistent launch: never more blocks than can be resident at once
-    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : 1;
-    int blocks = c->sms * bps;
-    if (c->cfg.max_blocks > 0) blocks = std::min(blocks, c->cfg.max_blocks);
+    Shape sh;
+    {
+        qc_status ss = launch_shape(c, t, sh);
+        if (ss != QC_OK) return ss;
+    }
+    const int wpb = sh.wpb, blocks = sh.blocks;
     int nwarps = blocks * wpb;
     WsLayout L = ws_layout(t);
     CK(c->ws.ensure((size_t)L.total * nwarps));
@@ -524,6 +572,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.ws_stride = L.total;
         P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = t;
+        P.smem_t = sh.smem_t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
@@ -535,7 +584,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
             P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
         }
         CK(cudaEventRecord(c->ev[1], s));
-        expand_kernel<<<blocks, wpb * 32, expand_smem_bytes(wpb), s>>>(P);
+        expand_kernel<<<blocks, wpb * 32, sh.smem_bytes, s>>>(P);
         CK(cudaGetLastError());
         c->launches += 1;
         CK(cudaEventRecord(c->ev[2], s));
@@ -867,14 +916,12 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     const int nroots = (int)meta.size();
     const int64_t total_rows = (int64_t)h_ids.size();
 
-    int wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
-    int resident = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, expand_kernel, wpb * 32,
-                                                     expand_smem_bytes(wpb)));
-    if (resident < 1) return fail(QC_ERR_CUDA, "expand_kernel cannot be resident");
-    int bps = c->cfg.blocks_per_sm > 0 ? std::min(c->cfg.blocks_per_sm, resident) : 1;
-    int blocks = c->sms * bps;
-    if (c->cfg.max_blocks > 0) blocks = std::min(blocks, c->cfg.max_blocks);
+    Shape sh;
+    {
+        qc_status ss = launch_shape(c, max_t, sh);
+        if (ss != QC_OK) return ss;
+    }
+    const int wpb = sh.wpb, blocks = sh.blocks;
     int nwarps = blocks * wpb;
     WsLayout L = ws_layout(max_t);
     CK(c->ws.ensure((size_t)L.total * nwarps));
@@ -964,6 +1011,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         P.ws_stride = L.total;
         P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = max_t;
+        P.smem_t = sh.smem_t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
@@ -974,7 +1022,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
             P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
         }
         CK(cudaEventRecord(c->ev[1], s));
-        expand_kernel<<<blocks, wpb * 32, expand_smem_bytes(wpb), s>>>(P);
+        expand_kernel<<<blocks, wpb * 32, sh.smem_bytes, s>>>(P);
         CK(cudaGetLastError());
         c->launches += 1;
         CK(cudaEventRecord(c->ev[2], s));

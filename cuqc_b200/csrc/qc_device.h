@@ -164,6 +164,7 @@ struct ExpandParams {
     char* ws;            // per-warp workspace
     int64_t ws_stride;   // bytes per warp
     unsigned long long arena_cap; // bytes of the record arena
+    int32_t smem_t;      // tasks of 33..smem_t vertices are staged in shared memory (0: none)
     int32_t max_t;       // largest task the workspace holds
     int32_t split;       // branches per work item before splitting
     int32_t small_path;  // 1: tasks of <= 32 vertices use the register path
@@ -231,6 +232,17 @@ __host__ __device__ inline WsLayout ws_layout(int max_t)
     L.masks = o;    o += align16(4 * W * 12);
     L.total = align16(o);
     return L;
+}
+
+// Shared memory of one warp: its WarpSmem, then (when tasks of up to smem_t
+// vertices are staged) a workspace laid out by ws_layout(smem_t) and a buffer
+// for one record body of smem_t vertices.
+__host__ __device__ inline uint64_t warp_smem_bytes(int smem_t)
+{
+    uint64_t b = align16(sizeof(WarpSmem));
+    if (smem_t > 0)
+        b += (uint64_t)ws_layout(smem_t).total + rec_bytes(smem_t, words_for(smem_t)) - rec_ids_off();
+    return align16(b);
 }
 
 } // namespace qcb

@@ -89,6 +89,12 @@ inline void __syncwarp(unsigned = 0xffffffffu) { emu_w->bar.arrive_and_wait(); }
 inline int __popc(unsigned x) { return __builtin_popcount(x); }
 template <class T> inline T __ldcg(const T* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 template <class T> inline T __ldg(const T* p) { return *p; }
+struct uint4 {
+    unsigned x, y, z, w;
+};
+inline uint4 __ldcg(const uint4* p) { return *p; }
+// every emulated address is host memory; the kernel's global-only loads work on all of it
+inline unsigned __isGlobal(const void*) { return 1; }
 inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
 inline int __ffs(unsigned x) { return x ? __builtin_ctz(x) + 1 : 0; }
 inline int __clz(unsigned x) { return x ? __builtin_clz(x) : 32; }

@@ -128,7 +128,10 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     P.small_path = small_path;
     P.wait_ns = 20000000000ll;
     P.deadline_ns = emu_deadline();
-    emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps));
+    // stage tasks of up to 96 vertices in (emulated) shared memory, as the
+    // library does with its per-SM budget, so both task paths run here
+    P.smem_t = t > 32 ? std::min(t, 96) : 0;
+    emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps, P.smem_t));
 
     counters[0] = (int64_t)ctl.tasks;
     counters[1] = (int64_t)ctl.branches;
@@ -262,7 +265,9 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     P.small_path = 1;
     P.wait_ns = 20000000000ll;
     P.deadline_ns = emu_deadline();
-    if (!items.empty()) emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps));
+    P.smem_t = max_t > 32 ? std::min(max_t, 96) : 0;
+    if (!items.empty())
+        emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps, P.smem_t));
     counters[0] = (int64_t)ctl.tasks;
     counters[1] = (int64_t)ctl.branches;
     counters[2] = ctl.status;
