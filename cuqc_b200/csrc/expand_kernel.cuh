@@ -190,6 +190,7 @@ struct Ws {
     int32_t* indeg;
     int32_t* exdeg;
     int32_t* aux;
+    int32_t* vlist; // compacted vertex positions (see compact)
     int32_t* hist;
     int32_t* pcnt;
     long long* psum;
@@ -211,6 +212,7 @@ __device__ __forceinline__ Ws ws_view(char* b, int max_t, WarpSmem* sm)
     w.indeg = (int32_t*)(b + L.indeg);
     w.exdeg = (int32_t*)(b + L.exdeg);
     w.aux = (int32_t*)(b + L.aux);
+    w.vlist = (int32_t*)(b + L.vlist);
     w.hist = (int32_t*)(b + L.hist);
     w.pcnt = (int32_t*)(b + L.pref_cnt);
     w.psum = (long long*)(b + L.pref_sum);
@@ -449,13 +451,30 @@ __device__ bool members_ok(const ExpandParams& P, const Rules& R, Ws& ws, const 
     return !__any_sync(QC_FULL, bad);
 }
 
+// positions v < t set in `mask`, ascending, into ws.vlist; returns their number.
+// Loops over the list keep all 32 lanes busy however sparse the mask is.
+__device__ int compact(Ws& ws, const uint32_t* mask, int t)
+{
+    int lane = lane_id();
+    int n = 0;
+    for (int base = 0; base < t; base += 32) {
+        int v = base + lane;
+        bool in = v < t && bit(mask, v);
+        unsigned bal = __ballot_sync(QC_FULL, in);
+        if (in) ws.vlist[n + __popc(bal & ((1u << lane) - 1u))] = v;
+        n += __popc(bal);
+    }
+    __syncwarp();
+    return n;
+}
+
 // exdeg[v] = |N(v) & R| for v in mask `who`
 __device__ void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, const uint32_t* R)
 {
-    int lane = lane_id();
-    for (int base = 0; base < T.t; base += 32) {
-        int v = base + lane;
-        if (v < T.t && bit(who, v)) ws.exdeg[v] = popc_and(T.A1 + (int64_t)v * T.W, R, T.W);
+    int n = compact(ws, who, T.t);
+    for (int i = lane_id(); i < n; i += 32) {
+        int v = ws.vlist[i];
+        ws.exdeg[v] = popc_and(T.A1 + (int64_t)v * T.W, R, T.W);
     }
     __syncwarp();
 }
@@ -1030,23 +1049,34 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
         cid[i] = rec_ld(T.ids + ws.sel[i]);
         cl2[i] = 0;
     }
-    // compacted rows: child bit j of row i = parent bit sel[j] of row sel[i]
-    for (int i = 0; i < tc; i++) {
-        const uint32_t* r1 = T.A1 + (int64_t)ws.sel[i] * T.W;
-        const uint32_t* r2 = T.A2 + (int64_t)ws.sel[i] * T.W;
-        for (int w = 0; w < Wc; w++) {
-            int j = w * 32 + lane;
-            bool b1 = false, b2 = false;
-            if (j < tc) {
-                int pj = ws.sel[j];
-                b1 = rec_bit(r1, pj);
-                b2 = rec_bit(r2, pj);
+    // compacted rows: child bit j of row i = parent bit sel[j] of row sel[i].
+    // Column word w: lane k holds the parent column sel[w*32+k]; rows go by in
+    // groups of 32 (lane r holds the parent row of child row i0+r), and the
+    // reads of different rows do not depend on each other.
+    for (int w = 0; w < Wc; w++) {
+        const int j = w * 32 + lane;
+        const int pj = j < tc ? ws.sel[j] : 0;
+        const int pw = pj >> 5, pb = pj & 31;
+        const bool col = j < tc;
+        for (int i0 = 0; i0 < tc; i0 += 32) {
+            const int rows = tc - i0 < 32 ? tc - i0 : 32;
+            const int my_row = lane < rows ? ws.sel[i0 + lane] : 0;
+            unsigned o1 = 0, o2 = 0;
+#pragma unroll 4
+            for (int r = 0; r < rows; r++) {
+                const int64_t base = (int64_t)__shfl_sync(QC_FULL, my_row, r) * T.W + pw;
+                const uint32_t x1 = col ? rec_ld(T.A1 + base) : 0u;
+                const uint32_t x2 = col ? rec_ld(T.A2 + base) : 0u;
+                const unsigned w1 = __ballot_sync(QC_FULL, (x1 >> pb) & 1u);
+                const unsigned w2 = __ballot_sync(QC_FULL, (x2 >> pb) & 1u);
+                if (lane == r) {
+                    o1 = w1;
+                    o2 = w2;
+                }
             }
-            unsigned w1 = __ballot_sync(QC_FULL, b1);
-            unsigned w2 = __ballot_sync(QC_FULL, b2);
-            if (lane == 0) {
-                c1[(int64_t)i * Wc + w] = w1;
-                c2[(int64_t)i * Wc + w] = w2;
+            if (lane < rows) {
+                c1[(int64_t)(i0 + lane) * Wc + w] = o1;
+                c2[(int64_t)(i0 + lane) * Wc + w] = o2;
             }
         }
     }
@@ -1085,19 +1115,25 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     __syncwarp();
     bs_range(PRE, W, T.m, q);
     int m1 = T.m + 1;
-    // degrees for members and PRE (add one vertex, main.cu:1465-1492)
-    for (int base = 0; base < t; base += 32) {
-        int v = base + lane;
-        if (v < t && (bit(M, v) || bit(PRE, v))) {
-            const uint32_t* row = T.A1 + (int64_t)v * W;
-            ws.indeg[v] = popc_and(row, M, W);
-            ws.exdeg[v] = popc_and(row, PRE, W);
-        }
-    }
     // diameter pruning (main.cu:1709-1732): PRE & N2(q)
     const uint32_t* r2q = T.A2 + (int64_t)q * W;
     for (int w = lane; w < W; w += 32) D[w] = PRE[w] & rec_ld(r2q + w);
     __syncwarp();
+    // degrees for members and PRE (add one vertex, main.cu:1465-1492); only the
+    // members and the candidates that survive the diameter test are ever read
+    {
+        uint32_t* MD = ws.mk[MK_U];
+        for (int w = lane; w < W; w += 32) MD[w] = M[w] | D[w];
+        __syncwarp();
+        int n = compact(ws, MD, t);
+        for (int i = lane; i < n; i += 32) {
+            int v = ws.vlist[i];
+            const uint32_t* row = T.A1 + (int64_t)v * W;
+            ws.indeg[v] = popc_and(row, M, W);
+            ws.exdeg[v] = popc_and(row, PRE, W);
+        }
+        __syncwarp();
+    }
     if (lane == 0) {
         ws.cnt->branches++;
         ws.cnt->parent_vertices += (unsigned long long)(q + 1);

@@ -207,7 +207,7 @@ struct WarpSmem {
 // Per-warp workspace (global memory) for the bit-matrix path, tasks of up
 // to max_t vertices.
 struct WsLayout {
-    int64_t indeg, exdeg, aux, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
+    int64_t indeg, exdeg, aux, vlist, hist, pref_cnt, pref_sum, sel, key_hi, key_lo, masks;
     int64_t total;
 };
 
@@ -223,6 +223,7 @@ __host__ __device__ inline WsLayout ws_layout(int max_t)
     L.indeg = o;    o += align16(4 * t);
     L.exdeg = o;    o += align16(4 * t);
     L.aux = o;      o += align16(4 * t);
+    L.vlist = o;    o += align16(4 * t);
     L.hist = o;     o += align16(4 * (t + 2));
     L.pref_cnt = o; o += align16(4 * (t + 2));
     L.pref_sum = o; o += align16(8 * (t + 2));
