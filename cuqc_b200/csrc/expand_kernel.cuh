@@ -182,22 +182,25 @@ __device__ void stage_record(const ExpandParams& P, TaskView& T, char* buf)
     T.A2 = (const uint32_t*)(b + rec_a2_off(T.t, T.W));
 }
 
+// A warp's workspace: one base pointer and the byte offsets of its arrays
+// (laid out by ws_layout), so the whole view fits in a few registers.
 struct Ws {
-    WarpSmem* sm;      // per-warp state in shared memory
-    WarpCount* cnt;    // this warp's work counters (lane 0)
-    unsigned long long* fhead; // private free list per size class: offset/16+1, 0 = empty
-    int32_t* fcount;           // blocks on each private list
-    int32_t* indeg;
-    int32_t* exdeg;
-    int32_t* aux;
-    int32_t* vlist; // compacted vertex positions (see compact)
-    int32_t* hist;
-    int32_t* pcnt;
-    long long* psum;
-    int32_t* sel;
-    unsigned long long* khi;
-    unsigned long long* klo;
-    uint32_t* mk[12];
+    WarpSmem* sm; // per-warp state in shared memory
+    char* b;      // workspace base (global or shared memory)
+    int32_t o_exdeg, o_aux, o_vlist, o_hist, o_pcnt, o_psum, o_sel, o_khi, o_klo, o_masks;
+    int32_t wm;   // words per mask
+    __device__ __forceinline__ int32_t* indeg() const { return (int32_t*)b; }
+    __device__ __forceinline__ int32_t* exdeg() const { return (int32_t*)(b + o_exdeg); }
+    __device__ __forceinline__ int32_t* aux() const { return (int32_t*)(b + o_aux); }
+    // compacted vertex positions (see compact)
+    __device__ __forceinline__ int32_t* vlist() const { return (int32_t*)(b + o_vlist); }
+    __device__ __forceinline__ int32_t* hist() const { return (int32_t*)(b + o_hist); }
+    __device__ __forceinline__ int32_t* pcnt() const { return (int32_t*)(b + o_pcnt); }
+    __device__ __forceinline__ long long* psum() const { return (long long*)(b + o_psum); }
+    __device__ __forceinline__ int32_t* sel() const { return (int32_t*)(b + o_sel); }
+    __device__ __forceinline__ unsigned long long* khi() const { return (unsigned long long*)(b + o_khi); }
+    __device__ __forceinline__ unsigned long long* klo() const { return (unsigned long long*)(b + o_klo); }
+    __device__ __forceinline__ uint32_t* mk(int i) const { return (uint32_t*)(b + o_masks) + i * wm; }
 };
 
 // workspace arrays laid out by ws_layout(max_t) from base b (global or shared)
@@ -206,22 +209,18 @@ __device__ __forceinline__ Ws ws_view(char* b, int max_t, WarpSmem* sm)
     WsLayout L = ws_layout(max_t);
     Ws w;
     w.sm = sm;
-    w.cnt = &sm->cnt;
-    w.fhead = sm->fhead;
-    w.fcount = sm->fcount;
-    w.indeg = (int32_t*)(b + L.indeg);
-    w.exdeg = (int32_t*)(b + L.exdeg);
-    w.aux = (int32_t*)(b + L.aux);
-    w.vlist = (int32_t*)(b + L.vlist);
-    w.hist = (int32_t*)(b + L.hist);
-    w.pcnt = (int32_t*)(b + L.pref_cnt);
-    w.psum = (long long*)(b + L.pref_sum);
-    w.sel = (int32_t*)(b + L.sel);
-    w.khi = (unsigned long long*)(b + L.key_hi);
-    w.klo = (unsigned long long*)(b + L.key_lo);
-    int Wm = words_for(max_t) + 2;
-    uint32_t* m0 = (uint32_t*)(b + L.masks);
-    for (int i = 0; i < 12; i++) w.mk[i] = m0 + (int64_t)i * Wm;
+    w.b = b + L.indeg;
+    w.o_exdeg = (int32_t)(L.exdeg - L.indeg);
+    w.o_aux = (int32_t)(L.aux - L.indeg);
+    w.o_vlist = (int32_t)(L.vlist - L.indeg);
+    w.o_hist = (int32_t)(L.hist - L.indeg);
+    w.o_pcnt = (int32_t)(L.pref_cnt - L.indeg);
+    w.o_psum = (int32_t)(L.pref_sum - L.indeg);
+    w.o_sel = (int32_t)(L.sel - L.indeg);
+    w.o_khi = (int32_t)(L.key_hi - L.indeg);
+    w.o_klo = (int32_t)(L.key_lo - L.indeg);
+    w.o_masks = (int32_t)(L.masks - L.indeg);
+    w.wm = words_for(max_t) + 2;
     return w;
 }
 
@@ -292,16 +291,16 @@ __device__ int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const u
                           bool filter_valid, int m, const Bounds& b)
 {
     int lane = lane_id();
-    for (int j = lane; j <= vmax + 1; j += 32) ws.hist[j] = 0;
+    for (int j = lane; j <= vmax + 1; j += 32) ws.hist()[j] = 0;
     __syncwarp();
     int cnt = 0;
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
         if (v < t && bit(cm, v)) {
-            int in = ws.indeg[v];
-            if (!filter_valid || cand_valid(R, in, ws.exdeg[v], m, b)) {
+            int in = ws.indeg()[v];
+            if (!filter_valid || cand_valid(R, in, ws.exdeg()[v], m, b)) {
                 int j = vmax - (in > vmax ? vmax : (in < 0 ? 0 : in));
-                atomicAdd(&ws.hist[j], 1);
+                atomicAdd(&ws.hist()[j], 1);
                 cnt++;
             }
         }
@@ -312,13 +311,13 @@ __device__ int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const u
     long long carry_s = 0;
     for (int base = 0; base <= vmax + 1; base += 32) {
         int j = base + lane;
-        int c = (j <= vmax + 1) ? ws.hist[j] : 0;
+        int c = (j <= vmax + 1) ? ws.hist()[j] : 0;
         long long s = (j <= vmax) ? (long long)c * (vmax - j) : 0;
         int ic = wscan(c);
         long long is = wscan64(s);
         if (j <= vmax + 1) {
-            ws.pcnt[j] = carry + ic - c;
-            ws.psum[j] = carry_s + is - s;
+            ws.pcnt()[j] = carry + ic - c;
+            ws.psum()[j] = carry_s + is - s;
         }
         carry += __shfl_sync(QC_FULL, ic, 31);
         carry_s += __shfl_sync(QC_FULL, is, 31);
@@ -334,11 +333,11 @@ __device__ __forceinline__ long long top_sum(const Ws& ws, int vmax, int k)
     int lo = 0, hi = vmax + 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (ws.pcnt[mid] <= k) lo = mid;
+        if (ws.pcnt()[mid] <= k) lo = mid;
         else hi = mid - 1;
     }
-    if (lo > vmax) return ws.psum[vmax + 1];
-    return ws.psum[lo] + (long long)(k - ws.pcnt[lo]) * (vmax - lo);
+    if (lo > vmax) return ws.psum()[vmax + 1];
+    return ws.psum()[lo] + (long long)(k - ws.pcnt()[lo]) * (vmax - lo);
 }
 
 // ------------------------------------------------------------------
@@ -355,7 +354,7 @@ __device__ bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const u
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
         if (v < t && bit(mm, v)) {
-            int in = ws.indeg[v], ex = ws.exdeg[v];
+            int in = ws.indeg()[v], ex = ws.exdeg()[v];
             mi = in < mi ? in : mi;
             mt = in + ex < mt ? in + ex : mt;
             si += in;
@@ -367,8 +366,8 @@ __device__ bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const u
     int me = 0x7fffffff;
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
-        if (v < t && bit(mm, v) && ws.indeg[v] == min_in) {
-            int ex = ws.exdeg[v];
+        if (v < t && bit(mm, v) && ws.indeg()[v] == min_in) {
+            int ex = ws.exdeg()[v];
             me = ex < me ? ex : me;
         }
     }
@@ -446,12 +445,12 @@ __device__ bool members_ok(const ExpandParams& P, const Rules& R, Ws& ws, const 
     int bad = 0;
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
-        if (v < t && bit(mm, v) && !vert_extendable(R, ws.indeg[v], ws.exdeg[v], m, b)) bad = 1;
+        if (v < t && bit(mm, v) && !vert_extendable(R, ws.indeg()[v], ws.exdeg()[v], m, b)) bad = 1;
     }
     return !__any_sync(QC_FULL, bad);
 }
 
-// positions v < t set in `mask`, ascending, into ws.vlist; returns their number.
+// positions v < t set in `mask`, ascending, into ws.vlist(); returns their number.
 // Loops over the list keep all 32 lanes busy however sparse the mask is.
 __device__ int compact(Ws& ws, const uint32_t* mask, int t)
 {
@@ -461,7 +460,7 @@ __device__ int compact(Ws& ws, const uint32_t* mask, int t)
         int v = base + lane;
         bool in = v < t && bit(mask, v);
         unsigned bal = __ballot_sync(QC_FULL, in);
-        if (in) ws.vlist[n + __popc(bal & ((1u << lane) - 1u))] = v;
+        if (in) ws.vlist()[n + __popc(bal & ((1u << lane) - 1u))] = v;
         n += __popc(bal);
     }
     __syncwarp();
@@ -473,8 +472,8 @@ __device__ void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, co
 {
     int n = compact(ws, who, T.t);
     for (int i = lane_id(); i < n; i += 32) {
-        int v = ws.vlist[i];
-        ws.exdeg[v] = popc_and(T.A1 + (int64_t)v * T.W, R, T.W);
+        int v = ws.vlist()[i];
+        ws.exdeg()[v] = popc_and(T.A1 + (int64_t)v * T.W, R, T.W);
     }
     __syncwarp();
 }
@@ -487,7 +486,7 @@ __device__ void filter_valid(const ExpandParams& P, const Rules& R, Ws& ws, cons
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
         bool in = v < t && bit(in_mask, v);
-        bool ok = in && cand_valid(R, ws.indeg[v], ws.exdeg[v], m, b);
+        bool ok = in && cand_valid(R, ws.indeg()[v], ws.exdeg()[v], m, b);
         unsigned bo = __ballot_sync(QC_FULL, ok);
         unsigned br = __ballot_sync(QC_FULL, in && !ok);
         if (lane == 0) {
@@ -514,8 +513,8 @@ __device__ bool degree_prune(const ExpandParams& P, const Rules& R, const TaskVi
                              Bounds& b)
 {
     const int t = T.t, W = T.W;
-    uint32_t* X = ws.mk[MK_X];
-    uint32_t* who = ws.mk[MK_U];
+    uint32_t* X = ws.mk(MK_X);
+    uint32_t* who = ws.mk(MK_U);
     Bounds dummy = {0, 0, 0};
     int nc = build_hist(P, R, ws, D, t, m, false, m, dummy);
     if (lu_bounds(P, R, ws, M, t, m, nc, m, b)) return true;
@@ -532,8 +531,8 @@ __device__ bool degree_prune(const ExpandParams& P, const Rules& R, const TaskVi
         if (lu_bounds(P, R, ws, M, t, m, nv, m, b)) return true;
         if (!members_ok(P, R, ws, M, t, m, b)) return true;
         // Rm' = valid(Rm), X = Rm \ Rm'
-        filter_valid(P, R, ws, Rm, t, W, m, b, ws.mk[MK_T], X);
-        bs_copy(Rm, ws.mk[MK_T], W);
+        filter_valid(P, R, ws, Rm, t, W, m, b, ws.mk(MK_T), X);
+        bs_copy(Rm, ws.mk(MK_T), W);
     }
     return false;
 }
@@ -595,7 +594,7 @@ __device__ void check_clique(const ExpandParams& P, const Rules& R, const TaskVi
     int bad = 0;
     for (int base = 0; base < T.t; base += 32) {
         int v = base + lane;
-        if (v < T.t && bit(mm, v) && ws.indeg[v] < need) bad = 1;
+        if (v < T.t && bit(mm, v) && ws.indeg()[v] < need) bad = 1;
     }
     if (!__any_sync(QC_FULL, bad)) emit_mask(P, R, T, mm, m);
 }
@@ -846,14 +845,14 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigne
     }
     unsigned long long size = arena_class_bytes(cls);
     // this warp's own free list: blocks it freed itself, no other warp touches it
-    if (ws.fcount[cls] > 0) {
-        unsigned long long off = (ws.fhead[cls] - 1) * 16;
-        if (ws.fhead[cls] == 0 || off + size > P.arena_cap) {
+    if (ws.sm->fcount[cls] > 0) {
+        unsigned long long off = (ws.sm->fhead[cls] - 1) * 16;
+        if (ws.sm->fhead[cls] == 0 || off + size > P.arena_cap) {
             check_fail(P, 13, off); // a private list that points outside the arena
             return ~0ull;
         }
-        ws.fhead[cls] = *(unsigned long long*)(P.arena + off) & kOffMask;
-        ws.fcount[cls]--;
+        ws.sm->fhead[cls] = *(unsigned long long*)(P.arena + off) & kOffMask;
+        ws.sm->fcount[cls]--;
         ((TaskHdr*)(P.arena + off))->refs = 0;
         return off;
     }
@@ -906,11 +905,11 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigne
 // kPrivateFreeCap blocks; beyond that, to the shared lock-free list.
 __device__ void arena_free(const ExpandParams& P, Ws& ws, unsigned long long off, int cls)
 {
-    if (ws.fcount[cls] < kPrivateFreeCap) {
-        *(unsigned long long*)(P.arena + off) = ws.fhead[cls];
+    if (ws.sm->fcount[cls] < kPrivateFreeCap) {
+        *(unsigned long long*)(P.arena + off) = ws.sm->fhead[cls];
         ((TaskHdr*)(P.arena + off))->refs = kFreeMagic;
-        ws.fhead[cls] = off / 16 + 1;
-        ws.fcount[cls]++;
+        ws.sm->fhead[cls] = off / 16 + 1;
+        ws.sm->fcount[cls]++;
         return;
     }
     unsigned long long* head = &P.ctl->free_head[cls * kArenaShards + (blockIdx.x % kArenaShards)];
@@ -966,9 +965,9 @@ __device__ void sort_keys(Ws& ws, int n)
     int N = 1;
     while (N < n) N <<= 1;
     for (int i = n + lane; i < N; i += 32) {
-        ws.khi[i] = ~0ull;
-        ws.klo[i] = ~0ull;
-        ws.sel[i] = -1;
+        ws.khi()[i] = ~0ull;
+        ws.klo()[i] = ~0ull;
+        ws.sel()[i] = -1;
     }
     __syncwarp();
     for (int k = 2; k <= N; k <<= 1) {
@@ -977,13 +976,13 @@ __device__ void sort_keys(Ws& ws, int n)
                 int p = i ^ j;
                 if (p > i) {
                     bool up = (i & k) == 0;
-                    unsigned long long ah = ws.khi[i], al = ws.klo[i];
-                    unsigned long long bh = ws.khi[p], bl = ws.klo[p];
+                    unsigned long long ah = ws.khi()[i], al = ws.klo()[i];
+                    unsigned long long bh = ws.khi()[p], bl = ws.klo()[p];
                     bool gt = key_less(bh, bl, ah, al);
                     if (gt == up) {
-                        ws.khi[i] = bh; ws.klo[i] = bl;
-                        ws.khi[p] = ah; ws.klo[p] = al;
-                        int s = ws.sel[i]; ws.sel[i] = ws.sel[p]; ws.sel[p] = s;
+                        ws.khi()[i] = bh; ws.klo()[i] = bl;
+                        ws.khi()[p] = ah; ws.klo()[p] = al;
+                        int s = ws.sel()[i]; ws.sel()[i] = ws.sel()[p]; ws.sel()[p] = s;
                     }
                 }
             }
@@ -1012,12 +1011,12 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
         if (in) {
             int r = written + __popc(bal & ((1u << lane) - 1u));
             unsigned long long cls = isM ? 0ull : 1ull;
-            unsigned long long in_k = 0xffffull - (unsigned long long)ws.indeg[v];
-            unsigned long long ex_k = 0xffffull - (unsigned long long)ws.exdeg[v];
+            unsigned long long in_k = 0xffffull - (unsigned long long)ws.indeg()[v];
+            unsigned long long ex_k = 0xffffull - (unsigned long long)ws.exdeg()[v];
             unsigned long long l2_k = 0xffffull - (unsigned long long)rec_ld(T.l2 + v);
-            ws.khi[r] = (cls << 48) | (in_k << 32) | (ex_k << 16) | l2_k;
-            ws.klo[r] = 0xffffffffull - (unsigned long long)(unsigned)rec_ld(T.ids + v);
-            ws.sel[r] = v;
+            ws.khi()[r] = (cls << 48) | (in_k << 32) | (ex_k << 16) | l2_k;
+            ws.klo()[r] = 0xffffffffull - (unsigned long long)(unsigned)rec_ld(T.ids + v);
+            ws.sel()[r] = v;
         }
         written += __popc(bal);
     }
@@ -1046,7 +1045,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     uint32_t* c1 = (uint32_t*)(rec + rec_a1_off(tc));
     uint32_t* c2 = (uint32_t*)(rec + rec_a2_off(tc, Wc));
     for (int i = lane; i < tc; i += 32) {
-        cid[i] = rec_ld(T.ids + ws.sel[i]);
+        cid[i] = rec_ld(T.ids + ws.sel()[i]);
         cl2[i] = 0;
     }
     // compacted rows: child bit j of row i = parent bit sel[j] of row sel[i].
@@ -1055,12 +1054,12 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     // reads of different rows do not depend on each other.
     for (int w = 0; w < Wc; w++) {
         const int j = w * 32 + lane;
-        const int pj = j < tc ? ws.sel[j] : 0;
+        const int pj = j < tc ? ws.sel()[j] : 0;
         const int pw = pj >> 5, pb = pj & 31;
         const bool col = j < tc;
         for (int i0 = 0; i0 < tc; i0 += 32) {
             const int rows = tc - i0 < 32 ? tc - i0 : 32;
-            const int my_row = lane < rows ? ws.sel[i0 + lane] : 0;
+            const int my_row = lane < rows ? ws.sel()[i0 + lane] : 0;
             unsigned o1 = 0, o2 = 0;
 #pragma unroll 4
             for (int r = 0; r < rows; r++) {
@@ -1082,8 +1081,8 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     }
     __syncwarp();
     if (lane == 0) {
-        ws.cnt->children++;
-        ws.cnt->child_vertices += (unsigned long long)tc;
+        ws.sm->cnt.children++;
+        ws.sm->cnt.child_vertices += (unsigned long long)tc;
         __threadfence();
         WorkItem it;
         it.rec = at;
@@ -1102,12 +1101,12 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
 {
     const int t = T.t, W = T.W;
     int lane = lane_id();
-    uint32_t* M = ws.mk[MK_M];
-    uint32_t* PRE = ws.mk[MK_PRE];
-    uint32_t* D = ws.mk[MK_D];
-    uint32_t* Rm = ws.mk[MK_R];
-    uint32_t* CA = ws.mk[MK_CA];
-    uint32_t* Kc = ws.mk[MK_K];
+    uint32_t* M = ws.mk(MK_M);
+    uint32_t* PRE = ws.mk(MK_PRE);
+    uint32_t* D = ws.mk(MK_D);
+    uint32_t* Rm = ws.mk(MK_R);
+    uint32_t* CA = ws.mk(MK_CA);
+    uint32_t* Kc = ws.mk(MK_K);
 
     // members M u {q}; candidates before q
     bs_range(M, W, 0, T.m);
@@ -1122,24 +1121,24 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     // degrees for members and PRE (add one vertex, main.cu:1465-1492); only the
     // members and the candidates that survive the diameter test are ever read
     {
-        uint32_t* MD = ws.mk[MK_U];
+        uint32_t* MD = ws.mk(MK_U);
         for (int w = lane; w < W; w += 32) MD[w] = M[w] | D[w];
         __syncwarp();
         int n = compact(ws, MD, t);
         for (int i = lane; i < n; i += 32) {
-            int v = ws.vlist[i];
+            int v = ws.vlist()[i];
             const uint32_t* row = T.A1 + (int64_t)v * W;
-            ws.indeg[v] = popc_and(row, M, W);
-            ws.exdeg[v] = popc_and(row, PRE, W);
+            ws.indeg()[v] = popc_and(row, M, W);
+            ws.exdeg()[v] = popc_and(row, PRE, W);
         }
         __syncwarp();
     }
     if (lane == 0) {
-        ws.cnt->branches++;
-        ws.cnt->parent_vertices += (unsigned long long)(q + 1);
+        ws.sm->cnt.branches++;
+        ws.sm->cnt.parent_vertices += (unsigned long long)(q + 1);
         int pid = rec_ld(T.ids + q);
         if (pid >= 0 && pid < R.n)
-            ws.cnt->p_rows += (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
+            ws.sm->cnt.p_rows += (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
                                                    (R.off2[pid + 1] - R.off2[pid]));
     }
 
@@ -1153,7 +1152,7 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     int critv = md_at(R, m1 + b.L);
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
-        bool k = v < t && bit(M, v) && ws.indeg[v] + ws.exdeg[v] == critv && ws.exdeg[v] > 0;
+        bool k = v < t && bit(M, v) && ws.indeg()[v] + ws.exdeg()[v] == critv && ws.exdeg()[v] > 0;
         unsigned bal = __ballot_sync(QC_FULL, k);
         if (lane == 0) Kc[base >> 5] = bal;
     }
@@ -1175,8 +1174,8 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     __syncwarp();
     int nca = bs_count(CA, W);
     int m2 = m1;
-    uint32_t* C2 = ws.mk[MK_C];
-    uint32_t* D2 = ws.mk[MK_D];
+    uint32_t* C2 = ws.mk(MK_C);
+    uint32_t* D2 = ws.mk(MK_D);
     if (nca > 0) {
         // add the critical-adjacent candidates; 2-hop counts to them
         int bad = 0;
@@ -1184,10 +1183,10 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
             int v = base + lane;
             if (v < t && (bit(M, v) || bit(Rm, v))) {
                 int d = popc_and(T.A1 + (int64_t)v * W, CA, W);
-                ws.indeg[v] += d;
-                ws.exdeg[v] -= d;
+                ws.indeg()[v] += d;
+                ws.exdeg()[v] -= d;
                 int a = popc_and(T.A2 + (int64_t)v * W, CA, W);
-                ws.aux[v] = a;
+                ws.aux()[v] = a;
                 if (bit(M, v) && a != nca) bad = 1;
                 if (bit(CA, v) && a < nca - 1) bad = 1;
             }
@@ -1202,7 +1201,7 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
         // diameter pruning against the added vertices (main.cu:1689-1697)
         for (int base = 0; base < t; base += 32) {
             int v = base + lane;
-            bool in = v < t && bit(C2, v) && ws.aux[v] == nca;
+            bool in = v < t && bit(C2, v) && ws.aux()[v] == nca;
             unsigned bal = __ballot_sync(QC_FULL, in);
             if (lane == 0) D2[base >> 5] = bal;
         }
@@ -1212,7 +1211,7 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
         bs_copy(C2, Rm, W);
         bs_copy(D2, Rm, W);
     }
-    uint32_t* R2 = ws.mk[MK_R];
+    uint32_t* R2 = ws.mk(MK_R);
     Bounds b2 = {0, 0, 0};
     bool fail2 = degree_prune(P, R, T, ws, M, m2, C2, D2, R2, b2);
     if (m2 >= R.min_size) check_clique(P, R, T, ws, M, m2);
@@ -1470,8 +1469,8 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
     }
     __syncwarp();
     if (lane == 0) {
-        ws.cnt->children++;
-        ws.cnt->child_vertices += (unsigned long long)tc;
+        ws.sm->cnt.children++;
+        ws.sm->cnt.child_vertices += (unsigned long long)tc;
         __threadfence();
         WorkItem it;
         it.rec = at;
@@ -1499,9 +1498,9 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
             rows = (R.off[T.id + 1] - R.off[T.id]) + (R.off2[T.id + 1] - R.off2[T.id]);
         rows = __shfl_sync(QC_FULL, rows, q);
         if (lane == 0) {
-            ws.cnt->branches++;
-            ws.cnt->parent_vertices += (unsigned long long)(q + 1);
-            ws.cnt->p_rows += (unsigned long long)rows;
+            ws.sm->cnt.branches++;
+            ws.sm->cnt.parent_vertices += (unsigned long long)(q + 1);
+            ws.sm->cnt.p_rows += (unsigned long long)rows;
         }
     }
     Bounds b = {0, 0, 0};
@@ -1555,8 +1554,8 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
     int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
     if (lane == 0) {
-        ws.cnt->tasks++;
-        if ((unsigned long long)t > ws.cnt->max_task) ws.cnt->max_task = t;
+        ws.sm->cnt.tasks++;
+        if ((unsigned long long)t > ws.sm->cnt.max_task) ws.sm->cnt.max_task = t;
     }
     // lookahead (main.cu:1349-1405)
     int need_t = md_at(R, t);
@@ -1565,7 +1564,7 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
         if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
         bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
         if (!__any_sync(QC_FULL, bad)) {
-            if (lane == 0) ws.cnt->lookahead_hits++;
+            if (lane == 0) ws.sm->cnt.lookahead_hits++;
             emit_small(P, R, low_mask(t), T.id);
             return;
         }
@@ -1606,7 +1605,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     int lane = lane_id();
     const bool staged = stage != nullptr && t > 32 && t <= P.smem_t && t <= P.max_t;
     if (staged) stage_record(P, T, stage);
-    Ws& ws = staged ? wss : wsg;
+    Ws ws = staged ? wss : wsg;
     Rules R = P.rules[T.inst];
     if (ws.sm->tab_inst != T.inst) {
         // refresh this warp's shared copy of the instance's gamma tables
@@ -1644,11 +1643,11 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     }
     if (q_lo < 0) {
         if (lane == 0) {
-            ws.cnt->tasks++;
-            if ((unsigned long long)t > ws.cnt->max_task) ws.cnt->max_task = t;
+            ws.sm->cnt.tasks++;
+            if ((unsigned long long)t > ws.sm->cnt.max_task) ws.sm->cnt.max_task = t;
         }
-        uint32_t* MM = ws.mk[MK_M];
-        uint32_t* CC = ws.mk[MK_C];
+        uint32_t* MM = ws.mk(MK_M);
+        uint32_t* CC = ws.mk(MK_C);
         bs_range(MM, W, 0, m);
         bs_range(CC, W, m, t);
         int nc = t - m;
@@ -1657,8 +1656,8 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
             int v = base + lane;
             if (v < t) {
                 const uint32_t* row = T.A1 + (int64_t)v * W;
-                ws.indeg[v] = popc_and(row, MM, W);
-                ws.exdeg[v] = popc_and(row, CC, W);
+                ws.indeg()[v] = popc_and(row, MM, W);
+                ws.exdeg()[v] = popc_and(row, CC, W);
             }
         }
         __syncwarp();
@@ -1666,20 +1665,20 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         int need_t = md_at(R, t);
         int bad = 0;
         for (int v = lane; v < m; v += 32)
-            if (ws.indeg[v] + ws.exdeg[v] < need_t) bad = 1;
+            if (ws.indeg()[v] + ws.exdeg()[v] < need_t) bad = 1;
         if (!__any_sync(QC_FULL, bad)) {
             int bad2 = 0;
             for (int v = m + lane; v < t; v += 32) {
                 int l2 = popc_and(T.A2 + (int64_t)v * W, CC, W);
                 T.l2[v] = l2;
                 if (T.l2g != T.l2) T.l2g[v] = l2; // branch items on other warps read the arena
-                if (l2 < nc - 1 || ws.indeg[v] + ws.exdeg[v] < need_t) bad2 = 1;
+                if (l2 < nc - 1 || ws.indeg()[v] + ws.exdeg()[v] < need_t) bad2 = 1;
             }
             __syncwarp();
             if (!__any_sync(QC_FULL, bad2)) {
-                uint32_t* all = ws.mk[MK_T];
+                uint32_t* all = ws.mk(MK_T);
                 bs_range(all, W, 0, t);
-                if (lane == 0) ws.cnt->lookahead_hits++;
+                if (lane == 0) ws.sm->cnt.lookahead_hits++;
                 emit_mask(P, R, T, all, t);
                 return shared;
             }
@@ -1688,7 +1687,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         int need = mindeg(R, m);
         int qmax = m + T.cov;
         for (int v = 0; v < m; v++) {
-            int k = need - ws.indeg[v];
+            int k = need - ws.indeg()[v];
             if (k <= 0) continue;
             // position of the k-th candidate neighbour of v
             const uint32_t* row = T.A1 + (int64_t)v * W;
