@@ -658,6 +658,63 @@ __device__ bool push_item(const ExpandParams& P, const WorkItem& it)
     return push_entry(P, e, home_shard());
 }
 
+// Whole warp: push `count` branch ranges of record `rec` onto the warp's home
+// shard with one reservation; range c covers the `split` branches ending at
+// hi_first - c*split (not below q_lo).  Every lane fills a share of the slots.
+// Returns false when the shard is full (the run then stops with
+// ST_TASK_OVERFLOW) or a slot wait gave up.
+__device__ bool push_ranges(const ExpandParams& P, unsigned long long rec, int q_lo, int hi_first,
+                            int split, int count)
+{
+    const int lane = lane_id();
+    const int shard = home_shard();
+    int base = 0;
+    if (lane == 0) {
+        atomicAdd(&P.ctl->pending, count);
+        base = atomicAdd(&P.ctl->stack_top[shard], count);
+        if (base + count > P.ctl->stack_cap) {
+            set_status(P, ST_TASK_OVERFLOW);
+            atomicSub(&P.ctl->pending, count);
+            base = -1;
+        }
+    }
+    base = __shfl_sync(QC_FULL, base, 0);
+    if (base < 0) return false;
+    int ok = 1;
+    for (int c = lane; c < count; c += 32) {
+        const long long at = (long long)shard * P.ctl->stack_cap + base + c;
+        unsigned long long t0 = now_ns();
+        unsigned spins = 0;
+        bool got = true;
+        while (atomicCAS(&P.slot[at], 0, 2) != 0) {
+            if ((++spins & 255u) == 0 &&
+                (now_ns() - t0 > (unsigned long long)P.wait_ns || *(volatile int*)&P.ctl->status)) {
+                set_status(P, ST_ITER_LIMIT);
+                P.ctl->wait_fail_where = 4;
+                got = false;
+                break;
+            }
+            __nanosleep(64);
+        }
+        if (!got) {
+            ok = 0;
+            continue;
+        }
+        const int hi = hi_first - c * split;
+        StackEntry e;
+        for (int i = 0; i < kBundle; i++) e.rec[i] = 0;
+        e.rec[0] = rec;
+        e.n = 1;
+        e.q_hi = hi;
+        e.q_lo = hi - split + 1 < q_lo ? q_lo : hi - split + 1;
+        e.pad = 0;
+        P.stack[at] = e;
+        __threadfence();
+        atomicExch(&P.slot[at], 1);
+    }
+    return __all_sync(QC_FULL, ok);
+}
+
 // lane 0: read the entry at position idx of shard s once its writer is done
 __device__ int take_slot(const ExpandParams& P, int s, int idx, StackEntry& out)
 {
@@ -671,10 +728,14 @@ __device__ int take_slot(const ExpandParams& P, int s, int idx, StackEntry& out)
     unsigned long long t1 = now_ns();
     unsigned s2 = 0;
     while (atomicCAS(&P.slot[at], 1, 3) != 1) {
-        if ((++s2 & 255u) == 0 && now_ns() - t1 > (unsigned long long)P.wait_ns) {
-            set_status(P, ST_ITER_LIMIT);
-            P.ctl->wait_fail_where = 2;
-            return -1;
+        if ((++s2 & 255u) == 0) {
+            // a run that is stopping may leave reserved slots unwritten
+            if (*(volatile int*)&P.ctl->status) return -1;
+            if (now_ns() - t1 > (unsigned long long)P.wait_ns) {
+                set_status(P, ST_ITER_LIMIT);
+                P.ctl->wait_fail_where = 2;
+                return -1;
+            }
         }
         __nanosleep(32);
     }
@@ -1722,17 +1783,12 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         if (nb > P.split) {
             __syncwarp();
             __threadfence();
-            if (lane == 0) {
-                int extra = (q_hi - P.split - q_lo) / P.split + 1;
-                atomicAdd(&((TaskHdr*)(P.arena + it.rec))->refs, extra);
-                for (int hi = q_hi - P.split; hi >= q_lo; hi -= P.split) {
-                    WorkItem s;
-                    s.rec = it.rec;
-                    s.q_hi = hi;
-                    s.q_lo = hi - P.split + 1 < q_lo ? q_lo : hi - P.split + 1;
-                    if (!push_item(P, s)) break;
-                }
-            }
+            // every range but the first goes to the shared stack, all at once;
+            // the references are counted before any range is published
+            const int extra = (q_hi - P.split - q_lo) / P.split + 1;
+            if (lane == 0) atomicAdd(&((TaskHdr*)(P.arena + it.rec))->refs, extra);
+            __syncwarp();
+            push_ranges(P, it.rec, q_lo, q_hi - P.split, P.split, extra);
             __syncwarp();
             q_lo = q_hi - P.split + 1;
             shared = true;
