@@ -1747,34 +1747,31 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         // branches executed before a member fails on removal (main.cu:1092-1099)
         int need = mindeg(R, m);
         int qmax = m + T.cov;
-        for (int v = 0; v < m; v++) {
-            int k = need - ws.indeg()[v];
-            if (k <= 0) continue;
-            // position of the k-th candidate neighbour of v
-            const uint32_t* row = T.A1 + (int64_t)v * W;
-            int pos = t - 1;
-            int seen = 0;
-            for (int base = 0; base < W * 32; base += 32 * 32) {
-                int w = (base >> 5) + lane;
-                uint32_t x = (w < W) ? (rec_ld(row + w) & CC[w]) : 0u;
-                int c = __popc(x);
-                int inc = wscan(c);
-                int tot = __shfl_sync(QC_FULL, inc, 31);
-                if (seen + tot >= k) {
-                    int need_here = k - seen;
-                    unsigned hit = __ballot_sync(QC_FULL, inc >= need_here && inc - c < need_here);
-                    int src = __ffs(hit) - 1;
-                    int before = __shfl_sync(QC_FULL, inc - c, src);
-                    uint32_t xw = __shfl_sync(QC_FULL, x, src);
-                    int r = need_here - before; // r-th set bit of xw (1-based)
-                    for (int s = 1; s < r; s++) xw &= xw - 1;
-                    int wsrc = (base >> 5) + src;
-                    pos = wsrc * 32 + __ffs(xw) - 1;
-                    break;
+        // lane per member: position of its k-th candidate neighbour (t-1 if it
+        // has fewer), scanning its own row word by word
+        for (int v0 = 0; v0 < m; v0 += 32) {
+            const int v = v0 + lane;
+            int pos = -1;
+            if (v < m) {
+                const int k = need - ws.indeg()[v];
+                if (k > 0) {
+                    const uint32_t* row = T.A1 + (int64_t)v * W;
+                    pos = t - 1;
+                    int seen = 0;
+                    for (int w = 0; w < W; w++) {
+                        uint32_t x = rec_ld(row + w) & CC[w];
+                        const int c = __popc(x);
+                        if (seen + c >= k) {
+                            for (int r = k - seen; r > 1; r--) x &= x - 1; // drop the lower ones
+                            pos = w * 32 + __ffs(x) - 1;
+                            break;
+                        }
+                        seen += c;
+                    }
                 }
-                seen += tot;
             }
-            qmax = pos > qmax ? pos : qmax;
+            const int best = wmax(pos);
+            qmax = best > qmax ? best : qmax;
         }
         q_lo = qmax > t - 1 ? t - 1 : qmax;
         q_hi = t - 1;

@@ -28,8 +28,27 @@ struct emu_dim3 {
 };
 inline thread_local emu_dim3 threadIdx, blockIdx, blockDim, gridDim;
 
+// Sense-reversing barrier of the 32 emulated lanes: lanes spin briefly, then
+// yield the core (the futex-based std::barrier spent most of its time in the
+// kernel with 32 threads per warp on a few cores).
+struct EmuBarrier {
+    std::atomic<int> count{0};
+    std::atomic<int> phase{0};
+    void arrive_and_wait()
+    {
+        int ph = phase.load(std::memory_order_acquire);
+        if (count.fetch_add(1, std::memory_order_acq_rel) == 31) {
+            count.store(0, std::memory_order_relaxed);
+            phase.store(ph + 1, std::memory_order_release);
+            return;
+        }
+        for (int spin = 0; phase.load(std::memory_order_acquire) == ph; spin++)
+            if (spin > 64) std::this_thread::yield();
+    }
+};
+
 struct EmuWarp {
-    std::barrier<> bar{32};
+    EmuBarrier bar;
     uint64_t slot[32];
 };
 inline thread_local EmuWarp* emu_w = nullptr;
@@ -99,7 +118,8 @@ inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
 inline int __ffs(unsigned x) { return x ? __builtin_ctz(x) + 1 : 0; }
 inline int __clz(unsigned x) { return x ? __builtin_clz(x) : 32; }
 inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
-inline void __nanosleep(unsigned) { std::this_thread::yield(); }
+// an idle emulated warp sleeps instead of spinning, so busy warps get the host cores
+inline void __nanosleep(unsigned ns) { std::this_thread::sleep_for(std::chrono::microseconds(20 + ns / 100)); }
 
 inline int atomicAdd(int* a, int v) { return __atomic_fetch_add(a, v, __ATOMIC_SEQ_CST); }
 inline unsigned long long atomicAdd(unsigned long long* a, unsigned long long v)
