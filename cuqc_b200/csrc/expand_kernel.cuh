@@ -105,18 +105,22 @@ __device__ __forceinline__ void bs_zero(uint32_t* d, int W)
     for (int w = lane_id(); w < W; w += 32) d[w] = 0;
     __syncwarp();
 }
+// bits [lo, hi) of word w as a mask
+__device__ __forceinline__ uint32_t range_word(int w, int lo, int hi)
+{
+    int a = lo - w * 32, b = hi - w * 32; // the range relative to the word
+    a = a < 0 ? 0 : (a > 32 ? 32 : a);
+    b = b < 0 ? 0 : (b > 32 ? 32 : b);
+    if (b <= a) return 0u;
+    const uint32_t upto_b = b >= 32 ? ~0u : ((1u << b) - 1u);
+    const uint32_t below_a = a >= 32 ? ~0u : ((1u << a) - 1u);
+    return upto_b & ~below_a;
+}
+
 // d = bits [lo, hi)
 __device__ __forceinline__ void bs_range(uint32_t* d, int W, int lo, int hi)
 {
-    for (int w = lane_id(); w < W; w += 32) {
-        int b0 = w * 32;
-        uint32_t x = 0;
-        for (int k = 0; k < 32; k++) {
-            int v = b0 + k;
-            if (v >= lo && v < hi) x |= 1u << k;
-        }
-        d[w] = x;
-    }
+    for (int w = lane_id(); w < W; w += 32) d[w] = range_word(w, lo, hi);
     __syncwarp();
 }
 __device__ __forceinline__ int bs_count(const uint32_t* a, int W)

@@ -356,9 +356,11 @@ static qc_status launch_shape(qc_context* c, int max_t, Shape& sh)
     const int want_bps = c->cfg.blocks_per_sm > 0 ? c->cfg.blocks_per_sm : 1;
     const size_t sm_budget = 220u << 10; // of the 228 KB of shared memory per SM
     sh.smem_t = 0;
-    if (max_t > 32) {
+    if (max_t > 32 && c->cfg.stage_max >= 0) {
         for (int cand : {256, 192, 128, 96, 64}) {
             int tt = std::min(cand, max_t);
+            if (c->cfg.stage_max > 0) tt = std::min(tt, c->cfg.stage_max);
+            if (tt <= 32) break;
             if (warp_smem_bytes(tt) * sh.wpb * want_bps <= sm_budget) {
                 sh.smem_t = tt;
                 break;

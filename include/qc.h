@@ -122,6 +122,8 @@ typedef struct {
     int32_t split;               /* branches per work item of a task over 32 vertices; 0: 2 */
     int32_t max_blocks;          /* cap on the persistent grid (share the GPU between
                                     contexts running at once); 0: every resident block */
+    int32_t stage_max;           /* largest task (vertices) worked on in shared memory;
+                                    0: as large as the shared memory allows, -1: none */
 } qc_config;
 
 /* Fill a config with defaults (device 0, everything autotuned). */
