@@ -137,14 +137,23 @@ std::string validate(const HostGraph& g, bool need_twohop)
                 return "1-hop rows must be sorted ascending without duplicates";
         }
     }
-    // symmetry: w in N(v) <=> v in N(w)
-    for (int32_t v = 0; v < n; v++) {
-        for (int64_t e = g.off[(size_t)v]; e < g.off[(size_t)v + 1]; e++) {
-            int32_t w = g.adj[(size_t)e];
-            const int32_t* b = g.adj.data() + g.off[(size_t)w];
-            const int32_t* z = g.adj.data() + g.off[(size_t)w + 1];
-            if (!std::binary_search(b, z, v)) return "graph is not undirected (asymmetric 1-hop rows)";
+    // symmetry: w in N(v) <=> v in N(w).  Visiting v in ascending order, the
+    // entries v of the sorted rows N(w) come up in order too, so one cursor
+    // per row checks every edge once; every row must be used up at the end.
+    {
+        std::vector<int64_t> cur(g.off.begin(), g.off.end() - 1);
+        for (int32_t v = 0; v < n; v++) {
+            for (int64_t e = g.off[(size_t)v]; e < g.off[(size_t)v + 1]; e++) {
+                int32_t w = g.adj[(size_t)e];
+                int64_t& c = cur[(size_t)w];
+                if (c >= g.off[(size_t)w + 1] || g.adj[(size_t)c] != v)
+                    return "graph is not undirected (asymmetric 1-hop rows)";
+                c++;
+            }
         }
+        for (int32_t w = 0; w < n; w++)
+            if (cur[(size_t)w] != g.off[(size_t)w + 1])
+                return "graph is not undirected (asymmetric 1-hop rows)";
     }
     if (!need_twohop) return "";
     if ((int64_t)g.off2.size() != (int64_t)n + 1) return "2-hop offsets must have n+1 entries";
