@@ -5,8 +5,8 @@
 // and the start offset of every set (written by the expansion kernel).
 //   1. one warp per set: sort its ids ascending into the sorted buffer and
 //      hash the set (sum of per-id 64-bit mixes, plus its size);
-//   2. radix-sort (hash, set) and drop exact duplicates (equal hash and equal
-//      contents; a hash collision with different contents keeps both);
+//   2. radix-sort (low 32 bits of the hash, set) and drop exact duplicates
+//      (equal contents within a run of equal keys; a collision keeps both);
 //   3. inverted index over the distinct sets: the (vertex, set) incidences,
 //      radix-sorted by vertex and, within a vertex, by set size descending,
 //      give every vertex its posting list with the largest sets first;
@@ -102,9 +102,11 @@ __global__ void dedupe_kernel(const int32_t* srt, const unsigned long long* star
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nsets) return;
-    unsigned long long h = hsorted[i];
+    // sets are sorted by the low 32 bits of their hash; equal sets have equal
+    // hashes, so an equal set sits in the same run of equal low halves
+    const unsigned h = (unsigned)hsorted[i];
     bool dup = false;
-    for (int64_t j = i - 1; j >= 0 && hsorted[j] == h; j--) {
+    for (int64_t j = i - 1; j >= 0 && (unsigned)hsorted[j] == h; j--) {
         if (same_set(srt, starts[osorted[i]], starts[osorted[j]])) {
             dup = true;
             break;
@@ -217,8 +219,40 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
             }
         }
         bool covered = false;
+        int64_t lo = 0, hi = 0;
         if (k > 0 && best_v >= 0) {
-            int64_t lo = poff[best_v], hi = poff[best_v + 1];
+            lo = poff[best_v];
+            hi = poff[best_v + 1];
+            // the largest candidates first, one at a time: every lane looks
+            // its share of S's ids up in the candidate by binary search, so a
+            // typical non-maximal S is settled after a few short steps
+            int tried = 0;
+            for (; lo < hi && tried < 8; lo++, tried++) {
+                if (inc_size(pkey[lo]) <= k) {
+                    lo = hi; // sorted by size: nothing larger follows
+                    break;
+                }
+                unsigned long long bt = starts[post[lo]];
+                int kt = srt[bt];
+                const int32_t* Tt = srt + bt + 1;
+                bool all = true;
+                for (int i = lane; i < k; i += 32) {
+                    int x = srt[a + 1 + i];
+                    int l = 0, r = kt - 1;
+                    while (l < r) {
+                        int mid = (l + r) >> 1;
+                        if (Tt[mid] < x) l = mid + 1;
+                        else r = mid;
+                    }
+                    if (Tt[l] != x) all = false;
+                }
+                if (__all_sync(0xffffffffu, all)) {
+                    covered = true;
+                    break;
+                }
+            }
+        }
+        if (!covered && lo < hi) {
             for (int64_t base = lo; base < hi; base += 32) {
                 int64_t e = base + lane;
                 bool larger = e < hi && inc_size(pkey[e]) > k;
@@ -325,7 +359,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     size_t tb = 0;
     FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)F.hash,
                                         (unsigned long long*)F.hash2, (int32_t*)F.order,
-                                        (int32_t*)F.order2, (int)nsets, 0, 64, s));
+                                        (int32_t*)F.order2, (int)nsets, 0, 32, s));
     size_t tb3 = 0;
     FCK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, (int64_t*)F.len, (int64_t*)F.pos,
                                       (int)nsets, s));
@@ -333,7 +367,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     tb = F.temp_n;
     FCK(cub::DeviceRadixSort::SortPairs(F.temp, tb, (unsigned long long*)F.hash,
                                         (unsigned long long*)F.hash2, (int32_t*)F.order,
-                                        (int32_t*)F.order2, (int)nsets, 0, 64, s));
+                                        (int32_t*)F.order2, (int)nsets, 0, 32, s));
     dedupe_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
         (int32_t*)F.sorted, d_starts, (unsigned long long*)F.hash2, (int32_t*)F.order2, nsets,
         (uint8_t*)F.keep);

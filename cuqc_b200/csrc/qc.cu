@@ -978,9 +978,9 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         std::vector<StackEntry> items((size_t)nroots);
         std::vector<int32_t> ones((size_t)nroots, 1);
         int64_t filled = 0;
-        for (int sh = 0; sh < kStackShards; sh++) {
+        for (int shard = 0; shard < kStackShards; shard++) {
             int cnt = 0;
-            for (int j = sh; j < nroots; j += kStackShards) {
+            for (int j = shard; j < nroots; j += kStackShards) {
                 StackEntry e{};
                 e.rec[0] = meta[(size_t)j].rec;
                 e.n = 1;
@@ -989,12 +989,12 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
                 items[(size_t)(filled + cnt)] = e;
                 cnt++;
             }
-            ctl.stack_top[sh] = cnt;
+            ctl.stack_top[shard] = cnt;
             if (cnt > 0) {
-                CK(cudaMemcpyAsync(c->stack.as<StackEntry>() + (size_t)sh * per_shard,
+                CK(cudaMemcpyAsync(c->stack.as<StackEntry>() + (size_t)shard * per_shard,
                                    items.data() + filled, sizeof(StackEntry) * cnt,
                                    cudaMemcpyHostToDevice, s));
-                CK(cudaMemcpyAsync(c->slot.as<int32_t>() + (size_t)sh * per_shard, ones.data(),
+                CK(cudaMemcpyAsync(c->slot.as<int32_t>() + (size_t)shard * per_shard, ones.data(),
                                    sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, s));
             }
             filled += cnt;
