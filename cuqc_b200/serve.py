@@ -10,6 +10,12 @@
 * Continuous batching: a free slot takes every queued query that fits (up to
   `max_batch`) and mines them in one persistent launch (qc_mine_batch); queries
   that arrive while others are on the GPU wait only for the next free slot.
+* Device-resident graphs: a query's graph object is handed to the library once
+  (one qc_graph per distinct graph object, kept by the server); each slot's
+  context keeps the graphs it has mined on the device, so repeated queries on a
+  graph skip the upload.  A graph object is treated as immutable once queued.
+* Warm-up: optional queries mined once on every slot before the server
+  accepts work, so device buffers are sized before the first timed query.
 * Latency of each query = completion time - arrival time; the server reports
   p50/p99 and instances/s.
 """
@@ -52,9 +58,9 @@ def estimate_bytes(g, gamma, min_size):
 
 
 class Server:
-    def __init__(self, slots=4, device=0, budget_fraction=0.8, max_batch=64, sms=148):
-        import ctypes
+    def __init__(self, slots=2, device=0, budget_fraction=0.8, max_batch=64, sms=148, warm=None):
         self.lock = threading.Condition()
+        self.dev_graphs = {}  # id(graph) -> (graph, DeviceGraph)
         self.queue = deque()
         self.inflight_bytes = 0
         self.completed = []
@@ -65,10 +71,24 @@ class Server:
         share = max(1, sms // slots)
         self.ctxs = [Context(device=device, warps_per_block=4, max_blocks=share)
                      for _ in range(slots)]
+        if warm:
+            for c in self.ctxs:
+                c.mine_batch([self._dev(g) for g, _, _ in warm], [gm for _, gm, _ in warm],
+                             [ms for _, _, ms in warm])
         self.threads = [threading.Thread(target=self._worker, args=(c,), daemon=True)
                         for c in self.ctxs]
         for t in self.threads:
             t.start()
+
+    def _dev(self, g):
+        """The library graph for a query's graph object (made once)."""
+        if isinstance(g, DeviceGraph):
+            return g
+        hit = self.dev_graphs.get(id(g))
+        if hit is None or hit[0] is not g:
+            hit = (g, DeviceGraph.from_graph(g))
+            self.dev_graphs[id(g)] = hit
+        return hit[1]
 
     @staticmethod
     def _free_bytes(device):
@@ -111,8 +131,9 @@ class Server:
                 time.sleep(0.0005)
                 continue
             try:
-                res = ctx.mine_batch([r.graph for r in batch], [r.gamma for r in batch],
-                                     [r.min_size for r in batch])
+                with self.lock:
+                    dgs = [self._dev(r.graph) for r in batch]
+                res = ctx.mine_batch(dgs, [r.gamma for r in batch], [r.min_size for r in batch])
                 now = time.perf_counter()
                 for r, x in zip(batch, res):
                     r.result, r.finish = x, now
