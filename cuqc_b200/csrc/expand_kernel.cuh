@@ -662,31 +662,30 @@ __device__ bool push_item(const ExpandParams& P, const WorkItem& it)
     return push_entry(P, e, home_shard());
 }
 
-// Whole warp: push `count` branch ranges of record `rec` onto the warp's home
-// shard with one reservation; range c covers the `split` branches ending at
-// hi_first - c*split (not below q_lo).  Every lane fills a share of the slots.
-// Returns false when the shard is full (the run then stops with
+// Whole warp: push `count` branch ranges of record `rec`, range c (covering
+// the `split` branches ending at hi_first - c*split, not below q_lo) onto
+// shard (home + c) mod S, so that many waiting warps can take them at once
+// instead of queueing on one shard's top.  Every lane pushes a share.
+// Returns false when a shard is full (the run then stops with
 // ST_TASK_OVERFLOW) or a slot wait gave up.
 __device__ bool push_ranges(const ExpandParams& P, unsigned long long rec, int q_lo, int hi_first,
                             int split, int count)
 {
     const int lane = lane_id();
-    const int shard = home_shard();
-    int base = 0;
-    if (lane == 0) {
-        atomicAdd(&P.ctl->pending, count);
-        base = atomicAdd(&P.ctl->stack_top[shard], count);
-        if (base + count > P.ctl->stack_cap) {
-            set_status(P, ST_TASK_OVERFLOW);
-            atomicSub(&P.ctl->pending, count);
-            base = -1;
-        }
-    }
-    base = __shfl_sync(QC_FULL, base, 0);
-    if (base < 0) return false;
+    const int home = home_shard();
+    if (lane == 0) atomicAdd(&P.ctl->pending, count);
+    __syncwarp();
     int ok = 1;
     for (int c = lane; c < count; c += 32) {
-        const long long at = (long long)shard * P.ctl->stack_cap + base + c;
+        const int shard = (home + c) % kStackShards;
+        const int idx = atomicAdd(&P.ctl->stack_top[shard], 1);
+        if (idx >= P.ctl->stack_cap) {
+            set_status(P, ST_TASK_OVERFLOW);
+            atomicSub(&P.ctl->pending, 1);
+            ok = 0;
+            continue;
+        }
+        const long long at = (long long)shard * P.ctl->stack_cap + idx;
         unsigned long long t0 = now_ns();
         unsigned spins = 0;
         bool got = true;
@@ -878,6 +877,8 @@ __device__ void donate(const ExpandParams& P, Ws& ws)
     int given = 0;
     const int home = home_shard();
     for (int pushes = 0; given < give && pushes < 8; pushes++) {
+        // successive bundles go to successive shards (see push_ranges)
+        const int shard = (home + pushes) % kStackShards;
         int k = give - given < per ? give - given : per;
         StackEntry e;
         for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[given + i] : 0ull;
@@ -885,7 +886,7 @@ __device__ void donate(const ExpandParams& P, Ws& ws)
         e.q_lo = -1;
         e.q_hi = -1;
         e.pad = 0;
-        if (!push_entry(P, e, home)) break;
+        if (!push_entry(P, e, shard)) break;
         given += k;
     }
     for (int i = given; i < n; i++) ws.sm->lstack[i - given] = ws.sm->lstack[i];
