@@ -840,8 +840,11 @@ __device__ int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out)
                 out.rec = e.rec[0];
                 out.q_lo = e.q_lo;
                 out.q_hi = e.q_hi;
-                for (int i = e.n - 1; i >= 1 && ws.sm->lcount < kLocalStack; i--)
-                    ws.sm->lstack[ws.sm->lcount++] = e.rec[i];
+                for (int i = e.n - 1; i >= 1 && ws.sm->lcount < kLocalStack; i--) {
+                    LocalTask lt{};
+                    lt.rec = e.rec[i]; // header read and checked when taken
+                    ws.sm->lstack[ws.sm->lcount++] = lt;
+                }
             }
         }
     }
@@ -853,12 +856,26 @@ __device__ int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out)
 // atomics); only when that stack is full does a child go to the shared one.
 // `pending` counts shared-stack items plus warps that hold work, so local
 // children change it only when they are donated (push_item).
-__device__ void schedule_child(const ExpandParams& P, Ws& ws, const WorkItem& it)
+__device__ void schedule_child(const ExpandParams& P, Ws& ws, unsigned long long rec, int t, int m,
+                               int W, int cls, int inst)
 {
     if (ws.sm->lcount < kLocalStack) {
-        ws.sm->lstack[ws.sm->lcount++] = it.rec;
+        LocalTask lt;
+        lt.rec = rec;
+        lt.t = t;
+        lt.m = m;
+        lt.W = W;
+        lt.cls = cls;
+        lt.inst = inst;
+        lt.pad = 0;
+        ws.sm->lstack[ws.sm->lcount++] = lt;
         return;
     }
+    // published to other warps: push_entry fences the record before the hand-off
+    WorkItem it;
+    it.rec = rec;
+    it.q_lo = -1;
+    it.q_hi = -1;
     push_item(P, it);
 }
 
@@ -869,7 +886,8 @@ __device__ void donate(const ExpandParams& P, Ws& ws)
 {
     int n = ws.sm->lcount;
     if (n < 2) return;
-    int hungry = *(volatile int*)&P.ctl->idle_warps;
+    // read when the previous item started (the read overlapped its work)
+    int hungry = ws.sm->hungry;
     if (hungry <= 0) return;
     int give = n - 1;
     int per = (give + hungry - 1) / hungry;
@@ -881,7 +899,7 @@ __device__ void donate(const ExpandParams& P, Ws& ws)
         const int shard = (home + pushes) % kStackShards;
         int k = give - given < per ? give - given : per;
         StackEntry e;
-        for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[given + i] : 0ull;
+        for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[given + i].rec : 0ull;
         e.n = k;
         e.q_lo = -1;
         e.q_hi = -1;
@@ -1149,12 +1167,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
     if (lane == 0) {
         ws.sm->cnt.children++;
         ws.sm->cnt.child_vertices += (unsigned long long)tc;
-        __threadfence();
-        WorkItem it;
-        it.rec = at;
-        it.q_lo = -1;
-        it.q_hi = -1;
-        schedule_child(P, ws, it);
+        schedule_child(P, ws, at, tc, m, Wc, cls, T.inst);
     }
     __syncwarp();
 }
@@ -1537,12 +1550,7 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
     if (lane == 0) {
         ws.sm->cnt.children++;
         ws.sm->cnt.child_vertices += (unsigned long long)tc;
-        __threadfence();
-        WorkItem it;
-        it.rec = at;
-        it.q_lo = -1;
-        it.q_hi = -1;
-        schedule_child(P, ws, it);
+        schedule_child(P, ws, at, tc, m2, 1, cls, T.inst);
     }
     __syncwarp();
 }
@@ -1886,6 +1894,7 @@ __global__ void expand_kernel(ExpandParams P)
     }
     if (lane == 0) {
         sm->lcount = 0;
+        sm->hungry = 0;
         sm->tab_inst = -1;
         sm->cnt = WarpCount{};
     }
@@ -1903,15 +1912,27 @@ __global__ void expand_kernel(ExpandParams P)
         if (__shfl_sync(QC_FULL, local, 0)) {
             if (lane == 0) {
                 donate(P, ws);
-                it.rec = sm->lstack[--sm->lcount];
+                const LocalTask lt = sm->lstack[--sm->lcount];
+                it.rec = lt.rec;
                 it.q_lo = -1;
                 it.q_hi = -1;
                 r = 1;
+                if (lt.t > 0) {
+                    // a child this warp wrote: its header is known
+                    hv.t = lt.t;
+                    hv.m = lt.m;
+                    hv.cov = 0;
+                    hv.W = lt.W;
+                    hv.cls = lt.cls;
+                    hv.inst = lt.inst;
+                    hv.refs = 1;
+                    r = 2;
+                }
             }
         } else {
             r = pop_item(P, ws, it);
         }
-        if (lane == 0 && r > 0 && !item_ok(P, it, hv)) r = -1;
+        if (lane == 0 && r == 1 && !item_ok(P, it, hv)) r = -1;
         r = __shfl_sync(QC_FULL, r, 0);
         if (r <= 0) break;
         it.rec = __shfl_sync(QC_FULL, it.rec, 0);
@@ -1922,10 +1943,10 @@ __global__ void expand_kernel(ExpandParams P)
         hv.cov = __shfl_sync(QC_FULL, hv.cov, 0);
         hv.W = __shfl_sync(QC_FULL, hv.W, 0);
         hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
-        __threadfence();
+        // idle warps, read now and used when the next local task is taken
+        if (lane == 0) sm->hungry = *(volatile int*)&P.ctl->idle_warps;
         bool shared = process_item(P, ws, wss, stage, it, hv);
         __syncwarp();
-        __threadfence();
         if (lane == 0) {
             release_record(P, ws, it.rec, !shared, hv);
             // the warp stays counted in `pending` while its own stack holds work

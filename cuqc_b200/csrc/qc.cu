@@ -79,7 +79,14 @@ static std::atomic<unsigned long long> g_graph_serial{1};
 struct qc_graph {
     HostGraph h;
     unsigned long long serial = g_graph_serial.fetch_add(1); // identity for device caches
+    mutable std::atomic<int> resident_in{0}; // contexts holding a device copy
 };
+
+// Graphs freed while contexts still hold their device copies: serial ->
+// contexts yet to notice.  A context reuses such a copy's buffers for the
+// next graph it uploads instead of allocating new ones.
+static std::mutex g_dead_mu;
+static std::unordered_map<unsigned long long, int> g_dead;
 
 struct qc_result {
     std::vector<int32_t> sets;
@@ -190,6 +197,13 @@ extern "C" void qc_context_free(qc_context* c)
 {
     if (!c) return;
     cudaSetDevice(c->cfg.device);
+    {
+        std::lock_guard<std::mutex> lk(g_dead_mu);
+        for (auto& kv : c->res) {
+            auto d = g_dead.find(kv.first);
+            if (d != g_dead.end() && --d->second <= 0) g_dead.erase(d);
+        }
+    }
     for (auto& kv : c->res) kv.second->release();
     c->res.clear();
     for (DevBuf* b : {&c->pos, &c->ids, &c->md, &c->ubt, &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts,
@@ -256,7 +270,16 @@ extern "C" const int64_t* qc_graph_offsets(const qc_graph* g) { return g ? g->h.
 extern "C" const int32_t* qc_graph_neighbors(const qc_graph* g) { return g ? g->h.adj.data() : nullptr; }
 extern "C" const int64_t* qc_graph_twohop_offsets(const qc_graph* g) { return g ? g->h.off2.data() : nullptr; }
 extern "C" const int32_t* qc_graph_twohop_neighbors(const qc_graph* g) { return g ? g->h.adj2.data() : nullptr; }
-extern "C" void qc_graph_free(qc_graph* g) { delete g; }
+extern "C" void qc_graph_free(qc_graph* g)
+{
+    if (!g) return;
+    int held = g->resident_in.load();
+    if (held > 0) {
+        std::lock_guard<std::mutex> lk(g_dead_mu);
+        g_dead[g->serial] += held;
+    }
+    delete g;
+}
 
 // ------------------------------------------------------------------
 // device kernels: root task record
@@ -407,7 +430,24 @@ static qc_status make_resident(qc_context* c, const qc_graph* g,
     cudaStream_t s = c->stream;
     auto it = c->res.find(g->serial);
     if (it == c->res.end()) {
-        std::unique_ptr<ResidentGraph> rg(new ResidentGraph());
+        std::unique_ptr<ResidentGraph> rg;
+        {
+            // reuse the buffers of a copy whose graph has been freed
+            std::lock_guard<std::mutex> lk(g_dead_mu);
+            if (!g_dead.empty()) {
+                for (auto j = c->res.begin(); j != c->res.end(); ++j) {
+                    auto d = g_dead.find(j->first);
+                    if (d == g_dead.end()) continue;
+                    if (--d->second <= 0) g_dead.erase(d);
+                    CK(cudaStreamSynchronize(s)); // queued work may still read it
+                    rg = std::move(j->second);
+                    c->res_bytes -= rg->bytes;
+                    c->res.erase(j);
+                    break;
+                }
+            }
+        }
+        if (!rg) rg.reset(new ResidentGraph());
         CK(upload(rg->off, h.off, s));
         CK(upload(rg->adj, h.adj, s));
         CK(upload(rg->off2, h.off2, s));
@@ -415,6 +455,7 @@ static qc_status make_resident(qc_context* c, const qc_graph* g,
         rg->bytes = rg->off.n + rg->adj.n + rg->off2.n + rg->adj2.n;
         c->res_bytes += rg->bytes;
         it = c->res.emplace(g->serial, std::move(rg)).first;
+        g->resident_in.fetch_add(1);
         while (c->res_bytes > c->res_budget && c->res.size() > 1) {
             auto victim = c->res.end();
             for (auto j = c->res.begin(); j != c->res.end(); ++j) {

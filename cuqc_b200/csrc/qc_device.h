@@ -192,11 +192,20 @@ constexpr int kTabCache = 128;
 // warp itself) before it pushes further children to the shared stack.
 constexpr int kLocalStack = 48;
 
+// A fresh task on a warp's own stack.  A child the warp wrote itself carries
+// its header (t > 0), so taking it needs no read of the record's header; a
+// task taken from a donated bundle has t = 0 and is read and checked.
+struct LocalTask {
+    unsigned long long rec;
+    int32_t t, m, W, cls, inst, pad;
+};
+
 // Per-warp state in shared memory: everything a warp touches on every task.
 struct WarpSmem {
     WarpCount cnt;
-    unsigned long long lstack[kLocalStack]; // this warp's own fresh child tasks (record offsets)
-    int32_t lcount;                          // entries on lstack
+    LocalTask lstack[kLocalStack]; // this warp's own fresh child tasks
+    int32_t lcount;                // entries on lstack
+    int32_t hungry;                // idle warps seen when the current item started
     int32_t tab_inst;            // instance whose gamma tables are cached (-1: none)
     unsigned long long fhead[kArenaClasses]; // private free lists: offset/16+1, 0 = empty
     int32_t fcount[kArenaClasses];

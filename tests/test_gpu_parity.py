@@ -194,3 +194,19 @@ def test_tune_picks_a_shape_and_keeps_results():
         assert best["warps_per_block"] in (2, 4, 8) and best["blocks_per_sm"] in (1, 2)
         assert best["split"] in (1, 2, 4)
         assert c.mine(g, 0.8, 10).sets == want
+
+
+def test_freed_graph_buffers_are_reused_correctly():
+    """A context keeps uploaded graphs on the device; once a graph is freed,
+    the next new graph reuses its device buffers.  Results stay exact across
+    a sequence of upload / free / upload of graphs of different sizes."""
+    gs = [graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11),
+          graphs.random_small(90, 0.2, 5, planted=2, size=12, density=0.95),
+          graphs.erdos_renyi_planted(500, 0.025, 4, 18, 0.95, seed=12)]
+    want = [oracle.solve(g, 0.8, 8)[0] for g in gs]
+    with Q.Context(device=0) as c:
+        for rnd in range(3):
+            for g, w in zip(gs, want):
+                dg = Q.DeviceGraph.from_graph(g)
+                assert c.mine(dg, 0.8, 8).sets == w
+                dg.close()
