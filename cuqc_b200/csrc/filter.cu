@@ -20,6 +20,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -225,15 +226,23 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
             hi = poff[best_v + 1];
             // the largest candidates first, one at a time: every lane looks
             // its share of S's ids up in the candidate by binary search, so a
-            // typical non-maximal S is settled after a few short steps
-            int tried = 0;
-            for (; lo < hi && tried < 8; lo++, tried++) {
-                if (inc_size(pkey[lo]) <= k) {
-                    lo = hi; // sorted by size: nothing larger follows
-                    break;
-                }
-                unsigned long long bt = starts[post[lo]];
-                int kt = srt[bt];
+            // typical non-maximal S is settled after a few short steps.  Lanes
+            // 0..7 fetch the first eight candidates' sizes and starts at once.
+            const int64_t e = lo + lane;
+            const bool valid = lane < 8 && e < hi;
+            const bool larger = valid && inc_size(pkey[e]) > k;
+            unsigned long long my_bt = 0;
+            int my_kt = 0;
+            if (larger) {
+                my_bt = starts[post[e]];
+                my_kt = srt[my_bt];
+            }
+            const unsigned lg = __ballot_sync(0xffffffffu, larger); // a prefix of lanes
+            const unsigned vd = __ballot_sync(0xffffffffu, valid);
+            const int ncand = __popc(lg);
+            for (int c = 0; c < ncand; c++) {
+                const unsigned long long bt = __shfl_sync(0xffffffffu, my_bt, c);
+                const int kt = __shfl_sync(0xffffffffu, my_kt, c);
                 const int32_t* Tt = srt + bt + 1;
                 bool all = true;
                 for (int i = lane; i < k; i += 32) {
@@ -251,6 +260,9 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
                     break;
                 }
             }
+            // sorted by size: once a fetched candidate is not larger, none after it is
+            if (lg != vd) lo = hi;
+            else lo += ncand;
         }
         if (!covered && lo < hi) {
             for (int64_t base = lo; base < hi; base += 32) {
@@ -376,18 +388,16 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
         (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep, (int64_t*)F.len);
     tb = F.temp_n;
     FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos, (int)nsets, s));
-    int64_t ilast_pos = 0, ilast_len = 0;
-    FCK(cudaMemcpyAsync(&ilast_pos, (int64_t*)F.pos + nsets - 1, sizeof(int64_t),
-                        cudaMemcpyDeviceToHost, s));
-    FCK(cudaMemcpyAsync(&ilast_len, (int64_t*)F.len + nsets - 1, sizeof(int64_t),
-                        cudaMemcpyDeviceToHost, s));
-    FCK(cudaStreamSynchronize(s));
-    const int64_t total = ilast_pos + ilast_len;
+    // sized by a bound (every emitted set's ids), so the host need not wait
+    // for the count of the kept sets' incidences; the unused tail holds keys
+    // above every real key and sorts to the end
+    const int64_t total = std::max<int64_t>(nints - nsets, 1);
     if (total > INT32_MAX) return "filter: more than 2^31 vertex incidences in the emitted sets";
-    ENS(ikey, ikey_n, sizeof(unsigned long long) * std::max<int64_t>(total, 1));
-    ENS(ikey2, ikey2_n, sizeof(unsigned long long) * std::max<int64_t>(total, 1));
-    ENS(ival, ival_n, sizeof(int32_t) * std::max<int64_t>(total, 1));
-    ENS(post, post_n, sizeof(int32_t) * std::max<int64_t>(total, 1));
+    ENS(ikey, ikey_n, sizeof(unsigned long long) * total);
+    ENS(ikey2, ikey2_n, sizeof(unsigned long long) * total);
+    ENS(ival, ival_n, sizeof(int32_t) * total);
+    ENS(post, post_n, sizeof(int32_t) * total);
+    FCK(cudaMemsetAsync(F.ikey, 0xff, sizeof(unsigned long long) * total, s));
     inc_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
                                            (int64_t*)F.pos, (unsigned long long*)F.ikey,
                                            (int32_t*)F.ival);
@@ -430,20 +440,35 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     FCK(cudaStreamSynchronize(s));
 #undef ENS
     // lexicographic order of the (already sorted) survivors
-    std::vector<std::pair<int64_t, int32_t>> idx;
+    // (key of the first two ids, offset): the key orders most pairs at once;
+    // equal keys fall back to comparing the remaining ids
+    struct Ent {
+        uint64_t key;
+        int64_t at;
+    };
+    std::vector<Ent> idx;
     for (int64_t p = 0; p < out_ints;) {
-        idx.emplace_back(p, flat[(size_t)p]);
-        p += 1 + flat[(size_t)p];
+        const int32_t k = flat[(size_t)p];
+        uint64_t key = k >= 1 ? (uint64_t)(uint32_t)flat[(size_t)p + 1] << 32 : 0;
+        if (k >= 2) key |= (uint64_t)(uint32_t)flat[(size_t)p + 2] + 1u;
+        idx.push_back(Ent{key, p});
+        p += 1 + k;
     }
-    std::sort(idx.begin(), idx.end(), [&](const auto& x, const auto& y) {
-        return std::lexicographical_compare(flat.begin() + x.first + 1,
-                                            flat.begin() + x.first + 1 + x.second,
-                                            flat.begin() + y.first + 1,
-                                            flat.begin() + y.first + 1 + y.second);
+    const int32_t* F0 = flat.data();
+    std::sort(idx.begin(), idx.end(), [&](const Ent& x, const Ent& y) {
+        if (x.key != y.key) return x.key < y.key;
+        const int32_t kx = F0[x.at], ky = F0[y.at];
+        if (kx < 2 || ky < 2) return kx < ky;
+        return std::lexicographical_compare(F0 + x.at + 3, F0 + x.at + 1 + kx, F0 + y.at + 3,
+                                            F0 + y.at + 1 + ky);
     });
-    host_out.reserve((size_t)out_ints);
-    for (auto& pr : idx)
-        host_out.insert(host_out.end(), flat.begin() + pr.first, flat.begin() + pr.first + 1 + pr.second);
+    host_out.resize((size_t)out_ints);
+    int32_t* o = host_out.data();
+    for (const Ent& e : idx) {
+        const int32_t k = F0[e.at];
+        std::memcpy(o, F0 + e.at, sizeof(int32_t) * (size_t)(k + 1));
+        o += k + 1;
+    }
     host_nsets = (int64_t)idx.size();
     return "";
 }
