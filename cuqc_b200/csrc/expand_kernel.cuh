@@ -1624,6 +1624,10 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     T.a1 = act ? rec_ld(V.A1 + lane) : 0u;
     T.a2 = act ? rec_ld(V.A2 + lane) : 0u;
     T.l2 = act ? rec_ld(V.l2 + lane) : 0;
+    if (__any_sync(QC_FULL, act && (T.id < 0 || T.id >= R.n))) {
+        if (lane == 0) check_fail(P, 8, V.rec); // a vertex id outside the instance
+        return;
+    }
     const int t = T.t, m = T.m;
     unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
     int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
@@ -1657,7 +1661,8 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     int qlo = rmax(pos);
     qlo = qlo > m + T.cov ? qlo : m + T.cov;
     if (qlo > t - 1) return;
-    if (*(volatile int*)&P.ctl->status) return;
+    // run status as read when the previous item started (no round trip here)
+    if (ws.sm->stat) return;
     for (int q = t - 1; q >= qlo; q--) branch_small(P, R, ws, T, q);
 }
 
@@ -1695,7 +1700,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     R.md_s = ws.sm->md;
     R.ubt_s = ws.sm->ubt;
     bool shared = it.q_lo >= 0;
-    {
+    if (!(it.q_lo < 0 && t <= 32 && P.small_path)) { // the register path checks its own ids
         int bad = 0;
         for (int v = lane; v < t; v += 32) {
             int id = rec_ld(T.ids + v);
@@ -1895,6 +1900,7 @@ __global__ void expand_kernel(ExpandParams P)
     if (lane == 0) {
         sm->lcount = 0;
         sm->hungry = 0;
+        sm->stat = 0;
         sm->tab_inst = -1;
         sm->cnt = WarpCount{};
     }
@@ -1943,11 +1949,18 @@ __global__ void expand_kernel(ExpandParams P)
         hv.cov = __shfl_sync(QC_FULL, hv.cov, 0);
         hv.W = __shfl_sync(QC_FULL, hv.W, 0);
         hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
-        // idle warps, read now and used when the next local task is taken
-        if (lane == 0) sm->hungry = *(volatile int*)&P.ctl->idle_warps;
+        // idle warps and run status, read now and looked at while the next
+        // item is taken and run, so the reads overlap this item's work
+        int idle_now = 0, stat_now = 0;
+        if (lane == 0) {
+            idle_now = *(volatile int*)&P.ctl->idle_warps;
+            stat_now = *(volatile int*)&P.ctl->status;
+        }
         bool shared = process_item(P, ws, wss, stage, it, hv);
         __syncwarp();
         if (lane == 0) {
+            sm->hungry = idle_now;
+            sm->stat = stat_now;
             release_record(P, ws, it.rec, !shared, hv);
             // the warp stays counted in `pending` while its own stack holds work
             if (sm->lcount == 0) atomicSub(&P.ctl->pending, 1);

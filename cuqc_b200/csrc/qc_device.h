@@ -205,7 +205,8 @@ struct WarpSmem {
     WarpCount cnt;
     LocalTask lstack[kLocalStack]; // this warp's own fresh child tasks
     int32_t lcount;                // entries on lstack
-    int32_t hungry;                // idle warps seen when the current item started
+    int32_t hungry;                // idle warps seen when the previous item started
+    int32_t stat;                  // run status seen when the previous item started
     int32_t tab_inst;            // instance whose gamma tables are cached (-1: none)
     unsigned long long fhead[kArenaClasses]; // private free lists: offset/16+1, 0 = empty
     int32_t fcount[kArenaClasses];
