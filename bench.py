@@ -80,18 +80,63 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region.
+
+    Reads NVML (the library nvidia-smi reports from) every 2 ms from a thread, so
+    a timed region of a few tens of milliseconds still gets samples; falls back
+    to `nvidia-smi -lms 200` where NVML is missing.  Read-only: no setting of the
+    GPU is touched."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.002):
         self.device = device
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.rows = []
         self.path = tempfile.mktemp(suffix=".csv")
 
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(
+                uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), [n for n in self.NAMES if r & bits[n]]))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
+
     def __enter__(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.nvml = nv
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -103,6 +148,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.nvml:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -112,6 +160,13 @@ class ClockSampler:
             self.f.close()
 
     def summary(self):
+        if self.nvml:
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.sm_max, "reasons": ["no samples"],
+                        "samples": 0, "source": "nvml"}
+            return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.sm_max,
+                    "reasons": sorted({n for r in self.rows for n in r[1]}),
+                    "samples": len(self.rows), "source": "nvml, every 2 ms"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
@@ -122,11 +177,10 @@ class ClockSampler:
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi -lms 200"}
 
 
 def make_graph(w):

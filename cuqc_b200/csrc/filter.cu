@@ -3,16 +3,19 @@
 //
 // Input: the emitted sets in the device result buffer, [k, id_1..id_k] each,
 // and the start offset of every set (written by the expansion kernel).
-//   1. one warp per set: sort its ids ascending into the sorted buffer and
-//      hash the set (sum of per-id 64-bit mixes, plus its size);
+//   1. one warp per set: sort its ids ascending into the sorted buffer, hash
+//      the set (sum of per-id 64-bit mixes, plus its size) and build its
+//      256-bit signature;
 //   2. radix-sort (low 32 bits of the hash, set) and drop exact duplicates
 //      (equal contents within a run of equal keys; a collision keeps both);
 //   3. inverted index over the distinct sets: the (vertex, set) incidences,
 //      radix-sorted by vertex and, within a vertex, by set size descending,
 //      give every vertex its posting list with the largest sets first;
 //   4. one warp per distinct set S: scan the posting list of S's rarest
-//      vertex while its sets are larger than S and test S against each by a
-//      sorted merge (largest first, so a non-maximal S usually stops early);
+//      vertex while its sets are larger than S, 128 candidates a round, and
+//      test each by its 256-bit signature (a bit per hashed id, written in
+//      step 1): a candidate whose signature lacks one of S's bits cannot
+//      contain S; the few that pass are checked exactly by the whole warp.
 //      S is maximal iff no such set contains it;
 //   5. the maximal sets are compacted and copied back; the host orders them
 //      lexicographically (the order the reference's prefix tree writes).
@@ -38,10 +41,13 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x)
     return x ^ (x >> 31);
 }
 
-// 1. per-set sort + hash (one warp per set)
+// signature bit of an id: the top 8 bits of a multiplicative (Fibonacci) hash
+__device__ __forceinline__ unsigned sig_bit(int32_t v) { return ((unsigned)v * 0x9E3779B1u) >> 24; }
+
+// 1. per-set sort + hash + signature (one warp per set)
 __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* starts, int64_t nsets,
                                  int32_t* sorted, unsigned long long* hash, int32_t* order,
-                                 int32_t* sizes)
+                                 int32_t* sizes, uint4* sig)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -52,11 +58,19 @@ __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* s
         const int32_t* in = res + a + 1;
         int32_t* out = sorted + a + 1;
         unsigned long long h = 0;
+        unsigned sg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int i = lane; i < k; i += 32) {
-            out[i] = in[i];
-            h += mix64((unsigned long long)(unsigned)in[i]);
+            const int32_t v = in[i];
+            out[i] = v;
+            h += mix64((unsigned long long)(unsigned)v);
+            const unsigned b = sig_bit(v);
+#pragma unroll
+            for (int w = 0; w < 8; w++)
+                if ((int)(b >> 5) == w) sg[w] |= 1u << (b & 31);
         }
         for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+#pragma unroll
+        for (int w = 0; w < 8; w++) sg[w] = __reduce_or_sync(0xffffffffu, sg[w]);
         __syncwarp();
         // bitonic sort of out[0..k), all compare-exchanges ascending (mirror
         // step, then half-cleaners), so virtual +inf padding at [k, N) never
@@ -83,6 +97,8 @@ __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* s
             hash[s] = mix64(h ^ ((unsigned long long)k << 40));
             order[s] = (int32_t)s;
             sizes[s] = k;
+            sig[2 * s] = make_uint4(sg[0], sg[1], sg[2], sg[3]);
+            sig[2 * s + 1] = make_uint4(sg[4], sg[5], sg[6], sg[7]);
         }
     }
 }
@@ -168,27 +184,41 @@ __global__ void inc_offsets_kernel(const unsigned long long* key, int64_t total,
     poff[v] = lo;
 }
 
-// is sorted set S (at a) a subset of sorted set T (at b)?  |T| > |S|
-__device__ bool subset_of(const int32_t* srt, unsigned long long a, unsigned long long b)
+// does signature T have every bit of signature S?
+__device__ __forceinline__ bool sig_covers(const uint4& s0, const uint4& s1, const uint4& t0,
+                                           const uint4& t1)
 {
-    int ks = srt[a], kt = srt[b];
-    int i = 0, j = 0;
-    const int32_t* S = srt + a + 1;
-    const int32_t* T = srt + b + 1;
-    while (i < ks && j < kt) {
-        if (ks - i > kt - j) return false;
-        int x = S[i], y = T[j];
-        if (x == y) { i++; j++; }
-        else if (x > y) j++;
-        else return false;
-    }
-    return i == ks;
+    return ((s0.x & ~t0.x) | (s0.y & ~t0.y) | (s0.z & ~t0.z) | (s0.w & ~t0.w) | (s1.x & ~t1.x) |
+            (s1.y & ~t1.y) | (s1.z & ~t1.z) | (s1.w & ~t1.w)) == 0;
 }
+
+// Is sorted set S (k ids at srt[a+1..]) contained in sorted set T (at bt)?
+// Warp-wide: every lane looks its share of S's ids up in T by binary search.
+__device__ __forceinline__ bool warp_subset(const int32_t* srt, unsigned long long a, int k,
+                                            unsigned long long bt, int lane)
+{
+    const int kt = srt[bt];
+    const int32_t* T = srt + bt + 1;
+    bool all = true;
+    for (int i = lane; i < k; i += 32) {
+        const int x = srt[a + 1 + i];
+        int l = 0, r = kt - 1;
+        while (l < r) {
+            const int mid = (l + r) >> 1;
+            if (T[mid] < x) l = mid + 1;
+            else r = mid;
+        }
+        if (T[l] != x) all = false;
+    }
+    return __all_sync(0xffffffffu, all);
+}
+
+constexpr int MAX_ROUND = 4; // candidate groups of 32 fetched per round
 
 // 4. superset test, one warp per kept set
 __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
                                const uint8_t* keep, const int64_t* poff, const int32_t* post,
-                               const unsigned long long* pkey, uint8_t* maximal)
+                               const unsigned long long* pkey, const uint4* sig, uint8_t* maximal)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -220,73 +250,55 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
             }
         }
         bool covered = false;
-        int64_t lo = 0, hi = 0;
         if (k > 0 && best_v >= 0) {
-            lo = poff[best_v];
-            hi = poff[best_v + 1];
-            // the largest candidates first, one at a time: every lane looks
-            // its share of S's ids up in the candidate by binary search, so a
-            // typical non-maximal S is settled after a few short steps.  Lanes
-            // 0..7 fetch the first eight candidates' sizes and starts at once.
-            const int64_t e = lo + lane;
-            const bool valid = lane < 8 && e < hi;
-            const bool larger = valid && inc_size(pkey[e]) > k;
-            unsigned long long my_bt = 0;
-            int my_kt = 0;
-            if (larger) {
-                my_bt = starts[post[e]];
-                my_kt = srt[my_bt];
-            }
-            const unsigned lg = __ballot_sync(0xffffffffu, larger); // a prefix of lanes
-            const unsigned vd = __ballot_sync(0xffffffffu, valid);
-            const int ncand = __popc(lg);
-            for (int c = 0; c < ncand; c++) {
-                const unsigned long long bt = __shfl_sync(0xffffffffu, my_bt, c);
-                const int kt = __shfl_sync(0xffffffffu, my_kt, c);
-                const int32_t* Tt = srt + bt + 1;
-                bool all = true;
-                for (int i = lane; i < k; i += 32) {
-                    int x = srt[a + 1 + i];
-                    int l = 0, r = kt - 1;
-                    while (l < r) {
-                        int mid = (l + r) >> 1;
-                        if (Tt[mid] < x) l = mid + 1;
-                        else r = mid;
+            const uint4 s0 = sig[2 * s], s1 = sig[2 * s + 1];
+            const int64_t lo = poff[best_v], hi = poff[best_v + 1];
+            // the list is ordered by size, largest first: past the sets larger
+            // than S nothing can contain it
+            for (int64_t base = lo; base < hi; base += 32 * MAX_ROUND) {
+                bool larger[MAX_ROUND];
+                int32_t t[MAX_ROUND];
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    const int64_t e = base + u * 32 + lane;
+                    larger[u] = e < hi && inc_size(pkey[e]) > k;
+                    t[u] = larger[u] ? post[e] : 0;
+                }
+                bool pass[MAX_ROUND];
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    pass[u] = false;
+                    if (larger[u]) {
+                        const uint4 t0 = sig[2 * (int64_t)t[u]], t1 = sig[2 * (int64_t)t[u] + 1];
+                        pass[u] = sig_covers(s0, s1, t0, t1);
                     }
-                    if (Tt[l] != x) all = false;
                 }
-                if (__all_sync(0xffffffffu, all)) {
-                    covered = true;
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    unsigned pb = __ballot_sync(0xffffffffu, pass[u]);
+                    while (pb && !covered) {
+                        const int c = __ffs(pb) - 1;
+                        pb &= pb - 1;
+                        const int32_t tt = __shfl_sync(0xffffffffu, t[u], c);
+                        covered = warp_subset(srt, a, k, starts[tt], lane);
+                    }
+                }
+                if (covered || __ballot_sync(0xffffffffu, larger[MAX_ROUND - 1]) != 0xffffffffu)
                     break;
-                }
-            }
-            // sorted by size: once a fetched candidate is not larger, none after it is
-            if (lg != vd) lo = hi;
-            else lo += ncand;
-        }
-        if (!covered && lo < hi) {
-            for (int64_t base = lo; base < hi; base += 32) {
-                int64_t e = base + lane;
-                bool larger = e < hi && inc_size(pkey[e]) > k;
-                if (larger && subset_of(srt, a, starts[post[e]])) covered = true;
-                // the list is ordered by size, largest first: past the sets
-                // larger than S nothing can contain it
-                unsigned more = __ballot_sync(0xffffffffu, larger);
-                if (__any_sync(0xffffffffu, covered) || more != 0xffffffffu) break;
             }
         }
-        covered = __any_sync(0xffffffffu, covered);
         if (lane == 0) maximal[s] = covered ? 0 : 1;
     }
 }
 
-// 5. survivors: sizes for a scan, then copy
+// 5. survivors: sizes for a scan (len[nsets] = 0, so the scan's last entry is
+// the total), then copy
 __global__ void survivor_len_kernel(const int32_t* srt, const unsigned long long* starts,
                                     int64_t nsets, const uint8_t* maximal, int64_t* len)
 {
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsets) return;
-    len[s] = maximal[s] ? (int64_t)srt[starts[s]] + 1 : 0;
+    if (s > nsets) return;
+    len[s] = s < nsets && maximal[s] ? (int64_t)srt[starts[s]] + 1 : 0;
 }
 
 __global__ void survivor_copy_kernel(const int32_t* srt, const unsigned long long* starts,
@@ -329,13 +341,16 @@ std::string FilterScratch::ensure(void** p, size_t* have, size_t need)
 
 void FilterScratch::release()
 {
-    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &sizes, &keep, &maximal, &cnt,
-                     &poff, &cursor, &post, &len, &pos, &out, &temp, &ikey, &ikey2, &ival}) {
+    if (host) cudaFreeHost(host);
+    host = nullptr;
+    host_n = 0;
+    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &sizes, &keep, &maximal, &sig,
+                     &poff, &post, &len, &pos, &temp, &ikey, &ikey2, &ival}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
-    sorted_n = hash_n = hash2_n = order_n = order2_n = sizes_n = keep_n = maximal_n = cnt_n =
-        poff_n = cursor_n = post_n = len_n = pos_n = out_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
+    sorted_n = hash_n = hash2_n = order_n = order2_n = sizes_n = keep_n = maximal_n = sig_n =
+        poff_n = post_n = len_n = pos_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -360,13 +375,14 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(sizes, sizes_n, sizeof(int32_t) * nsets);
     ENS(keep, keep_n, nsets);
     ENS(maximal, maximal_n, nsets);
+    ENS(sig, sig_n, 2 * sizeof(uint4) * nsets);
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
-    ENS(len, len_n, sizeof(int64_t) * nsets);
+    ENS(len, len_n, sizeof(int64_t) * (nsets + 1));
     ENS(pos, pos_n, sizeof(int64_t) * (nsets + 1));
     const int blocks = sms * 8;
     sort_hash_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
                                             (unsigned long long*)F.hash, (int32_t*)F.order,
-                                            (int32_t*)F.sizes);
+                                            (int32_t*)F.sizes, (uint4*)F.sig);
     // radix sort (hash, order)
     size_t tb = 0;
     FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)F.hash,
@@ -393,7 +409,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     // above every real key and sorts to the end
     const int64_t total = std::max<int64_t>(nints - nsets, 1);
     if (total > INT32_MAX) return "filter: more than 2^31 vertex incidences in the emitted sets";
-    ENS(ikey, ikey_n, sizeof(unsigned long long) * total);
+    ENS(ikey, ikey_n, std::max(sizeof(unsigned long long) * total, sizeof(int32_t) * nints));
     ENS(ikey2, ikey2_n, sizeof(unsigned long long) * total);
     ENS(ival, ival_n, sizeof(int32_t) * total);
     ENS(post, post_n, sizeof(int32_t) * total);
@@ -416,28 +432,44 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
         (unsigned long long*)F.ikey2, total, nv, (int64_t*)F.poff);
     maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
                                           (int64_t*)F.poff, (int32_t*)F.post,
-                                          (unsigned long long*)F.ikey2, (uint8_t*)F.maximal);
-    survivor_len_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
+                                          (unsigned long long*)F.ikey2, (const uint4*)F.sig,
+                                          (uint8_t*)F.maximal);
+    survivor_len_kernel<<<(unsigned)((nsets + 1 + 255) / 256), 256, 0, s>>>(
         (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.maximal, (int64_t*)F.len);
     tb = F.temp_n;
-    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos, (int)nsets, s));
-    int64_t last_pos = 0, last_len = 0;
-    FCK(cudaMemcpyAsync(&last_pos, (int64_t*)F.pos + nsets - 1, sizeof(int64_t),
-                        cudaMemcpyDeviceToHost, s));
-    FCK(cudaMemcpyAsync(&last_len, (int64_t*)F.len + nsets - 1, sizeof(int64_t),
-                        cudaMemcpyDeviceToHost, s));
-    FCK(cudaStreamSynchronize(s));
-    int64_t out_ints = last_pos + last_len;
-    ENS(out, out_n, sizeof(int32_t) * std::max<int64_t>(out_ints, 1));
+    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos,
+                                      (int)(nsets + 1), s));
+    // the survivors go to the incidence keys' first buffer, free after the
+    // sort and large enough for every emitted int (8 B per incidence)
+    int32_t* d_out = (int32_t*)F.ikey;
     survivor_copy_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets,
-                                                (uint8_t*)F.maximal, (int64_t*)F.pos,
-                                                (int32_t*)F.out);
+                                                (uint8_t*)F.maximal, (int64_t*)F.pos, d_out);
     FCK(cudaGetLastError());
     if (launches) *launches += 8;
-    std::vector<int32_t> flat((size_t)out_ints);
-    if (out_ints)
-        FCK(cudaMemcpyAsync(flat.data(), F.out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
+    if (!F.host || F.host_n < 2) {
+        if (F.host) cudaFreeHost(F.host);
+        F.host = nullptr;
+        F.host_n = 0;
+        FCK(cudaHostAlloc((void**)&F.host, 4096, cudaHostAllocDefault));
+        F.host_n = 4096 / sizeof(int32_t);
+    }
+    FCK(cudaMemcpyAsync(F.host, (int64_t*)F.pos + nsets, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     FCK(cudaStreamSynchronize(s));
+    int64_t out_ints = 0;
+    std::memcpy(&out_ints, F.host, sizeof(int64_t));
+    if (out_ints < 0 || out_ints > nints) return "filter: survivor count out of range";
+    if ((size_t)out_ints > F.host_n) {
+        const size_t want = std::max<size_t>((size_t)out_ints, 2 * F.host_n);
+        cudaFreeHost(F.host);
+        F.host = nullptr;
+        F.host_n = 0;
+        FCK(cudaHostAlloc((void**)&F.host, sizeof(int32_t) * want, cudaHostAllocDefault));
+        F.host_n = want;
+    }
+    if (out_ints) {
+        FCK(cudaMemcpyAsync(F.host, d_out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
+        FCK(cudaStreamSynchronize(s));
+    }
 #undef ENS
     // lexicographic order of the (already sorted) survivors
     // (key of the first two ids, offset): the key orders most pairs at once;
@@ -447,14 +479,15 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
         int64_t at;
     };
     std::vector<Ent> idx;
+    const int32_t* F0 = F.host;
     for (int64_t p = 0; p < out_ints;) {
-        const int32_t k = flat[(size_t)p];
-        uint64_t key = k >= 1 ? (uint64_t)(uint32_t)flat[(size_t)p + 1] << 32 : 0;
-        if (k >= 2) key |= (uint64_t)(uint32_t)flat[(size_t)p + 2] + 1u;
+        const int32_t k = F0[p];
+        if (k < 0 || p + 1 + k > out_ints) return "filter: malformed survivor record";
+        uint64_t key = k >= 1 ? (uint64_t)(uint32_t)F0[p + 1] << 32 : 0;
+        if (k >= 2) key |= (uint64_t)(uint32_t)F0[p + 2] + 1u;
         idx.push_back(Ent{key, p});
         p += 1 + k;
     }
-    const int32_t* F0 = flat.data();
     std::sort(idx.begin(), idx.end(), [&](const Ent& x, const Ent& y) {
         if (x.key != y.key) return x.key < y.key;
         const int32_t kx = F0[x.at], ky = F0[y.at];
