@@ -879,36 +879,54 @@ __device__ void schedule_child(const ExpandParams& P, Ws& ws, unsigned long long
     push_item(P, it);
 }
 
-// lane 0: while other warps wait for work, hand them all but the newest task
-// of this warp's own stack, oldest (shallowest, usually largest) first, in
-// bundles sized so each waiting warp can take one.
+// waiting warps from which a small task's children are donated between its
+// branches, not only between items
+constexpr int kEagerHungry = 4;
+
+// Whole warp: while other warps wait for work, hand them all but the newest
+// task of this warp's own stack, oldest (shallowest, usually largest) first,
+// in bundles sized so each waiting warp can take one.  Lane b pushes bundle b
+// to shard (home + b), so the pushes' round trips overlap.
 __device__ void donate(const ExpandParams& P, Ws& ws)
 {
-    int n = ws.sm->lcount;
-    if (n < 2) return;
+    const int lane = lane_id();
+    __syncwarp(); // lane 0's stack and counters written before the call
+    const int n = ws.sm->lcount;
     // read when the previous item started (the read overlapped its work)
-    int hungry = ws.sm->hungry;
-    if (hungry <= 0) return;
-    int give = n - 1;
+    const int hungry = ws.sm->hungry;
+    if (n < 2 || hungry <= 0) return;
+    const int give = n - 1;
     int per = (give + hungry - 1) / hungry;
     per = per < 1 ? 1 : (per > kBundle ? kBundle : per);
-    int given = 0;
-    const int home = home_shard();
-    for (int pushes = 0; given < give && pushes < 8; pushes++) {
-        // successive bundles go to successive shards (see push_ranges)
-        const int shard = (home + pushes) % kStackShards;
-        int k = give - given < per ? give - given : per;
+    int nb = (give + per - 1) / per;
+    nb = nb > 8 ? 8 : nb;
+    bool pushed = false;
+    if (lane < nb) {
+        const int first = lane * per;
+        const int k = give - first < per ? give - first : per;
         StackEntry e;
-        for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[given + i].rec : 0ull;
+        for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[first + i].rec : 0ull;
         e.n = k;
         e.q_lo = -1;
         e.q_hi = -1;
         e.pad = 0;
-        if (!push_entry(P, e, shard)) break;
-        given += k;
+        pushed = push_entry(P, e, (home_shard() + lane) % kStackShards);
     }
-    for (int i = given; i < n; i++) ws.sm->lstack[i - given] = ws.sm->lstack[i];
-    ws.sm->lcount = n - given;
+    const unsigned ok = __ballot_sync(QC_FULL, pushed);
+    __syncwarp();
+    if (lane == 0) {
+        // keep, in order, the tasks of bundles that were not pushed (a failed
+        // push has stopped the run) and the tasks past the last bundle
+        int keep = 0;
+        for (int i = 0; i < n; i++) {
+            const int b = i / per;
+            if (i < give && b < nb && ((ok >> b) & 1u)) continue;
+            ws.sm->lstack[keep++] = ws.sm->lstack[i];
+        }
+        ws.sm->lcount = keep;
+        ws.sm->hungry = hungry > nb ? hungry - nb : 0;
+    }
+    __syncwarp();
 }
 
 // ------------------------------------------------------------------
@@ -1215,10 +1233,6 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     if (lane == 0) {
         ws.sm->cnt.branches++;
         ws.sm->cnt.parent_vertices += (unsigned long long)(q + 1);
-        int pid = rec_ld(T.ids + q);
-        if (pid >= 0 && pid < R.n)
-            ws.sm->cnt.p_rows += (unsigned long long)((R.off[pid + 1] - R.off[pid]) +
-                                                   (R.off2[pid + 1] - R.off2[pid]));
     }
 
     Bounds b = {0, 0, 0};
@@ -1345,26 +1359,38 @@ __device__ __forceinline__ unsigned low_mask(int k) { return k >= 32 ? ~0u : ((1
 struct SmallTask {
     int t, m, cov, inst, id, l2;
     unsigned a1, a2;
+    int rows; // deg + |N2| of this lane's vertex (work accounting only)
+    int idr;  // lanes of the task with a larger id than this lane's
 };
 
-// values sorted descending across lanes; returns S = sum of this lane's value
-// and all larger-ranked ones (inclusive), so S(k) = shfl(S, k-1)
-__device__ __forceinline__ int sort_desc_prefix(int v)
+// Sum of the k largest values `in` of the lanes in `cs` (0 for k = 0, all
+// of them for k >= popc(cs)), for each lane's own k: a radix select over the
+// values' bits (values 0..63) on six ballots, with no data exchange between
+// the lanes after them.  The select keeps `gt` (lanes whose value is above
+// the k-th largest) and narrows `eq` to the lanes equal to it so far.
+__device__ __forceinline__ int top_k_sum(unsigned cs, int in, int k)
 {
-    int lane = lane_id();
-    // bitonic sort ascending on -v
-    int x = -v;
-    for (int k = 2; k <= 32; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            int y = __shfl_xor_sync(QC_FULL, x, j);
-            bool up = (lane & k) == 0;
-            bool lower = (lane & j) == 0;
-            int mn = x < y ? x : y, mx = x < y ? y : x;
-            x = (lower == up) ? mn : mx;
+    const bool c = in_set(cs, lane_id());
+    unsigned B[6];
+#pragma unroll
+    for (int b = 0; b < 6; b++) B[b] = __ballot_sync(QC_FULL, c && ((in >> b) & 1));
+    unsigned eq = cs, gt = 0;
+    int x = 0;
+#pragma unroll
+    for (int b = 5; b >= 0; b--) {
+        const unsigned hi = eq & B[b];
+        if (__popc(gt) + __popc(hi) >= k) {
+            x |= 1 << b;
+            eq = hi;
+        } else {
+            gt |= hi;
+            eq &= ~B[b];
         }
-    int val = -x; // descending values, padding lanes hold -INT_MAX.. -> guarded below
-    int s = val > 0 ? val : 0;
-    return wscan(s);
+    }
+    int sum = 0;
+#pragma unroll
+    for (int b = 0; b < 6; b++) sum += __popc(gt & B[b]) << b;
+    return sum + (k - __popc(gt)) * x;
 }
 
 // LU bounds (main.cu:1857-1972) for members set M (m of them) and the
@@ -1400,10 +1426,8 @@ __device__ bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int 
         if (ub > ncand) ub = ncand;
         if (lb < ub) {
             // S(k) for k = lane: sum of the k largest candidate indegrees
-            int incl = sort_desc_prefix(in_set(cs, lane) ? in : -1);
-            int excl = __shfl_up_sync(QC_FULL, incl, 1);
-            if (lane == 0) excl = 0;
-            int s_at_32 = __shfl_sync(QC_FULL, incl, 31);
+            // (indegrees within at most 32 members: 0..31)
+            const int excl = top_k_sum(cs, in, lane);
             // g(k) for k in [lb, ub] (ub <= 31): k == ub or sum_in + S(k) >= m*md[m+k]
             int k = lane;
             long long Sk = excl;
@@ -1411,7 +1435,8 @@ __device__ bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int 
                      (k == ub || (long long)sum_in + Sk >= (long long)m * md_at(R, m + k));
             unsigned bal = __ballot_sync(QC_FULL, g);
             int idx = bal ? __ffs(bal) - 1 : ub;
-            long long Sidx = idx < 32 ? __shfl_sync(QC_FULL, excl, idx & 31) : s_at_32;
+            // idx <= ub <= ncand < 32: a task of at most 32 vertices has a member
+            long long Sidx = __shfl_sync(QC_FULL, excl, idx & 31);
             if ((long long)sum_in + Sidx < (long long)m * md_at(R, m + idx)) {
                 lb = ub + 1;
                 invalid = true;
@@ -1457,32 +1482,61 @@ __device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, 
     return false;
 }
 
-__device__ void emit_small(const ExpandParams& P, const Rules& R, unsigned S, int id)
+// Whole warp: append the buffered sets to the result buffer under one
+// reservation of result ints and one of set indices.
+__device__ void emit_flush(const ExpandParams& P, Ws& ws)
 {
-    int lane = lane_id();
-    int k = __popc(S);
-    unsigned long long at = 0;
+    const int lane = lane_id();
+    __syncwarp();
+    const int n = ws.sm->en, ns = ws.sm->es;
+    if (n == 0) return;
+    unsigned long long at = 0, idx = 0;
     if (lane == 0) {
-        at = atomicAdd(&P.ctl->result_top, (unsigned long long)(k + 1));
-        unsigned long long idx = atomicAdd(&P.ctl->emitted, 1ull);
-        if (at + k + 1 > P.ctl->result_cap || idx >= P.ctl->set_cap) {
+        at = atomicAdd(&P.ctl->result_top, (unsigned long long)n);
+        idx = atomicAdd(&P.ctl->emitted, (unsigned long long)ns);
+        if (at + n > P.ctl->result_cap || idx + ns > P.ctl->set_cap) {
             set_status(P, ST_RESULT_OVERFLOW);
             at = ~0ull;
-        } else {
-            P.set_starts[idx] = at;
-            P.results[at] = k;
         }
     }
     at = __shfl_sync(QC_FULL, at, 0);
-    if (at == ~0ull) return;
-    if (in_set(S, lane)) P.results[at + 1 + __popc(S & low_mask(lane))] = id + R.vbase;
+    idx = __shfl_sync(QC_FULL, idx, 0);
+    if (at != ~0ull) {
+        for (int i = lane; i < n; i += 32) P.results[at + i] = ws.sm->ebuf[i];
+        for (int j = lane; j < ns; j += 32) P.set_starts[idx + j] = at + ws.sm->eset[j];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        ws.sm->en = 0;
+        ws.sm->es = 0;
+    }
+    __syncwarp();
 }
 
-__device__ __forceinline__ void clique_small(const ExpandParams& P, const Rules& R, unsigned M, int m, int in, int id)
+// Whole warp: buffer the set of lanes in S (ids `id`, at most 32 of them)
+__device__ void emit_small(const ExpandParams& P, const Rules& R, Ws& ws, unsigned S, int id)
+{
+    const int lane = lane_id();
+    const int k = __popc(S);
+    if (ws.sm->en + k + 1 > kEmitInts || ws.sm->es >= kEmitSets) emit_flush(P, ws);
+    const int base = ws.sm->en;
+    __syncwarp(); // every lane has read `en` before lane 0 moves it
+    if (in_set(S, lane)) ws.sm->ebuf[base + 1 + __popc(S & low_mask(lane))] = id + R.vbase;
+    if (lane == 0) {
+        ws.sm->ebuf[base] = k;
+        ws.sm->eset[ws.sm->es] = base;
+        ws.sm->en = base + k + 1;
+        ws.sm->es += 1;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void clique_small(const ExpandParams& P, const Rules& R, Ws& ws, unsigned M, int m, int in,
+                                             int id)
 {
     int lane = lane_id();
     int need = md_at(R, m);
-    if (!__any_sync(QC_FULL, in_set(M, lane) && in < need)) emit_small(P, R, M, id);
+    if (!__any_sync(QC_FULL, in_set(M, lane) && in < need)) emit_small(P, R, ws, M, id);
 }
 
 // child record of the vertices in M2 | R2, Q-sorted, matrices compacted
@@ -1492,28 +1546,26 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
     int lane = lane_id();
     unsigned S = M2 | R2;
     int tc = __popc(S);
-    unsigned long long hi = ~0ull, lo = ~0ull;
+    // child order (main.cu cmp of the Q sort): members first, then indegree,
+    // exdegree and two-hop count descending, then id descending.  Within a
+    // task of at most 32 vertices each count is 0..31 and T.idr ranks the ids,
+    // so the whole key and the source lane fit one 32-bit word.
+    unsigned key = ~0u;
     if (in_set(S, lane)) {
-        unsigned long long cls = in_set(M2, lane) ? 0ull : 1ull;
-        hi = (cls << 48) | ((0xffffull - (unsigned long long)in) << 32) |
-             ((0xffffull - (unsigned long long)ex) << 16) | (0xffffull - (unsigned long long)T.l2);
-        lo = ((0xffffffffull - (unsigned long long)(unsigned)T.id) << 5) | (unsigned long long)lane;
+        const unsigned cls = in_set(M2, lane) ? 0u : 1u;
+        key = (cls << 25) | ((unsigned)(31 - in) << 20) | ((unsigned)(31 - ex) << 15) |
+              ((unsigned)(31 - T.l2) << 10) | ((unsigned)T.idr << 5) | (unsigned)lane;
     }
-    // bitonic sort ascending on (hi, lo); lo carries the source lane
+    // bitonic sort ascending
     for (int k = 2; k <= 32; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
-            unsigned long long oh = __shfl_xor_sync(QC_FULL, hi, j);
-            unsigned long long ol = __shfl_xor_sync(QC_FULL, lo, j);
-            bool up = (lane & k) == 0;
-            bool lower = (lane & j) == 0;
-            bool mine_less = hi < oh || (hi == oh && lo < ol);
-            bool take_min = (lower == up);
-            if (take_min != mine_less) {
-                hi = oh;
-                lo = ol;
-            }
+            const unsigned o = __shfl_xor_sync(QC_FULL, key, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            const bool take_min = (lower == up);
+            if (take_min != (key < o)) key = o;
         }
-    int src = (int)(lo & 31ull);
+    int src = (int)(key & 31u);
     unsigned sa1 = __shfl_sync(QC_FULL, T.a1, src);
     unsigned sa2 = __shfl_sync(QC_FULL, T.a2, src);
     int sid = __shfl_sync(QC_FULL, T.id, src);
@@ -1567,10 +1619,7 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
     unsigned r2q = __shfl_sync(QC_FULL, T.a2, q);
     unsigned D = PRE & r2q;
     {
-        long long rows = 0;
-        if (lane == q && T.id >= 0 && T.id < R.n)
-            rows = (R.off[T.id + 1] - R.off[T.id]) + (R.off2[T.id + 1] - R.off2[T.id]);
-        rows = __shfl_sync(QC_FULL, rows, q);
+        const int rows = __shfl_sync(QC_FULL, T.rows, q);
         if (lane == 0) {
             ws.sm->cnt.branches++;
             ws.sm->cnt.parent_vertices += (unsigned long long)(q + 1);
@@ -1580,7 +1629,7 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
     Bounds b = {0, 0, 0};
     unsigned Rm = 0;
     if (prune_small(P, R, T.a1, M1, m1, PRE, D, Rm, in, ex, b)) {
-        if (m1 >= R.min_size) clique_small(P, R, M1, m1, in, T.id);
+        if (m1 >= R.min_size) clique_small(P, R, ws, M1, m1, in, T.id);
         return;
     }
     // critical vertices (main.cu:1526-1707)
@@ -1605,7 +1654,7 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
     Bounds b2 = {0, 0, 0};
     unsigned R2 = 0;
     bool fail2 = prune_small(P, R, T.a1, M2, m2, C2, D2, R2, in, ex, b2);
-    if (m2 >= R.min_size) clique_small(P, R, M2, m2, in, T.id);
+    if (m2 >= R.min_size) clique_small(P, R, ws, M2, m2, in, T.id);
     if (fail2) return;
     if (R2) child_small(P, R, ws, T, M2, m2, R2, in, ex);
 }
@@ -1628,6 +1677,8 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
         if (lane == 0) check_fail(P, 8, V.rec); // a vertex id outside the instance
         return;
     }
+    // issued now, first read by a branch after the lookahead has run
+    T.rows = act ? (int)((R.off[T.id + 1] - R.off[T.id]) + (R.off2[T.id + 1] - R.off2[T.id])) : 0;
     const int t = T.t, m = T.m;
     unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
     int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
@@ -1643,7 +1694,7 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
         bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
         if (!__any_sync(QC_FULL, bad)) {
             if (lane == 0) ws.sm->cnt.lookahead_hits++;
-            emit_small(P, R, low_mask(t), T.id);
+            emit_small(P, R, ws, low_mask(t), T.id);
             return;
         }
     }
@@ -1663,7 +1714,18 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     if (qlo > t - 1) return;
     // run status as read when the previous item started (no round trip here)
     if (ws.sm->stat) return;
-    for (int q = t - 1; q >= qlo; q--) branch_small(P, R, ws, T, q);
+    // rank of each id among the task's, largest first (the children's order)
+    T.idr = 0;
+    for (int j = 0; j < 32; j++) {
+        const int o = __shfl_sync(QC_FULL, T.id, j);
+        T.idr += (j < t && o > T.id) ? 1 : 0;
+    }
+    for (int q = t - 1; q >= qlo; q--) {
+        branch_small(P, R, ws, T, q);
+        // children of this task can go to waiting warps before its last branch
+        // when many warps wait (not for the odd one that will soon get work)
+        if (q > qlo && ws.sm->hungry >= kEagerHungry) donate(P, ws);
+    }
 }
 
 // ------------------------------------------------------------------
@@ -1809,14 +1871,26 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
             shared = true;
         }
     }
+    // deg + |N2| of every branch vertex (work accounting only): loads issued
+    // here, summed after the branches
+    long long rows = 0;
+    for (int q = q_lo + lane; q <= q_hi; q += 32) {
+        const int pid = rec_ld(T.ids + q);
+        if (pid >= 0 && pid < R.n)
+            rows += (R.off[pid + 1] - R.off[pid]) + (R.off2[pid + 1] - R.off2[pid]);
+    }
     for (int q = q_hi; q >= q_lo; q--) {
-        if (*(volatile int*)&P.ctl->status) return shared;
+        int stop = 0;
+        if (lane == 0) stop = *(volatile int*)&P.ctl->status;
+        if (__shfl_sync(QC_FULL, stop, 0)) break;
         if (P.deadline_ns && now_ns() > P.deadline_ns) {
             if (lane == 0) set_status(P, ST_DEADLINE);
-            return shared;
+            break;
         }
         expand_branch(P, R, T, ws, q);
     }
+    rows = wsum64(rows);
+    if (lane == 0) ws.sm->cnt.p_rows += (unsigned long long)rows;
     return shared;
 }
 
@@ -1902,6 +1976,8 @@ __global__ void expand_kernel(ExpandParams P)
         sm->hungry = 0;
         sm->stat = 0;
         sm->tab_inst = -1;
+        sm->en = 0;
+        sm->es = 0;
         sm->cnt = WarpCount{};
     }
     for (int c = lane; c < kArenaClasses; c += 32) {
@@ -1916,8 +1992,8 @@ __global__ void expand_kernel(ExpandParams P)
         int local = 0;
         if (lane == 0) local = sm->lcount > 0;
         if (__shfl_sync(QC_FULL, local, 0)) {
+            donate(P, ws);
             if (lane == 0) {
-                donate(P, ws);
                 const LocalTask lt = sm->lstack[--sm->lcount];
                 it.rec = lt.rec;
                 it.q_lo = -1;
@@ -1966,6 +2042,7 @@ __global__ void expand_kernel(ExpandParams P)
             if (sm->lcount == 0) atomicSub(&P.ctl->pending, 1);
         }
     }
+    emit_flush(P, ws);
     if (lane == 0) {
         const WarpCount& c = sm->cnt;
         if (c.tasks) atomicAdd(&P.ctl->tasks, c.tasks);

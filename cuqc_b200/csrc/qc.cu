@@ -374,8 +374,9 @@ struct Shape {
 static qc_status launch_shape(qc_context* c, int max_t, Shape& sh)
 {
     // expand_kernel is compiled with __launch_bounds__(256, 2): at most 8 warps a
-    // block.  The default is one block of 4 warps per SM.
-    sh.wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 4;
+    // block.  The default is one block of 8 warps per SM (two warps per SM
+    // sub-partition, so one hides the other's latency).
+    sh.wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 8;
     const int want_bps = c->cfg.blocks_per_sm > 0 ? c->cfg.blocks_per_sm : 1;
     const size_t sm_budget = 220u << 10; // of the 228 KB of shared memory per SM
     sh.smem_t = 0;

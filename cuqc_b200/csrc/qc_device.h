@@ -192,6 +192,11 @@ constexpr int kTabCache = 128;
 // warp itself) before it pushes further children to the shared stack.
 constexpr int kLocalStack = 48;
 
+// Sets of at most 32 vertices a warp has found, kept in shared memory and
+// appended to the result buffer together (one reservation for many sets).
+constexpr int kEmitInts = 256;
+constexpr int kEmitSets = 64;
+
 // A fresh task on a warp's own stack.  A child the warp wrote itself carries
 // its header (t > 0), so taking it needs no read of the record's header; a
 // task taken from a donated bundle has t = 0 and is read and checked.
@@ -212,6 +217,9 @@ struct WarpSmem {
     int32_t fcount[kArenaClasses];
     int32_t md[kTabCache];
     int32_t ubt[kTabCache];
+    int32_t ebuf[kEmitInts];       // buffered sets, [k, ids..] each
+    int32_t eset[kEmitSets];       // start of each buffered set in ebuf
+    int32_t en, es;                // ints and sets buffered
 };
 
 // Per-warp workspace (global memory) for the bit-matrix path, tasks of up

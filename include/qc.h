@@ -111,8 +111,8 @@ void qc_graph_free(qc_graph* g);
 
 typedef struct {
     int32_t device;              /* CUDA device ordinal                               */
-    int32_t warps_per_block;     /* 0: autotuned                                      */
-    int32_t blocks_per_sm;       /* 0: autotuned                                      */
+    int32_t warps_per_block;     /* 0: 8 (qc_tune picks the fastest for a workload)  */
+    int32_t blocks_per_sm;       /* 0: 1 (qc_tune picks the fastest for a workload)  */
     int64_t arena_bytes;         /* task-record arena; 0: default                     */
     int64_t stack_slots;         /* task stack capacity; 0: default                   */
     int64_t result_ints;         /* emitted-set buffer (ints); 0: default             */
