@@ -8,17 +8,20 @@
 //      256-bit signature;
 //   2. radix-sort (low 32 bits of the hash, set) and drop exact duplicates
 //      (equal contents within a run of equal keys; a collision keeps both);
-//   3. inverted index over the distinct sets: the (vertex, set) incidences,
-//      radix-sorted by vertex and, within a vertex, by set size descending,
-//      give every vertex its posting list with the largest sets first;
+//      each kept set writes its (vertex, set) incidences at once, to slots
+//      reserved with an atomic add (their order does not matter: 3 sorts);
+//   3. inverted index over the distinct sets: the incidences radix-sorted
+//      by vertex and, within a vertex, by set size descending, give every
+//      vertex its posting list with the largest sets first;
 //   4. one warp per distinct set S: scan the posting list of S's rarest
 //      vertex while its sets are larger than S, 128 candidates a round, and
 //      test each by its 256-bit signature (a bit per hashed id, written in
 //      step 1): a candidate whose signature lacks one of S's bits cannot
 //      contain S; the few that pass are checked exactly by the whole warp.
 //      S is maximal iff no such set contains it;
-//   5. the maximal sets are compacted and copied back; the host orders them
-//      lexicographically (the order the reference's prefix tree writes).
+//   5. each maximal set is appended to the output at a slot reserved with an
+//      atomic add; the host reads them back and orders them lexicographically
+//      (the order the reference's prefix tree writes).
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -47,7 +50,7 @@ __device__ __forceinline__ unsigned sig_bit(int32_t v) { return ((unsigned)v * 0
 // 1. per-set sort + hash + signature (one warp per set)
 __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* starts, int64_t nsets,
                                  int32_t* sorted, unsigned long long* hash, int32_t* order,
-                                 int32_t* sizes, uint4* sig)
+                                 uint4* sig)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -61,7 +64,7 @@ __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* s
         unsigned sg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int i = lane; i < k; i += 32) {
             const int32_t v = in[i];
-            out[i] = v;
+            if (k > 32) out[i] = v;
             h += mix64((unsigned long long)(unsigned)v);
             const unsigned b = sig_bit(v);
 #pragma unroll
@@ -71,65 +74,49 @@ __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* s
         for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
 #pragma unroll
         for (int w = 0; w < 8; w++) sg[w] = __reduce_or_sync(0xffffffffu, sg[w]);
-        __syncwarp();
-        // bitonic sort of out[0..k), all compare-exchanges ascending (mirror
-        // step, then half-cleaners), so virtual +inf padding at [k, N) never
-        // moves into the real range
-        int N = 1;
-        while (N < k) N <<= 1;
-        for (int sz = 2; sz <= N; sz <<= 1) {
-            for (int j = sz >> 1; j > 0; j >>= 1) {
-                for (int i = lane; i < N; i += 32) {
-                    int p = (j == (sz >> 1)) ? (i ^ (sz - 1)) : (i ^ j);
-                    if (p > i && p < k) {
-                        int x = out[i], y = out[p];
-                        if (x > y) {
-                            out[i] = y;
-                            out[p] = x;
+        if (k <= 32) {
+            // one id per lane, bitonic sort in registers (ids are >= 0, the
+            // padding lanes hold INT_MAX and sort to the end)
+            int x = lane < k ? in[lane] : INT_MAX;
+            for (int sz = 2; sz <= 32; sz <<= 1)
+                for (int j = sz >> 1; j > 0; j >>= 1) {
+                    const int o = __shfl_xor_sync(0xffffffffu, x, j);
+                    const bool up = (lane & sz) == 0;
+                    const bool lower = (lane & j) == 0;
+                    if ((lower == up) != (x < o)) x = o;
+                }
+            if (lane < k) out[lane] = x;
+        } else {
+            __syncwarp();
+            // bitonic sort of out[0..k) in place, all compare-exchanges
+            // ascending (mirror step, then half-cleaners), so virtual +inf
+            // padding at [k, N) never moves into the real range
+            int N = 1;
+            while (N < k) N <<= 1;
+            for (int sz = 2; sz <= N; sz <<= 1) {
+                for (int j = sz >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < N; i += 32) {
+                        int p = (j == (sz >> 1)) ? (i ^ (sz - 1)) : (i ^ j);
+                        if (p > i && p < k) {
+                            int x = out[i], y = out[p];
+                            if (x > y) {
+                                out[i] = y;
+                                out[p] = x;
+                            }
                         }
                     }
+                    __syncwarp();
                 }
-                __syncwarp();
             }
         }
         if (lane == 0) {
             sorted[a] = k;
             hash[s] = mix64(h ^ ((unsigned long long)k << 40));
             order[s] = (int32_t)s;
-            sizes[s] = k;
             sig[2 * s] = make_uint4(sg[0], sg[1], sg[2], sg[3]);
             sig[2 * s + 1] = make_uint4(sg[4], sg[5], sg[6], sg[7]);
         }
     }
-}
-
-__device__ bool same_set(const int32_t* srt, unsigned long long a, unsigned long long b)
-{
-    int k = srt[a];
-    if (srt[b] != k) return false;
-    for (int i = 1; i <= k; i++)
-        if (srt[a + i] != srt[b + i]) return false;
-    return true;
-}
-
-// 2. duplicates: in hash order, a set equal to an earlier one of its hash run is dropped
-__global__ void dedupe_kernel(const int32_t* srt, const unsigned long long* starts,
-                              const unsigned long long* hsorted, const int32_t* osorted,
-                              int64_t nsets, uint8_t* keep)
-{
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nsets) return;
-    // sets are sorted by the low 32 bits of their hash; equal sets have equal
-    // hashes, so an equal set sits in the same run of equal low halves
-    const unsigned h = (unsigned)hsorted[i];
-    bool dup = false;
-    for (int64_t j = i - 1; j >= 0 && (unsigned)hsorted[j] == h; j--) {
-        if (same_set(srt, starts[osorted[i]], starts[osorted[j]])) {
-            dup = true;
-            break;
-        }
-    }
-    keep[osorted[i]] = dup ? 0 : 1;
 }
 
 // incidence key: vertex in the high bits, then the set's size descending
@@ -139,31 +126,39 @@ __device__ __forceinline__ unsigned long long inc_key(int v, int k)
 }
 __device__ __forceinline__ int inc_size(unsigned long long key) { return 0xffff - (int)(key & 0xffffull); }
 
-// 3a. incidences per kept set
-__global__ void inc_len_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
-                               const uint8_t* keep, int64_t* len)
+// 2. duplicates: in hash order, a set equal to an earlier one of its hash run
+// is dropped; a kept set writes its (vertex, size) keys and set ids at slots
+// reserved with one atomic add on `inc_top` (one warp per sorted position).
+__global__ void dedupe_emit_kernel(const int32_t* srt, const unsigned long long* starts,
+                                   const unsigned long long* hsorted, const int32_t* osorted,
+                                   int64_t nsets, uint8_t* keep, unsigned long long* inc_top,
+                                   unsigned long long* key, int32_t* val)
 {
-    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nsets) return;
-    len[s] = keep[s] ? (int64_t)srt[starts[s]] : 0;
-}
-
-// 3b. (vertex, size) keys and set ids of every incidence, one warp per set
-__global__ void inc_emit_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
-                                const uint8_t* keep, const int64_t* pos,
-                                unsigned long long* key, int32_t* val)
-{
-    int lane = threadIdx.x & 31;
-    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t s = warp; s < nsets; s += nw) {
-        if (!keep[s]) continue;
-        unsigned long long a = starts[s];
-        int k = srt[a];
-        int64_t at = pos[s];
-        for (int i = lane; i < k; i += 32) {
-            key[at + i] = inc_key(srt[a + 1 + i], k);
-            val[at + i] = (int32_t)s;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < nsets; i += nw) {
+        // sets are sorted by the low 32 bits of their hash; equal sets have
+        // equal hashes, so an equal set sits in the same run of equal low halves
+        const unsigned h = (unsigned)hsorted[i];
+        const int32_t s = osorted[i];
+        const unsigned long long a = starts[s];
+        const int k = srt[a];
+        bool dup = false;
+        for (int64_t j = i - 1; j >= 0 && (unsigned)hsorted[j] == h && !dup; j--) {
+            const unsigned long long b = starts[osorted[j]];
+            bool diff = srt[b] != k;
+            for (int x = lane; x < k && !diff; x += 32) diff = srt[a + 1 + x] != srt[b + 1 + x];
+            dup = !__any_sync(0xffffffffu, diff);
+        }
+        if (lane == 0) keep[s] = dup ? 0 : 1;
+        if (dup) continue;
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(inc_top, (unsigned long long)k);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        for (int x = lane; x < k; x += 32) {
+            key[at + x] = inc_key(srt[a + 1 + x], k);
+            val[at + x] = s;
         }
     }
 }
@@ -218,16 +213,14 @@ constexpr int MAX_ROUND = 4; // candidate groups of 32 fetched per round
 // 4. superset test, one warp per kept set
 __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
                                const uint8_t* keep, const int64_t* poff, const int32_t* post,
-                               const unsigned long long* pkey, const uint4* sig, uint8_t* maximal)
+                               const unsigned long long* pkey, const uint4* sig,
+                               unsigned long long* out_top, int32_t* out)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s = warp; s < nsets; s += nw) {
-        if (!keep[s]) {
-            if (lane == 0) maximal[s] = 0;
-            continue;
-        }
+        if (!keep[s]) continue;
         unsigned long long a = starts[s];
         int k = srt[a];
         // rarest vertex of S
@@ -287,32 +280,12 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
                     break;
             }
         }
-        if (lane == 0) maximal[s] = covered ? 0 : 1;
-    }
-}
-
-// 5. survivors: sizes for a scan (len[nsets] = 0, so the scan's last entry is
-// the total), then copy
-__global__ void survivor_len_kernel(const int32_t* srt, const unsigned long long* starts,
-                                    int64_t nsets, const uint8_t* maximal, int64_t* len)
-{
-    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s > nsets) return;
-    len[s] = s < nsets && maximal[s] ? (int64_t)srt[starts[s]] + 1 : 0;
-}
-
-__global__ void survivor_copy_kernel(const int32_t* srt, const unsigned long long* starts,
-                                     int64_t nsets, const uint8_t* maximal, const int64_t* pos,
-                                     int32_t* out)
-{
-    int lane = threadIdx.x & 31;
-    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t s = warp; s < nsets; s += nw) {
-        if (!maximal[s]) continue;
-        unsigned long long a = starts[s];
-        int k = srt[a];
-        for (int i = lane; i <= k; i += 32) out[pos[s] + i] = srt[a + i];
+        if (covered) continue;
+        // a maximal set: [k, ids..] to a reserved slot of the output
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(out_top, (unsigned long long)(k + 1));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        for (int i = lane; i <= k; i += 32) out[at + i] = srt[a + i];
     }
 }
 
@@ -344,13 +317,13 @@ void FilterScratch::release()
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_n = 0;
-    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &sizes, &keep, &maximal, &sig,
-                     &poff, &post, &len, &pos, &temp, &ikey, &ikey2, &ival}) {
+    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &keep, &sig, &poff, &post, &ctr,
+                     &temp, &ikey, &ikey2, &ival}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
-    sorted_n = hash_n = hash2_n = order_n = order2_n = sizes_n = keep_n = maximal_n = sig_n =
-        poff_n = post_n = len_n = pos_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
+    sorted_n = hash_n = hash2_n = order_n = order2_n = keep_n = sig_n = poff_n = post_n = ctr_n =
+        temp_n = ikey_n = ikey2_n = ival_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -372,51 +345,42 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(hash2, hash2_n, sizeof(unsigned long long) * nsets);
     ENS(order, order_n, sizeof(int32_t) * nsets);
     ENS(order2, order2_n, sizeof(int32_t) * nsets);
-    ENS(sizes, sizes_n, sizeof(int32_t) * nsets);
     ENS(keep, keep_n, nsets);
-    ENS(maximal, maximal_n, nsets);
     ENS(sig, sig_n, 2 * sizeof(uint4) * nsets);
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
-    ENS(len, len_n, sizeof(int64_t) * (nsets + 1));
-    ENS(pos, pos_n, sizeof(int64_t) * (nsets + 1));
+    ENS(ctr, ctr_n, 2 * sizeof(unsigned long long)); // incidences, output ints
     const int blocks = sms * 8;
     sort_hash_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
                                             (unsigned long long*)F.hash, (int32_t*)F.order,
-                                            (int32_t*)F.sizes, (uint4*)F.sig);
+                                            (uint4*)F.sig);
     // radix sort (hash, order)
     size_t tb = 0;
     FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)F.hash,
                                         (unsigned long long*)F.hash2, (int32_t*)F.order,
                                         (int32_t*)F.order2, (int)nsets, 0, 32, s));
-    size_t tb3 = 0;
-    FCK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, (int64_t*)F.len, (int64_t*)F.pos,
-                                      (int)nsets, s));
-    ENS(temp, temp_n, std::max(tb, tb3) + 256);
+    ENS(temp, temp_n, tb + 256);
     tb = F.temp_n;
     FCK(cub::DeviceRadixSort::SortPairs(F.temp, tb, (unsigned long long*)F.hash,
                                         (unsigned long long*)F.hash2, (int32_t*)F.order,
                                         (int32_t*)F.order2, (int)nsets, 0, 32, s));
-    dedupe_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
-        (int32_t*)F.sorted, d_starts, (unsigned long long*)F.hash2, (int32_t*)F.order2, nsets,
-        (uint8_t*)F.keep);
-    // inverted index: incidences sorted by (vertex, size descending)
-    inc_len_kernel<<<(unsigned)((nsets + 255) / 256), 256, 0, s>>>(
-        (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep, (int64_t*)F.len);
-    tb = F.temp_n;
-    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos, (int)nsets, s));
-    // sized by a bound (every emitted set's ids), so the host need not wait
-    // for the count of the kept sets' incidences; the unused tail holds keys
-    // above every real key and sorts to the end
+    // inverted index: incidences sorted by (vertex, size descending).  Sized
+    // by a bound (every emitted set's ids), so the host need not wait for the
+    // count of the kept sets' incidences; the unused tail holds keys above
+    // every real key and sorts to the end.  The first key buffer later takes
+    // the survivors (at most every emitted int).
     const int64_t total = std::max<int64_t>(nints - nsets, 1);
     if (total > INT32_MAX) return "filter: more than 2^31 vertex incidences in the emitted sets";
     ENS(ikey, ikey_n, std::max(sizeof(unsigned long long) * total, sizeof(int32_t) * nints));
     ENS(ikey2, ikey2_n, sizeof(unsigned long long) * total);
     ENS(ival, ival_n, sizeof(int32_t) * total);
     ENS(post, post_n, sizeof(int32_t) * total);
+    unsigned long long* ctr = (unsigned long long*)F.ctr;
     FCK(cudaMemsetAsync(F.ikey, 0xff, sizeof(unsigned long long) * total, s));
-    inc_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
-                                           (int64_t*)F.pos, (unsigned long long*)F.ikey,
-                                           (int32_t*)F.ival);
+    FCK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), s));
+    dedupe_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts,
+                                              (unsigned long long*)F.hash2, (int32_t*)F.order2,
+                                              nsets, (uint8_t*)F.keep, ctr,
+                                              (unsigned long long*)F.ikey, (int32_t*)F.ival);
     int vbits = 1;
     while (vbits < 47 && ((int64_t)1 << vbits) <= nv) vbits++;
     size_t tb4 = 0;
@@ -430,22 +394,13 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
                                         (int32_t*)F.post, (int)total, 0, 16 + vbits, s));
     inc_offsets_kernel<<<(unsigned)((nv + 1 + 255) / 256), 256, 0, s>>>(
         (unsigned long long*)F.ikey2, total, nv, (int64_t*)F.poff);
+    int32_t* d_out = (int32_t*)F.ikey;
     maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
                                           (int64_t*)F.poff, (int32_t*)F.post,
                                           (unsigned long long*)F.ikey2, (const uint4*)F.sig,
-                                          (uint8_t*)F.maximal);
-    survivor_len_kernel<<<(unsigned)((nsets + 1 + 255) / 256), 256, 0, s>>>(
-        (int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.maximal, (int64_t*)F.len);
-    tb = F.temp_n;
-    FCK(cub::DeviceScan::ExclusiveSum(F.temp, tb, (int64_t*)F.len, (int64_t*)F.pos,
-                                      (int)(nsets + 1), s));
-    // the survivors go to the incidence keys' first buffer, free after the
-    // sort and large enough for every emitted int (8 B per incidence)
-    int32_t* d_out = (int32_t*)F.ikey;
-    survivor_copy_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets,
-                                                (uint8_t*)F.maximal, (int64_t*)F.pos, d_out);
+                                          ctr + 1, d_out);
     FCK(cudaGetLastError());
-    if (launches) *launches += 8;
+    if (launches) *launches += 4;
     if (!F.host || F.host_n < 2) {
         if (F.host) cudaFreeHost(F.host);
         F.host = nullptr;
@@ -453,7 +408,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
         FCK(cudaHostAlloc((void**)&F.host, 4096, cudaHostAllocDefault));
         F.host_n = 4096 / sizeof(int32_t);
     }
-    FCK(cudaMemcpyAsync(F.host, (int64_t*)F.pos + nsets, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    FCK(cudaMemcpyAsync(F.host, ctr + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     FCK(cudaStreamSynchronize(s));
     int64_t out_ints = 0;
     std::memcpy(&out_ints, F.host, sizeof(int64_t));
