@@ -20,10 +20,12 @@
 //      contain S; the few that pass are checked exactly by the whole warp.
 //      S is maximal iff no such set contains it;
 //   5. each maximal set is appended to the output at a slot reserved with an
-//      atomic add; the host reads them back and orders them lexicographically
-//      (the order the reference's prefix tree writes).
+//      atomic add, with an entry (key of its first two ids, offset); a merge
+//      sort of the entries with a lexicographic comparison gives the order the
+//      reference's prefix tree writes, and the host gathers the sets in it.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
+#include <cub/device/device_merge_sort.cuh>
 
 #include <algorithm>
 #include <cstring>
@@ -211,10 +213,45 @@ __device__ __forceinline__ bool warp_subset(const int32_t* srt, unsigned long lo
 constexpr int MAX_ROUND = 4; // candidate groups of 32 fetched per round
 
 // 4. superset test, one warp per kept set
+// a surviving set: key of its first two ids (see set_key) and its offset in
+// the output
+struct SetEnt {
+    unsigned long long key;
+    long long at;
+};
+
+// ids (sorted ascending) of a set at p: the first id in the high half, the
+// second + 1 in the low half (0 for a set of one id), so that comparing keys
+// compares the first two ids lexicographically
+__device__ __forceinline__ unsigned long long set_key(const int32_t* d, long long p)
+{
+    const int k = d[p];
+    unsigned long long key = k >= 1 ? (unsigned long long)(unsigned)d[p + 1] << 32 : 0ull;
+    if (k >= 2) key |= (unsigned long long)((unsigned)d[p + 2] + 1u);
+    return key;
+}
+
+// lexicographic order of two sets of the output (ids sorted ascending; a
+// prefix orders first)
+struct SetLess {
+    const int32_t* d;
+    __device__ bool operator()(const SetEnt& x, const SetEnt& y) const
+    {
+        if (x.key != y.key) return x.key < y.key;
+        const int kx = d[x.at], ky = d[y.at];
+        const int n = kx < ky ? kx : ky;
+        for (int i = 2; i < n; i++) {
+            const int a = d[x.at + 1 + i], b = d[y.at + 1 + i];
+            if (a != b) return a < b;
+        }
+        return kx < ky;
+    }
+};
+
 __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
                                const uint8_t* keep, const int64_t* poff, const int32_t* post,
                                const unsigned long long* pkey, const uint4* sig,
-                               unsigned long long* out_top, int32_t* out)
+                               unsigned long long* ctr, int32_t* out, SetEnt* ents)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -281,9 +318,14 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
             }
         }
         if (covered) continue;
-        // a maximal set: [k, ids..] to a reserved slot of the output
+        // a maximal set: [k, ids..] to a reserved slot of the output, and
+        // its entry for the ordering
         unsigned long long at = 0;
-        if (lane == 0) at = atomicAdd(out_top, (unsigned long long)(k + 1));
+        if (lane == 0) {
+            at = atomicAdd(&ctr[1], (unsigned long long)(k + 1));
+            const unsigned long long j = atomicAdd(&ctr[2], 1ull);
+            ents[j] = SetEnt{set_key(srt, (long long)a), (long long)at};
+        }
         at = __shfl_sync(0xffffffffu, at, 0);
         for (int i = lane; i <= k; i += 32) out[at + i] = srt[a + i];
     }
@@ -317,13 +359,13 @@ void FilterScratch::release()
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_n = 0;
-    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &keep, &sig, &poff, &post, &ctr,
+    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &keep, &sig, &poff, &post, &ctr, &ents,
                      &temp, &ikey, &ikey2, &ival}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
     sorted_n = hash_n = hash2_n = order_n = order2_n = keep_n = sig_n = poff_n = post_n = ctr_n =
-        temp_n = ikey_n = ikey2_n = ival_n = 0;
+        ents_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -348,7 +390,8 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(keep, keep_n, nsets);
     ENS(sig, sig_n, 2 * sizeof(uint4) * nsets);
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
-    ENS(ctr, ctr_n, 2 * sizeof(unsigned long long)); // incidences, output ints
+    ENS(ctr, ctr_n, 3 * sizeof(unsigned long long)); // incidences, output ints, output sets
+    ENS(ents, ents_n, sizeof(SetEnt) * nsets);
     const int blocks = sms * 8;
     sort_hash_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
                                             (unsigned long long*)F.hash, (int32_t*)F.order,
@@ -376,7 +419,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(post, post_n, sizeof(int32_t) * total);
     unsigned long long* ctr = (unsigned long long*)F.ctr;
     FCK(cudaMemsetAsync(F.ikey, 0xff, sizeof(unsigned long long) * total, s));
-    FCK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), s));
+    FCK(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), s));
     dedupe_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts,
                                               (unsigned long long*)F.hash2, (int32_t*)F.order2,
                                               nsets, (uint8_t*)F.keep, ctr,
@@ -398,66 +441,65 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
                                           (int64_t*)F.poff, (int32_t*)F.post,
                                           (unsigned long long*)F.ikey2, (const uint4*)F.sig,
-                                          ctr + 1, d_out);
+                                          ctr, d_out, (SetEnt*)F.ents);
     FCK(cudaGetLastError());
     if (launches) *launches += 4;
-    if (!F.host || F.host_n < 2) {
+    if (!F.host || F.host_n < 4) {
         if (F.host) cudaFreeHost(F.host);
         F.host = nullptr;
         F.host_n = 0;
         FCK(cudaHostAlloc((void**)&F.host, 4096, cudaHostAllocDefault));
         F.host_n = 4096 / sizeof(int32_t);
     }
-    FCK(cudaMemcpyAsync(F.host, ctr + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    FCK(cudaMemcpyAsync(F.host, ctr + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     FCK(cudaStreamSynchronize(s));
-    int64_t out_ints = 0;
+    int64_t out_ints = 0, out_sets = 0;
     std::memcpy(&out_ints, F.host, sizeof(int64_t));
-    if (out_ints < 0 || out_ints > nints) return "filter: survivor count out of range";
-    if ((size_t)out_ints > F.host_n) {
-        const size_t want = std::max<size_t>((size_t)out_ints, 2 * F.host_n);
+    std::memcpy(&out_sets, (char*)F.host + sizeof(int64_t), sizeof(int64_t));
+    if (out_ints < 0 || out_ints > nints || out_sets < 0 || out_sets > nsets)
+        return "filter: survivor count out of range";
+    // lexicographic order of the survivors on the device
+    if (out_sets > 1) {
+        size_t tbm = 0;
+        FCK(cub::DeviceMergeSort::SortKeys(nullptr, tbm, (SetEnt*)F.ents, (int64_t)out_sets,
+                                           SetLess{d_out}, s));
+        ENS(temp, temp_n, tbm + 256);
+        tbm = F.temp_n;
+        FCK(cub::DeviceMergeSort::SortKeys(F.temp, tbm, (SetEnt*)F.ents, (int64_t)out_sets,
+                                           SetLess{d_out}, s));
+    }
+    // read back: the sets as appended, then their entries in order
+    const size_t want_ints = (size_t)out_ints + 4 + 4 * (size_t)out_sets; // SetEnt = 4 ints
+    if (want_ints > F.host_n) {
+        const size_t want = std::max<size_t>(want_ints, 2 * F.host_n);
         cudaFreeHost(F.host);
         F.host = nullptr;
         F.host_n = 0;
         FCK(cudaHostAlloc((void**)&F.host, sizeof(int32_t) * want, cudaHostAllocDefault));
         F.host_n = want;
     }
+    const SetEnt* he = (const SetEnt*)(F.host + (size_t)out_ints + ((size_t)out_ints & 3u ? 4 - ((size_t)out_ints & 3u) : 0));
     if (out_ints) {
         FCK(cudaMemcpyAsync(F.host, d_out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
+        FCK(cudaMemcpyAsync((void*)he, F.ents, sizeof(SetEnt) * out_sets, cudaMemcpyDeviceToHost, s));
         FCK(cudaStreamSynchronize(s));
     }
 #undef ENS
-    // lexicographic order of the (already sorted) survivors
-    // (key of the first two ids, offset): the key orders most pairs at once;
-    // equal keys fall back to comparing the remaining ids
-    struct Ent {
-        uint64_t key;
-        int64_t at;
-    };
-    std::vector<Ent> idx;
     const int32_t* F0 = F.host;
-    for (int64_t p = 0; p < out_ints;) {
-        const int32_t k = F0[p];
-        if (k < 0 || p + 1 + k > out_ints) return "filter: malformed survivor record";
-        uint64_t key = k >= 1 ? (uint64_t)(uint32_t)F0[p + 1] << 32 : 0;
-        if (k >= 2) key |= (uint64_t)(uint32_t)F0[p + 2] + 1u;
-        idx.push_back(Ent{key, p});
-        p += 1 + k;
-    }
-    std::sort(idx.begin(), idx.end(), [&](const Ent& x, const Ent& y) {
-        if (x.key != y.key) return x.key < y.key;
-        const int32_t kx = F0[x.at], ky = F0[y.at];
-        if (kx < 2 || ky < 2) return kx < ky;
-        return std::lexicographical_compare(F0 + x.at + 3, F0 + x.at + 1 + kx, F0 + y.at + 3,
-                                            F0 + y.at + 1 + ky);
-    });
     host_out.resize((size_t)out_ints);
     int32_t* o = host_out.data();
-    for (const Ent& e : idx) {
-        const int32_t k = F0[e.at];
-        std::memcpy(o, F0 + e.at, sizeof(int32_t) * (size_t)(k + 1));
+    int64_t done = 0;
+    for (int64_t j = 0; j < out_sets; j++) {
+        const long long at = he[j].at;
+        const int32_t k = at >= 0 && at < out_ints ? F0[at] : -1;
+        if (k < 0 || at + 1 + k > out_ints || done + 1 + k > out_ints)
+            return "filter: malformed survivor record";
+        std::memcpy(o, F0 + at, sizeof(int32_t) * (size_t)(k + 1));
         o += k + 1;
+        done += k + 1;
     }
-    host_nsets = (int64_t)idx.size();
+    if (done != out_ints) return "filter: survivor records do not cover the output";
+    host_nsets = out_sets;
     return "";
 }
 
