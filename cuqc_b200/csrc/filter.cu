@@ -220,6 +220,115 @@ struct SetEnt {
     long long at;
 };
 
+// The maximal sets form an antichain: no set is a subset, so none is a
+// prefix, of another.  For such sets with ids sorted ascending, the
+// lexicographic order is the descending order of the bit vectors that set bit
+// 255 - r for every id of rank r in the survivors' universe (the smallest id
+// is the most significant bit): at the first position where two sets differ,
+// the smaller id is in one set only and every smaller id is in both or
+// neither.  With at most 256 distinct ids, four words order every pair.
+constexpr int kBitUniverse = 256;
+struct BitEnt {
+    unsigned long long w[4]; // w[0] most significant
+    long long at;
+};
+struct BitMore {
+    __device__ bool operator()(const BitEnt& x, const BitEnt& y) const
+    {
+        for (int i = 0; i < 4; i++)
+            if (x.w[i] != y.w[i]) return x.w[i] > y.w[i];
+        return false;
+    }
+};
+
+// survivors' ids into a presence bitmap over the vertex range (one warp per
+// survivor; the count of survivors is read on the device)
+__global__ void uni_mark_kernel(const int32_t* out, const SetEnt* ents, const unsigned long long* ctr,
+                                uint32_t* bitmap)
+{
+    const int lane = threadIdx.x & 31;
+    const long long nsurv = (long long)ctr[2];
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long j = warp; j < nsurv; j += nw) {
+        const long long at = ents[j].at;
+        const int k = out[at];
+        for (int i = lane; i < k; i += 32) {
+            const int v = out[at + 1 + i];
+            atomicOr(&bitmap[v >> 5], 1u << (v & 31));
+        }
+    }
+}
+
+// one block: rank_base[w] = ids present in bitmap words before w; ctr[3] =
+// the universe size
+__global__ void __launch_bounds__(1024) uni_rank_kernel(const uint32_t* bitmap, int nwords,
+                                                        uint32_t* rank_base, unsigned long long* ctr)
+{
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nwords; base += blockDim.x) {
+        const int w = base + threadIdx.x;
+        const uint32_t c = w < nwords ? (uint32_t)__popc(bitmap[w]) : 0u;
+        uint32_t x = c; // inclusive scan within the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0u;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t; // inclusive over warps
+        }
+        __syncthreads();
+        const uint32_t before = (wid ? warp_tot[wid - 1] : 0u) + x - c;
+        if (w < nwords) rank_base[w] = carry + before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_tot[(blockDim.x >> 5) - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) ctr[3] = carry;
+}
+
+// bit-vector key of every survivor (universe of at most kBitUniverse ids)
+__global__ void bit_key_kernel(const int32_t* out, const SetEnt* ents, long long nsurv,
+                               const uint32_t* bitmap, const uint32_t* rank_base, BitEnt* bents)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long j = warp; j < nsurv; j += nw) {
+        const long long at = ents[j].at;
+        const int k = out[at];
+        unsigned h[8] = {0, 0, 0, 0, 0, 0, 0, 0}; // 32-bit halves, h[0] most significant
+        for (int i = lane; i < k; i += 32) {
+            const int v = out[at + 1 + i];
+            const unsigned r = rank_base[v >> 5] + (unsigned)__popc(bitmap[v >> 5] & ((1u << (v & 31)) - 1u));
+            const unsigned p = 255u - (r < 256u ? r : 255u); // bit position, 255 = most significant
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if ((int)(p >> 5) == 7 - q) h[q] |= 1u << (p & 31);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) h[q] = __reduce_or_sync(0xffffffffu, h[q]);
+        if (lane == 0) {
+            BitEnt e;
+            for (int i = 0; i < 4; i++)
+                e.w[i] = ((unsigned long long)h[2 * i] << 32) | (unsigned long long)h[2 * i + 1];
+            e.at = at;
+            bents[j] = e;
+        }
+    }
+}
+
 // ids (sorted ascending) of a set at p: the first id in the high half, the
 // second + 1 in the low half (0 for a set of one id), so that comparing keys
 // compares the first two ids lexicographically
@@ -359,13 +468,13 @@ void FilterScratch::release()
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_n = 0;
-    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &keep, &sig, &poff, &post, &ctr, &ents,
+    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &keep, &sig, &poff, &post, &ctr, &ents, &bents,
                      &temp, &ikey, &ikey2, &ival}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
     sorted_n = hash_n = hash2_n = order_n = order2_n = keep_n = sig_n = poff_n = post_n = ctr_n =
-        ents_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
+        ents_n = bents_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -390,7 +499,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(keep, keep_n, nsets);
     ENS(sig, sig_n, 2 * sizeof(uint4) * nsets);
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
-    ENS(ctr, ctr_n, 3 * sizeof(unsigned long long)); // incidences, output ints, output sets
+    ENS(ctr, ctr_n, 4 * sizeof(unsigned long long)); // incidences, output ints and sets, universe
     ENS(ents, ents_n, sizeof(SetEnt) * nsets);
     const int blocks = sms * 8;
     sort_hash_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
@@ -419,7 +528,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(post, post_n, sizeof(int32_t) * total);
     unsigned long long* ctr = (unsigned long long*)F.ctr;
     FCK(cudaMemsetAsync(F.ikey, 0xff, sizeof(unsigned long long) * total, s));
-    FCK(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), s));
+    FCK(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), s));
     dedupe_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts,
                                               (unsigned long long*)F.hash2, (int32_t*)F.order2,
                                               nsets, (uint8_t*)F.keep, ctr,
@@ -442,8 +551,16 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
                                           (int64_t*)F.poff, (int32_t*)F.post,
                                           (unsigned long long*)F.ikey2, (const uint4*)F.sig,
                                           ctr, d_out, (SetEnt*)F.ents);
+    // the survivors' universe: presence bitmap and ranks over the vertex range
+    // (in the posting-list offsets' buffer, no longer read)
+    const int nwords = (int)((nv + 31) / 32);
+    uint32_t* bitmap = (uint32_t*)F.poff;
+    uint32_t* rank_base = bitmap + nwords;
+    FCK(cudaMemsetAsync(bitmap, 0, sizeof(uint32_t) * nwords, s));
+    uni_mark_kernel<<<blocks, 256, 0, s>>>(d_out, (const SetEnt*)F.ents, ctr, bitmap);
+    uni_rank_kernel<<<1, 1024, 0, s>>>(bitmap, nwords, rank_base, ctr);
     FCK(cudaGetLastError());
-    if (launches) *launches += 4;
+    if (launches) *launches += 6;
     if (!F.host || F.host_n < 4) {
         if (F.host) cudaFreeHost(F.host);
         F.host = nullptr;
@@ -451,15 +568,30 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
         FCK(cudaHostAlloc((void**)&F.host, 4096, cudaHostAllocDefault));
         F.host_n = 4096 / sizeof(int32_t);
     }
-    FCK(cudaMemcpyAsync(F.host, ctr + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    FCK(cudaMemcpyAsync(F.host, ctr + 1, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     FCK(cudaStreamSynchronize(s));
-    int64_t out_ints = 0, out_sets = 0;
+    int64_t out_ints = 0, out_sets = 0, universe = 0;
     std::memcpy(&out_ints, F.host, sizeof(int64_t));
     std::memcpy(&out_sets, (char*)F.host + sizeof(int64_t), sizeof(int64_t));
+    std::memcpy(&universe, (char*)F.host + 2 * sizeof(int64_t), sizeof(int64_t));
     if (out_ints < 0 || out_ints > nints || out_sets < 0 || out_sets > nsets)
         return "filter: survivor count out of range";
-    // lexicographic order of the survivors on the device
-    if (out_sets > 1) {
+    // lexicographic order of the survivors on the device: by bit vectors when
+    // the universe is small, else by comparing the sets
+    const bool bits = universe <= kBitUniverse && out_sets > 1;
+    if (bits) {
+        ENS(bents, bents_n, sizeof(BitEnt) * out_sets);
+        bit_key_kernel<<<blocks, 256, 0, s>>>(d_out, (const SetEnt*)F.ents, (long long)out_sets,
+                                              bitmap, rank_base, (BitEnt*)F.bents);
+        size_t tbm = 0;
+        FCK(cub::DeviceMergeSort::SortKeys(nullptr, tbm, (BitEnt*)F.bents, (int64_t)out_sets,
+                                           BitMore{}, s));
+        ENS(temp, temp_n, tbm + 256);
+        tbm = F.temp_n;
+        FCK(cub::DeviceMergeSort::SortKeys(F.temp, tbm, (BitEnt*)F.bents, (int64_t)out_sets,
+                                           BitMore{}, s));
+        if (launches) *launches += 1;
+    } else if (out_sets > 1) {
         size_t tbm = 0;
         FCK(cub::DeviceMergeSort::SortKeys(nullptr, tbm, (SetEnt*)F.ents, (int64_t)out_sets,
                                            SetLess{d_out}, s));
@@ -469,7 +601,8 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
                                            SetLess{d_out}, s));
     }
     // read back: the sets as appended, then their entries in order
-    const size_t want_ints = (size_t)out_ints + 4 + 4 * (size_t)out_sets; // SetEnt = 4 ints
+    const size_t ent_ints = (bits ? sizeof(BitEnt) : sizeof(SetEnt)) / sizeof(int32_t);
+    const size_t want_ints = (size_t)out_ints + 4 + ent_ints * (size_t)out_sets;
     if (want_ints > F.host_n) {
         const size_t want = std::max<size_t>(want_ints, 2 * F.host_n);
         cudaFreeHost(F.host);
@@ -481,7 +614,10 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     const SetEnt* he = (const SetEnt*)(F.host + (size_t)out_ints + ((size_t)out_ints & 3u ? 4 - ((size_t)out_ints & 3u) : 0));
     if (out_ints) {
         FCK(cudaMemcpyAsync(F.host, d_out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
-        FCK(cudaMemcpyAsync((void*)he, F.ents, sizeof(SetEnt) * out_sets, cudaMemcpyDeviceToHost, s));
+        if (bits)
+            FCK(cudaMemcpyAsync((void*)he, F.bents, sizeof(BitEnt) * out_sets, cudaMemcpyDeviceToHost, s));
+        else
+            FCK(cudaMemcpyAsync((void*)he, F.ents, sizeof(SetEnt) * out_sets, cudaMemcpyDeviceToHost, s));
         FCK(cudaStreamSynchronize(s));
     }
 #undef ENS
@@ -490,7 +626,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     int32_t* o = host_out.data();
     int64_t done = 0;
     for (int64_t j = 0; j < out_sets; j++) {
-        const long long at = he[j].at;
+        const long long at = bits ? ((const BitEnt*)he)[j].at : he[j].at;
         const int32_t k = at >= 0 && at < out_ints ? F0[at] : -1;
         if (k < 0 || at + 1 + k > out_ints || done + 1 + k > out_ints)
             return "filter: malformed survivor record";
