@@ -121,22 +121,42 @@ std::string write_serialized(const HostGraph& g, const char* path)
     return "";
 }
 
+// Rows of ids: every row strictly ascending (sorted, no duplicates) with its
+// ids in [0, n), checked with branch-free passes the compiler vectorises (a
+// row's ids are in range when its first and last are); the exact message is
+// looked up only for a failing row.
+static std::string check_rows(const int64_t* off, const int32_t* adj, int32_t n, bool no_self,
+                              const char* what)
+{
+    for (int32_t v = 0; v < n; v++) {
+        const int64_t a = off[v], b = off[(size_t)v + 1];
+        if (b < a) return std::string(what) + " offsets decrease";
+        if (a == b) continue;
+        const int32_t* r = adj + a;
+        const int64_t len = b - a;
+        int bad = r[0] < 0 || r[len - 1] >= n;
+        for (int64_t i = 1; i < len; i++) bad |= r[i - 1] >= r[i];
+        if (no_self)
+            for (int64_t i = 0; i < len; i++) bad |= r[i] == v;
+        if (!bad) continue;
+        for (int64_t i = 0; i < len; i++) {
+            if (r[i] < 0 || r[i] >= n) return std::string(what) + " neighbour id out of range";
+            if (no_self && r[i] == v) return std::string("self loop in ") + what + " list";
+            if (i > 0 && r[i - 1] >= r[i])
+                return std::string(what) + " rows must be sorted ascending without duplicates";
+        }
+    }
+    return "";
+}
+
 std::string validate(const HostGraph& g, bool need_twohop)
 {
     const int32_t n = g.n;
     if ((int64_t)g.off.size() != (int64_t)n + 1) return "1-hop offsets must have n+1 entries";
     if (g.off[0] != 0 || g.off[(size_t)n] != (int64_t)g.adj.size())
         return "1-hop offsets must start at 0 and end at 2|E|";
-    for (int32_t v = 0; v < n; v++) {
-        if (g.off[(size_t)v + 1] < g.off[(size_t)v]) return "1-hop offsets decrease";
-        for (int64_t e = g.off[(size_t)v]; e < g.off[(size_t)v + 1]; e++) {
-            int32_t w = g.adj[(size_t)e];
-            if (w < 0 || w >= n) return "1-hop neighbour id out of range";
-            if (w == v) return "self loop in 1-hop list";
-            if (e > g.off[(size_t)v] && g.adj[(size_t)e - 1] >= w)
-                return "1-hop rows must be sorted ascending without duplicates";
-        }
-    }
+    std::string e = check_rows(g.off.data(), g.adj.data(), n, true, "1-hop");
+    if (!e.empty()) return e;
     // symmetry: w in N(v) <=> v in N(w).  Visiting v in ascending order, the
     // entries v of the sorted rows N(w) come up in order too, so one cursor
     // per row checks every edge once; every row must be used up at the end.
@@ -159,16 +179,7 @@ std::string validate(const HostGraph& g, bool need_twohop)
     if ((int64_t)g.off2.size() != (int64_t)n + 1) return "2-hop offsets must have n+1 entries";
     if (g.off2[0] != 0 || g.off2[(size_t)n] != (int64_t)g.adj2.size())
         return "2-hop offsets must start at 0 and end at the 2-hop count";
-    for (int32_t v = 0; v < n; v++) {
-        if (g.off2[(size_t)v + 1] < g.off2[(size_t)v]) return "2-hop offsets decrease";
-        for (int64_t e = g.off2[(size_t)v]; e < g.off2[(size_t)v + 1]; e++) {
-            int32_t w = g.adj2[(size_t)e];
-            if (w < 0 || w >= n) return "2-hop neighbour id out of range";
-            if (e > g.off2[(size_t)v] && g.adj2[(size_t)e - 1] >= w)
-                return "2-hop rows must be sorted ascending without duplicates";
-        }
-    }
-    return "";
+    return check_rows(g.off2.data(), g.adj2.data(), n, false, "2-hop");
 }
 
 // ------------------------------------------------------------------
