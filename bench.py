@@ -378,7 +378,7 @@ def run_serving(args):
     rates_out = []
     # every slot mines the distinct query graphs once before the timed rates
     warm = [(g, float(gm), ms) for g, gm, ms in pool + big]
-    srv = Server(slots=args.serve_slots, warm=warm)
+    srv = Server(slots=args.serve_slots, warm=warm, warps_per_block=args.serve_warps)
     try:
         for rate in args.serve_rates:
             reqs = [Request(graph=g, gamma=float(gm), min_size=ms, rid=i)
@@ -396,6 +396,7 @@ def run_serving(args):
         "steps": len(args.serve_rates), "warmup": 8, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": "cfg5", "requests_per_rate": n_req, "slots": args.serve_slots,
+                   "warps_per_block": args.serve_warps,
                    "mix": "90% batched-workload instances (first 64 of the manifest), 10% "
                           "config-1-sized graphs"},
         "rates": rates_out,
@@ -558,6 +559,7 @@ def main():
                     help="skip the batched-vs-plain comparison in the default run")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-warps", type=int, default=8, help="warps per block of each slot")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10, 30, 100, 300, 1000])
     args = ap.parse_args()
     if args.impl == "reference":

@@ -58,7 +58,8 @@ def estimate_bytes(g, gamma, min_size):
 
 
 class Server:
-    def __init__(self, slots=2, device=0, budget_fraction=0.8, max_batch=64, sms=148, warm=None):
+    def __init__(self, slots=2, device=0, budget_fraction=0.8, max_batch=64, sms=148, warm=None,
+                 warps_per_block=8):
         self.lock = threading.Condition()
         self.dev_graphs = {}  # id(graph) -> (graph, DeviceGraph)
         self.queue = deque()
@@ -69,7 +70,7 @@ class Server:
         self.budget = int(free * budget_fraction)
         self.max_batch = max_batch
         share = max(1, sms // slots)
-        self.ctxs = [Context(device=device, warps_per_block=4, max_blocks=share)
+        self.ctxs = [Context(device=device, warps_per_block=warps_per_block, max_blocks=share)
                      for _ in range(slots)]
         if warm:
             for c in self.ctxs:
