@@ -37,7 +37,7 @@ EXPORTS = [
     "qc_graph_twohop_offsets", "qc_graph_twohop_neighbors", "qc_graph_free", "qc_config_default",
     "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
-    "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune",
+    "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune", "qc_maximal_sets",
 ]
 
 
@@ -124,6 +124,7 @@ def lib():
         L.qc_tune.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.POINTER(Config)]
         L.qc_twohop_noalloc.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int64, P64, vp]
         L.qc_twohop_noalloc_max_vertices.restype = C.c_int32
+        L.qc_maximal_sets.argtypes = [vp, P32, C.c_int64, C.c_int32, C.POINTER(vp)]
         _lib = L
     return _lib
 
@@ -294,6 +295,14 @@ class Context:
         _check(L.qc_mine_batch(self.h, ga, gm.ctypes.data_as(C.POINTER(C.c_double)), _p32(ms), k,
                                outs))
         return [self._result(C.c_void_p(o)) for o in outs]
+
+    def maximal_sets(self, flat, n_vertices):
+        """The maximal sets of a family given flat as [k, ids..] per set
+        (qc_maximal_sets); returns a Result."""
+        f = np.ascontiguousarray(flat, np.int32)
+        r = C.c_void_p()
+        _check(lib().qc_maximal_sets(self.h, _p32(f), len(f), int(n_vertices), C.byref(r)))
+        return self._result(r)
 
     def close(self):
         if self.h:

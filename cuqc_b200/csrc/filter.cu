@@ -3,22 +3,21 @@
 //
 // Input: the emitted sets in the device result buffer, [k, id_1..id_k] each,
 // and the start offset of every set (written by the expansion kernel).
-//   1. one warp per set: sort its ids ascending into the sorted buffer, hash
-//      the set (sum of per-id 64-bit mixes, plus its size) and build its
-//      256-bit signature;
-//   2. radix-sort (low 32 bits of the hash, set) and drop exact duplicates
-//      (equal contents within a run of equal keys; a collision keeps both);
-//      each kept set writes its (vertex, set) incidences at once, to slots
+//   1. one warp per set: sort its ids ascending into the sorted buffer and
+//      build its 256-bit signature;
+//   2. each set writes its (vertex, set) incidences at once, to slots
 //      reserved with an atomic add (their order does not matter: 3 sorts);
-//   3. inverted index over the distinct sets: the incidences radix-sorted
-//      by vertex and, within a vertex, by set size descending, give every
-//      vertex its posting list with the largest sets first;
+//   3. inverted index: the incidences radix-sorted by vertex and, within a
+//      vertex, by set size descending, give every vertex its posting list
+//      with the largest sets first;
 //   4. one warp per distinct set S: scan the posting list of S's rarest
 //      vertex while its sets are larger than S, 128 candidates a round, and
 //      test each by its 256-bit signature (a bit per hashed id, written in
 //      step 1): a candidate whose signature lacks one of S's bits cannot
 //      contain S; the few that pass are checked exactly by the whole warp.
-//      S is maximal iff no such set contains it;
+//      S is maximal iff no such set contains it.  Exact copies of a maximal
+//      set follow the larger sets in the same list: the copy of the smallest
+//      index is kept (copies that a larger set contains need no check);
 //   5. each maximal set is appended to the output at a slot reserved with an
 //      atomic add, with an entry (key of its first two ids, offset); a merge
 //      sort of the entries with a lexicographic comparison gives the order the
@@ -38,21 +37,12 @@ namespace qcb {
 
 namespace {
 
-__device__ __forceinline__ unsigned long long mix64(unsigned long long x)
-{
-    x += 0x9e3779b97f4a7c15ull;
-    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
-    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
-    return x ^ (x >> 31);
-}
-
 // signature bit of an id: the top 8 bits of a multiplicative (Fibonacci) hash
 __device__ __forceinline__ unsigned sig_bit(int32_t v) { return ((unsigned)v * 0x9E3779B1u) >> 24; }
 
-// 1. per-set sort + hash + signature (one warp per set)
-__global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* starts, int64_t nsets,
-                                 int32_t* sorted, unsigned long long* hash, int32_t* order,
-                                 uint4* sig)
+// 1. per-set sort + signature (one warp per set)
+__global__ void sort_sig_kernel(const int32_t* res, const unsigned long long* starts, int64_t nsets,
+                                int32_t* sorted, uint4* sig)
 {
     int lane = threadIdx.x & 31;
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -62,18 +52,15 @@ __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* s
         int k = res[a];
         const int32_t* in = res + a + 1;
         int32_t* out = sorted + a + 1;
-        unsigned long long h = 0;
         unsigned sg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int i = lane; i < k; i += 32) {
             const int32_t v = in[i];
             if (k > 32) out[i] = v;
-            h += mix64((unsigned long long)(unsigned)v);
             const unsigned b = sig_bit(v);
 #pragma unroll
             for (int w = 0; w < 8; w++)
                 if ((int)(b >> 5) == w) sg[w] |= 1u << (b & 31);
         }
-        for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
 #pragma unroll
         for (int w = 0; w < 8; w++) sg[w] = __reduce_or_sync(0xffffffffu, sg[w]);
         if (k <= 32) {
@@ -113,8 +100,6 @@ __global__ void sort_hash_kernel(const int32_t* res, const unsigned long long* s
         }
         if (lane == 0) {
             sorted[a] = k;
-            hash[s] = mix64(h ^ ((unsigned long long)k << 40));
-            order[s] = (int32_t)s;
             sig[2 * s] = make_uint4(sg[0], sg[1], sg[2], sg[3]);
             sig[2 * s + 1] = make_uint4(sg[4], sg[5], sg[6], sg[7]);
         }
@@ -128,39 +113,25 @@ __device__ __forceinline__ unsigned long long inc_key(int v, int k)
 }
 __device__ __forceinline__ int inc_size(unsigned long long key) { return 0xffff - (int)(key & 0xffffull); }
 
-// 2. duplicates: in hash order, a set equal to an earlier one of its hash run
-// is dropped; a kept set writes its (vertex, size) keys and set ids at slots
-// reserved with one atomic add on `inc_top` (one warp per sorted position).
-__global__ void dedupe_emit_kernel(const int32_t* srt, const unsigned long long* starts,
-                                   const unsigned long long* hsorted, const int32_t* osorted,
-                                   int64_t nsets, uint8_t* keep, unsigned long long* inc_top,
-                                   unsigned long long* key, int32_t* val)
+// 2. every set writes its (vertex, size) keys and set id at slots reserved
+// with one atomic add on `inc_top` (one warp per set; the order does not
+// matter, the keys are sorted next)
+__global__ void emit_incidences_kernel(const int32_t* srt, const unsigned long long* starts,
+                                       int64_t nsets, unsigned long long* inc_top,
+                                       unsigned long long* key, int32_t* val)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < nsets; i += nw) {
-        // sets are sorted by the low 32 bits of their hash; equal sets have
-        // equal hashes, so an equal set sits in the same run of equal low halves
-        const unsigned h = (unsigned)hsorted[i];
-        const int32_t s = osorted[i];
+    for (int64_t s = warp; s < nsets; s += nw) {
         const unsigned long long a = starts[s];
         const int k = srt[a];
-        bool dup = false;
-        for (int64_t j = i - 1; j >= 0 && (unsigned)hsorted[j] == h && !dup; j--) {
-            const unsigned long long b = starts[osorted[j]];
-            bool diff = srt[b] != k;
-            for (int x = lane; x < k && !diff; x += 32) diff = srt[a + 1 + x] != srt[b + 1 + x];
-            dup = !__any_sync(0xffffffffu, diff);
-        }
-        if (lane == 0) keep[s] = dup ? 0 : 1;
-        if (dup) continue;
         unsigned long long at = 0;
         if (lane == 0) at = atomicAdd(inc_top, (unsigned long long)k);
         at = __shfl_sync(0xffffffffu, at, 0);
         for (int x = lane; x < k; x += 32) {
             key[at + x] = inc_key(srt[a + 1 + x], k);
-            val[at + x] = s;
+            val[at + x] = (int32_t)s;
         }
     }
 }
@@ -358,7 +329,7 @@ struct SetLess {
 };
 
 __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
-                               const uint8_t* keep, const int64_t* poff, const int32_t* post,
+                               const int64_t* poff, const int32_t* post,
                                const unsigned long long* pkey, const uint4* sig,
                                unsigned long long* ctr, int32_t* out, SetEnt* ents)
 {
@@ -366,7 +337,6 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
     int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s = warp; s < nsets; s += nw) {
-        if (!keep[s]) continue;
         unsigned long long a = starts[s];
         int k = srt[a];
         // rarest vertex of S
@@ -392,6 +362,7 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
         if (k > 0 && best_v >= 0) {
             const uint4 s0 = sig[2 * s], s1 = sig[2 * s + 1];
             const int64_t lo = poff[best_v], hi = poff[best_v + 1];
+            int64_t eq = hi; // first entry not larger than S
             // the list is ordered by size, largest first: past the sets larger
             // than S nothing can contain it
             for (int64_t base = lo; base < hi; base += 32 * MAX_ROUND) {
@@ -422,8 +393,39 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
                         covered = warp_subset(srt, a, k, starts[tt], lane);
                     }
                 }
-                if (covered || __ballot_sync(0xffffffffu, larger[MAX_ROUND - 1]) != 0xffffffffu)
-                    break;
+                if (covered) break;
+                bool end = false;
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    const unsigned lb = __ballot_sync(0xffffffffu, larger[u]); // a prefix of lanes
+                    if (!end && lb != 0xffffffffu) {
+                        eq = base + u * 32 + __popc(lb);
+                        end = true;
+                    }
+                }
+                if (end) break;
+            }
+            // Exact copies of S (same size, after the larger sets in the
+            // list): the copy of the smallest index stands for all of them.
+            // Only sets no larger set contains get here.
+            for (int64_t base = eq < hi ? eq : hi; !covered && base < hi; base += 32) {
+                const int64_t e = base + lane;
+                const bool same = e < hi && inc_size(pkey[e]) == k;
+                const int32_t tt = same ? post[e] : 0;
+                bool pass = false;
+                if (same && tt < s) {
+                    const uint4 t0 = sig[2 * (int64_t)tt], t1 = sig[2 * (int64_t)tt + 1];
+                    pass = s0.x == t0.x && s0.y == t0.y && s0.z == t0.z && s0.w == t0.w &&
+                           s1.x == t1.x && s1.y == t1.y && s1.z == t1.z && s1.w == t1.w;
+                }
+                unsigned pb = __ballot_sync(0xffffffffu, pass);
+                while (pb && !covered) {
+                    const int c = __ffs(pb) - 1;
+                    pb &= pb - 1;
+                    const int32_t t2 = __shfl_sync(0xffffffffu, tt, c);
+                    covered = warp_subset(srt, a, k, starts[t2], lane); // equal sizes: equal sets
+                }
+                if (__ballot_sync(0xffffffffu, same) != 0xffffffffu) break;
             }
         }
         if (covered) continue;
@@ -468,12 +470,12 @@ void FilterScratch::release()
     if (host) cudaFreeHost(host);
     host = nullptr;
     host_n = 0;
-    for (auto* pp : {&sorted, &hash, &hash2, &order, &order2, &keep, &sig, &poff, &post, &ctr, &ents, &bents,
+    for (auto* pp : {&sorted, &sig, &poff, &post, &ctr, &ents, &bents,
                      &temp, &ikey, &ikey2, &ival}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
-    sorted_n = hash_n = hash2_n = order_n = order2_n = keep_n = sig_n = poff_n = post_n = ctr_n =
+    sorted_n = sig_n = poff_n = post_n = ctr_n =
         ents_n = bents_n = temp_n = ikey_n = ikey2_n = ival_n = 0;
 }
 
@@ -492,34 +494,16 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     e = F.ensure((void**)&F.ptr, &F.ptr##_n, (size_t)(bytes));          \
     if (!e.empty()) return e;
     ENS(sorted, sorted_n, sizeof(int32_t) * nints);
-    ENS(hash, hash_n, sizeof(unsigned long long) * nsets);
-    ENS(hash2, hash2_n, sizeof(unsigned long long) * nsets);
-    ENS(order, order_n, sizeof(int32_t) * nsets);
-    ENS(order2, order2_n, sizeof(int32_t) * nsets);
-    ENS(keep, keep_n, nsets);
     ENS(sig, sig_n, 2 * sizeof(uint4) * nsets);
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
     ENS(ctr, ctr_n, 4 * sizeof(unsigned long long)); // incidences, output ints and sets, universe
     ENS(ents, ents_n, sizeof(SetEnt) * nsets);
     const int blocks = sms * 8;
-    sort_hash_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
-                                            (unsigned long long*)F.hash, (int32_t*)F.order,
-                                            (uint4*)F.sig);
-    // radix sort (hash, order)
-    size_t tb = 0;
-    FCK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)F.hash,
-                                        (unsigned long long*)F.hash2, (int32_t*)F.order,
-                                        (int32_t*)F.order2, (int)nsets, 0, 32, s));
-    ENS(temp, temp_n, tb + 256);
-    tb = F.temp_n;
-    FCK(cub::DeviceRadixSort::SortPairs(F.temp, tb, (unsigned long long*)F.hash,
-                                        (unsigned long long*)F.hash2, (int32_t*)F.order,
-                                        (int32_t*)F.order2, (int)nsets, 0, 32, s));
-    // inverted index: incidences sorted by (vertex, size descending).  Sized
-    // by a bound (every emitted set's ids), so the host need not wait for the
-    // count of the kept sets' incidences; the unused tail holds keys above
-    // every real key and sorts to the end.  The first key buffer later takes
-    // the survivors (at most every emitted int).
+    sort_sig_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
+                                           (uint4*)F.sig);
+    // inverted index: incidences sorted by (vertex, size descending), one
+    // per id of every emitted set.  The first key buffer later takes the
+    // survivors (at most every emitted int).
     const int64_t total = std::max<int64_t>(nints - nsets, 1);
     if (total > INT32_MAX) return "filter: more than 2^31 vertex incidences in the emitted sets";
     ENS(ikey, ikey_n, std::max(sizeof(unsigned long long) * total, sizeof(int32_t) * nints));
@@ -527,12 +511,9 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(ival, ival_n, sizeof(int32_t) * total);
     ENS(post, post_n, sizeof(int32_t) * total);
     unsigned long long* ctr = (unsigned long long*)F.ctr;
-    FCK(cudaMemsetAsync(F.ikey, 0xff, sizeof(unsigned long long) * total, s));
     FCK(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), s));
-    dedupe_emit_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts,
-                                              (unsigned long long*)F.hash2, (int32_t*)F.order2,
-                                              nsets, (uint8_t*)F.keep, ctr,
-                                              (unsigned long long*)F.ikey, (int32_t*)F.ival);
+    emit_incidences_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, ctr,
+                                                  (unsigned long long*)F.ikey, (int32_t*)F.ival);
     int vbits = 1;
     while (vbits < 47 && ((int64_t)1 << vbits) <= nv) vbits++;
     size_t tb4 = 0;
@@ -547,8 +528,7 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     inc_offsets_kernel<<<(unsigned)((nv + 1 + 255) / 256), 256, 0, s>>>(
         (unsigned long long*)F.ikey2, total, nv, (int64_t*)F.poff);
     int32_t* d_out = (int32_t*)F.ikey;
-    maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (uint8_t*)F.keep,
-                                          (int64_t*)F.poff, (int32_t*)F.post,
+    maximal_kernel<<<blocks, 256, 0, s>>>((int32_t*)F.sorted, d_starts, nsets, (int64_t*)F.poff, (int32_t*)F.post,
                                           (unsigned long long*)F.ikey2, (const uint4*)F.sig,
                                           ctr, d_out, (SetEnt*)F.ents);
     // the survivors' universe: presence bitmap and ranks over the vertex range

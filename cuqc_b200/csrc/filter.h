@@ -10,10 +10,9 @@ namespace qcb {
 
 // Device scratch owned by a context, grown on demand.
 struct FilterScratch {
-    void *sorted = nullptr, *hash = nullptr, *hash2 = nullptr, *order = nullptr, *order2 = nullptr,
-         *keep = nullptr, *sig = nullptr, *poff = nullptr, *post = nullptr, *ctr = nullptr, *ents = nullptr, *bents = nullptr,
+    void *sorted = nullptr, *sig = nullptr, *poff = nullptr, *post = nullptr, *ctr = nullptr, *ents = nullptr, *bents = nullptr,
          *temp = nullptr, *ikey = nullptr, *ikey2 = nullptr, *ival = nullptr;
-    size_t sorted_n = 0, hash_n = 0, hash2_n = 0, order_n = 0, order2_n = 0, keep_n = 0, sig_n = 0,
+    size_t sorted_n = 0, sig_n = 0,
            poff_n = 0, post_n = 0, ctr_n = 0, ents_n = 0, bents_n = 0, temp_n = 0, ikey_n = 0, ikey2_n = 0, ival_n = 0;
     // page-locked host buffer the survivors are read back into (grown on demand)
     int32_t* host = nullptr;

@@ -711,6 +711,55 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     return QC_OK;
 }
 
+extern "C" qc_status qc_maximal_sets(qc_context* c, const int32_t* flat, int64_t n_ints,
+                                     int32_t n_vertices, qc_result** out)
+{
+    if (!c || !out || n_ints < 0 || (n_ints > 0 && !flat) || n_vertices < 0)
+        return fail(QC_ERR_ARGS, "bad arguments");
+    *out = nullptr;
+    // set starts, with the checks the device filter relies on
+    std::vector<unsigned long long> starts;
+    std::vector<uint8_t> seen((size_t)n_vertices, 0);
+    for (int64_t p = 0; p < n_ints;) {
+        const int32_t k = flat[p];
+        if (k < 1 || p + 1 + k > n_ints) return fail(QC_ERR_FORMAT, "malformed set record");
+        for (int32_t i = 0; i < k; i++) {
+            const int32_t v = flat[p + 1 + i];
+            if (v < 0 || v >= n_vertices) return fail(QC_ERR_FORMAT, "vertex id out of range");
+            if (seen[(size_t)v]) return fail(QC_ERR_FORMAT, "repeated id within a set");
+            seen[(size_t)v] = 1;
+        }
+        for (int32_t i = 0; i < k; i++) seen[(size_t)flat[p + 1 + i]] = 0;
+        starts.push_back((unsigned long long)p);
+        p += 1 + k;
+    }
+    CK(cudaSetDevice(c->cfg.device));
+    std::unique_ptr<qc_result> r(new qc_result());
+    auto t0 = clk::now();
+    const int64_t nsets = (int64_t)starts.size();
+    if (nsets > 0) {
+        cudaStream_t s = c->stream;
+        CK(c->results.ensure(sizeof(int32_t) * (size_t)n_ints));
+        CK(c->starts.ensure(sizeof(unsigned long long) * (size_t)nsets));
+        CK(cudaMemcpyAsync(c->results.p, flat, sizeof(int32_t) * (size_t)n_ints,
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(c->starts.p, starts.data(), sizeof(unsigned long long) * (size_t)nsets,
+                           cudaMemcpyHostToDevice, s));
+        std::string fe = filter_maximal(c->filt, c->results.as<int32_t>(), n_ints,
+                                        c->starts.as<unsigned long long>(), nsets,
+                                        std::max<int32_t>(n_vertices, 1), s, c->sms, r->sets,
+                                        r->nsets, &c->launches);
+        if (!fe.empty()) return fail(QC_ERR_CUDA, fe);
+    }
+    r->st.emitted = nsets;
+    r->st.emitted_ints = n_ints;
+    r->st.maximal = r->nsets;
+    r->st.filter_ms = ms_since(t0);
+    r->st.total_ms = r->st.filter_ms;
+    *out = r.release();
+    return QC_OK;
+}
+
 extern "C" qc_status qc_context_upload(qc_context* c, const qc_graph* g)
 {
     if (!c || !g) return fail(QC_ERR_ARGS, "NULL argument");

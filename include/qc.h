@@ -198,6 +198,16 @@ qc_status qc_tune(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_
 qc_status qc_mine_batch(qc_context* ctx, const qc_graph* const* graphs, const double* gammas,
                         const int32_t* min_sizes, int32_t count, qc_result** outs);
 
+/* The maximal sets of a family of vertex sets, on the device: the
+ * non-maximal removal step alone (RemoveNonMax, main.cu:4571-4960), e.g. to
+ * merge the results of instances mined separately over parts of one graph.
+ * `flat` holds n_sets sets as [k, id_1 .. id_k] (k >= 1, ids in
+ * [0, n_vertices), any order; a set may repeat, a repeated id within a set
+ * is an error).  The result lists each maximal set once, in the order of
+ * qc_result_sets. */
+qc_status qc_maximal_sets(qc_context* ctx, const int32_t* flat, int64_t n_ints,
+                          int32_t n_vertices, qc_result** out);
+
 /* Result access.  Sets are sorted ascending and listed in lexicographic
  * order of their id sequences, as the reference's result file. */
 int64_t qc_result_count(const qc_result* r);
