@@ -91,6 +91,32 @@ def test_malformed_graphs_are_rejected(mutate, msg):
     assert e.value.status == 3 and msg in str(e.value)
 
 
+@pytest.mark.parametrize("mutate,msg", [
+    ("unsorted", "2-hop rows must be sorted"), ("duplicate", "2-hop rows must be sorted"),
+    ("range", "2-hop neighbour id out of range"), ("negative", "2-hop neighbour id out of range"),
+    ("offsets", "2-hop offsets"),
+])
+def test_malformed_twohop_lists_are_rejected(mutate, msg):
+    g = graphs.random_small(24, 0.3, 5)
+    off2, adj2 = g.off2.copy(), g.adj2.copy()
+    v = int(np.argmax(np.diff(off2) > 2))
+    a = int(off2[v])
+    if mutate == "unsorted":
+        adj2[a], adj2[a + 1] = adj2[a + 1], adj2[a]
+    elif mutate == "duplicate":
+        adj2[a + 1] = adj2[a]
+    elif mutate == "range":
+        adj2[int(off2[v + 1]) - 1] = g.n  # last of a row: one past the ids
+    elif mutate == "negative":
+        adj2[a] = -1
+    elif mutate == "offsets":
+        off2[v + 1] = off2[v] - 1
+    bad = graphs.Graph(n=g.n, off=g.off, adj=g.adj, off2=off2, adj2=adj2)
+    with pytest.raises(Q.QCError) as e:
+        Q.DeviceGraph.from_graph(bad)
+    assert e.value.status == 3 and msg in str(e.value)
+
+
 def test_truncated_file_is_a_format_error():
     g = graphs.random_small(20, 0.3, 4)
     d = tempfile.mkdtemp()
