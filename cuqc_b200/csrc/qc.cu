@@ -148,7 +148,7 @@ struct qc_context {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    DevBuf pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts, rules;
+    DevBuf pos, ids, md, ubt, ctl, arena, stack, slot, results, ws, starts, rules, lvl0;
     FilterScratch filt;
     int32_t pos_n = 0;
     // graphs kept on the device, by graph serial; least recently used ones are
@@ -206,7 +206,7 @@ extern "C" void qc_context_free(qc_context* c)
     }
     for (auto& kv : c->res) kv.second->release();
     c->res.clear();
-    for (DevBuf* b : {&c->pos, &c->ids, &c->md, &c->ubt, &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts,
+    for (DevBuf* b : {&c->pos, &c->ids, &c->md, &c->ubt, &c->ctl, &c->arena, &c->stack, &c->slot, &c->results, &c->ws, &c->starts, &c->lvl0,
                       &c->rules})
         b->release();
     c->filt.release();
@@ -311,6 +311,120 @@ __global__ void root_rows_kernel(const int64_t* off, const int32_t* adj, const i
             int p = pos[adj2[e]];
             if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
         }
+    }
+}
+
+// Level 0 on the device for graphs of at most kLevel0DeviceMax vertices
+// (initialize_tasks, main.cu:846-998; the host form is build_root in
+// host.cpp): one block keeps the vertices with deg >= need and
+// |N2| >= min_size-1, peels to the subgraph where every vertex keeps >= need
+// neighbours (the k-core of the kept vertices is unique, so removing the
+// vertices in rounds instead of the reference's order keeps the same ones),
+// marks the cover vertex (largest exdeg, smallest id on ties) and its
+// surviving neighbours, and writes the survivors in Q order: covered,
+// candidates, cover, then exdeg, 2-hop size and id, all descending.
+// info = {root size, covered count}.
+constexpr int kLevel0DeviceMax = 65536;
+__global__ void __launch_bounds__(1024) level0_kernel(const int64_t* off, const int32_t* adj,
+                                                      const int64_t* off2, int n, int need,
+                                                      int min_size, int32_t* exdeg, int32_t* label,
+                                                      int32_t* l2, unsigned long long* keys,
+                                                      int32_t* ids, int32_t* info)
+{
+    __shared__ int changed, cnt, ncov;
+    __shared__ unsigned long long best;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int v = tid; v < n; v += nt) {
+        const int d = (int)(off[v + 1] - off[v]);
+        const int d2 = (int)(off2[v + 1] - off2[v]);
+        l2[v] = d2;
+        label[v] = (d >= need && d2 >= min_size - 1) ? 0 : -1;
+    }
+    __syncthreads();
+    for (int v = tid; v < n; v += nt) {
+        if (label[v] != 0) continue;
+        int c = 0;
+        for (int64_t e = off[v]; e < off[v + 1]; e++) c += label[adj[e]] == 0;
+        exdeg[v] = c;
+    }
+    __syncthreads();
+    for (;;) {
+        if (tid == 0) changed = 0;
+        __syncthreads();
+        for (int v = tid; v < n; v += nt)
+            if (label[v] == 0 && exdeg[v] < need) {
+                label[v] = -2;
+                changed = 1;
+            }
+        __syncthreads();
+        if (!changed) break;
+        for (int v = tid; v < n; v += nt)
+            if (label[v] == -2)
+                for (int64_t e = off[v]; e < off[v + 1]; e++) {
+                    const int w = adj[e];
+                    if (label[w] == 0) atomicSub(&exdeg[w], 1);
+                }
+        __syncthreads();
+        for (int v = tid; v < n; v += nt)
+            if (label[v] == -2) label[v] = -1;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        best = 0;
+        cnt = 0;
+        ncov = 0;
+    }
+    __syncthreads();
+    for (int v = tid; v < n; v += nt)
+        if (label[v] == 0 && exdeg[v] > 0)
+            atomicMax(&best, ((unsigned long long)(unsigned)exdeg[v] << 32) |
+                                 (unsigned long long)(0xffffffffu - (unsigned)v));
+    __syncthreads();
+    if (best) {
+        const int bv = (int)(0xffffffffu - (unsigned)(best & 0xffffffffull));
+        for (int64_t e = off[bv] + tid; e < off[bv + 1]; e += nt) {
+            const int w = adj[e];
+            if (label[w] == 0) label[w] = 2;
+        }
+        __syncthreads();
+        if (tid == 0) label[bv] = 3;
+    }
+    __syncthreads();
+    for (int v = tid; v < n; v += nt) {
+        const int lb = label[v];
+        if (lb < 0) continue;
+        const unsigned long long rank = lb == 2 ? 0ull : (lb == 0 ? 1ull : 2ull);
+        const unsigned long long key = (rank << 51) |
+                                       ((unsigned long long)(0x1ffff - exdeg[v]) << 34) |
+                                       ((unsigned long long)(0x1ffff - l2[v]) << 17) |
+                                       (unsigned long long)(0x1ffff - v);
+        keys[atomicAdd(&cnt, 1)] = key;
+        if (lb == 2) atomicAdd(&ncov, 1);
+    }
+    __syncthreads();
+    const int t = cnt;
+    int N = 1;
+    while (N < t) N <<= 1;
+    for (int i = t + tid; i < N; i += nt) keys[i] = ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < N; i += nt) {
+                const int p = i ^ j;
+                if (p > i) {
+                    const unsigned long long x = keys[i], y = keys[p];
+                    if ((x > y) == ((i & k) == 0)) {
+                        keys[i] = y;
+                        keys[p] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = tid; i < t; i += nt) ids[i] = 0x1ffff - (int)(keys[i] & 0x1ffffull);
+    if (tid == 0) {
+        info[0] = t;
+        info[1] = ncov;
     }
 }
 
@@ -503,19 +617,47 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     std::vector<int32_t> md, ubt;
     gamma_tables(gamma, h.n, min_size, md, ubt);
     std::vector<int32_t> ids;
-    int cov = 0;
-    build_root(h, md.data(), min_size, ids, cov);
-    r->st.root_size = (int64_t)ids.size();
-    if (ids.empty()) {
+    int cov = 0, t = 0;
+    const bool l0_dev = h.n > 0 && h.n <= kLevel0DeviceMax;
+    if (l0_dev) {
+        // root ids straight into c->ids; only the root size and the covered
+        // count come back
+        int P = 1;
+        while (P < h.n) P <<= 1;
+        // int32 arrays of n (exdeg, label, 2-hop size), then the 64-bit sort
+        // keys, then two ints of results: every array starts 16-byte aligned
+        const size_t nb = ((size_t)h.n * 4 + 15) & ~(size_t)15;
+        CK(c->lvl0.ensure(3 * nb + 8 * (size_t)P + 64));
+        CK(c->ids.ensure(std::max<size_t>((size_t)h.n * 4, 16)));
+        char* z = c->lvl0.as<char>();
+        int32_t* info = (int32_t*)(z + 3 * nb + 8 * (size_t)P);
+        level0_kernel<<<1, 1024, 0, s>>>(rg->off.as<int64_t>(), rg->adj.as<int32_t>(),
+                                         rg->off2.as<int64_t>(), h.n, md[(size_t)min_size],
+                                         min_size, (int32_t*)z, (int32_t*)(z + nb),
+                                         (int32_t*)(z + 2 * nb), (unsigned long long*)(z + 3 * nb),
+                                         c->ids.as<int32_t>(), info);
+        CK(cudaGetLastError());
+        c->launches += 1;
+        int32_t hinfo[2] = {0, 0};
+        CK(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        t = hinfo[0];
+        cov = hinfo[1];
+        if (t < 0 || t > h.n || cov < 0 || cov > t) return fail(QC_ERR_CUDA, "level 0 size out of range");
+    } else {
+        build_root(h, md.data(), min_size, ids, cov);
+        t = (int)ids.size();
+    }
+    r->st.root_size = (int64_t)t;
+    if (t == 0) {
         r->st.enum_ms = ms_since(t_enum);
         r->st.total_ms = ms_since(t_all);
         return QC_OK;
     }
-    const int t = (int)ids.size();
     const int W = words_for(t);
     CK(upload(c->md, md, s));
     CK(upload(c->ubt, ubt, s));
-    CK(upload(c->ids, ids, s));
+    if (!l0_dev) CK(upload(c->ids, ids, s));
 
     Shape sh;
     {
@@ -559,8 +701,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         hd.cls = root_cls;
         hd.inst = 0;
         CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(rec + rec_ids_off(), ids.data(), sizeof(int32_t) * t,
-                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(rec + rec_ids_off(), c->ids.p, sizeof(int32_t) * t,
+                           cudaMemcpyDeviceToDevice, s));
         root_pos_kernel<<<(t + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), t,
                                                         c->pos.as<int32_t>(), 1);
         root_rows_kernel<<<std::min(blocks * 4, (t + 7) / 8), 256, 0, s>>>(

@@ -54,6 +54,31 @@ def test_random_graphs(ctx, seed):
     res = ctx.mine(g, gamma, ms)
     assert canon(res.emitted) == canon(want_flat)
     assert res.sets == oracle.maximal(want_flat)
+    # level 0 (on the device up to 65,536 vertices) gives the oracle's root
+    assert res.stats["root_size"] == len(oracle.root(g, gamma, ms)[0])
+    assert res.stats["tasks"] == st["tasks"] and res.stats["branches"] == st["branches"]
+
+
+def test_level0_on_the_host_above_the_device_limit(ctx):
+    # 70,000 vertices: level 0 runs on the host (the device form takes graphs
+    # of at most 65,536); sparse background, two planted groups survive
+    rng = np.random.default_rng(21)
+    n = 70000
+    src, dst = rng.integers(0, n, 3 * n), rng.integers(0, n, 3 * n)  # mean degree ~6
+    groups = [rng.choice(n, 15, replace=False) for _ in range(2)]
+    for grp in groups:
+        iu, ju = np.triu_indices(15, 1)
+        keep = rng.random(len(iu)) < 0.95
+        src = np.concatenate([src, grp[iu[keep]]])
+        dst = np.concatenate([dst, grp[ju[keep]]])
+    ok = src != dst
+    dg = Q.DeviceGraph.from_graph(graphs.from_edges(n, src[ok], dst[ok], with_twohop=False))
+    g = dg.to_graph()  # with the two-hop lists built on the device
+    want_flat, st = oracle.mine(g, 0.95, 12, "clean")
+    res = ctx.mine(dg, 0.95, 12)
+    assert res.stats["root_size"] == len(oracle.root(g, 0.95, 12)[0])
+    assert res.stats["tasks"] == st["tasks"] and res.stats["branches"] == st["branches"]
+    assert res.sets == oracle.maximal(want_flat)
 
 
 def test_small_arena_grows_and_stays_exact():
