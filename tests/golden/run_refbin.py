@@ -3,7 +3,7 @@
 The binary is oracle/_ref/cuQC_ref, compiled from the reference's main.cu for
 sm_100a by oracle/Makefile (built where the reference sources exist and
 shipped prebuilt).  For each case it writes, under OUT (default
-gpurun_out/refbin):
+refbin_out/ at the repository root):
   <name>.refbin.result  the binary's result file
   <name>.refbin.temp    its temp.txt (every emitted set, maximal or not)
   <name>.refbin.log     its stdout (LOADING / ENUMERATION / ... lines)
@@ -31,7 +31,7 @@ BIN = os.path.join(ROOT, "oracle", "_ref", "cuQC_ref")
 
 
 def main():
-    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "refbin")
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "refbin_out")
     os.makedirs(out, exist_ok=True)
     summary = {}
     for case in golden_cases():
