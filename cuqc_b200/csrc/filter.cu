@@ -408,24 +408,39 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
             // Exact copies of S (same size, after the larger sets in the
             // list): the copy of the smallest index stands for all of them.
             // Only sets no larger set contains get here.
-            for (int64_t base = eq < hi ? eq : hi; !covered && base < hi; base += 32) {
-                const int64_t e = base + lane;
-                const bool same = e < hi && inc_size(pkey[e]) == k;
-                const int32_t tt = same ? post[e] : 0;
-                bool pass = false;
-                if (same && tt < s) {
-                    const uint4 t0 = sig[2 * (int64_t)tt], t1 = sig[2 * (int64_t)tt + 1];
-                    pass = s0.x == t0.x && s0.y == t0.y && s0.z == t0.z && s0.w == t0.w &&
-                           s1.x == t1.x && s1.y == t1.y && s1.z == t1.z && s1.w == t1.w;
+            for (int64_t base = eq < hi ? eq : hi; !covered && base < hi;
+                 base += 32 * MAX_ROUND) {
+                bool same[MAX_ROUND];
+                int32_t tt[MAX_ROUND];
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    const int64_t e = base + u * 32 + lane;
+                    same[u] = e < hi && inc_size(pkey[e]) == k;
+                    tt[u] = same[u] ? post[e] : 0;
                 }
-                unsigned pb = __ballot_sync(0xffffffffu, pass);
-                while (pb && !covered) {
-                    const int c = __ffs(pb) - 1;
-                    pb &= pb - 1;
-                    const int32_t t2 = __shfl_sync(0xffffffffu, tt, c);
-                    covered = warp_subset(srt, a, k, starts[t2], lane); // equal sizes: equal sets
+                bool pass[MAX_ROUND];
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    pass[u] = false;
+                    if (same[u] && tt[u] < s) {
+                        const uint4 t0 = sig[2 * (int64_t)tt[u]], t1 = sig[2 * (int64_t)tt[u] + 1];
+                        pass[u] = s0.x == t0.x && s0.y == t0.y && s0.z == t0.z && s0.w == t0.w &&
+                                  s1.x == t1.x && s1.y == t1.y && s1.z == t1.z && s1.w == t1.w;
+                    }
                 }
-                if (__ballot_sync(0xffffffffu, same) != 0xffffffffu) break;
+#pragma unroll
+                for (int u = 0; u < MAX_ROUND; u++) {
+                    unsigned pb = __ballot_sync(0xffffffffu, pass[u]);
+                    while (pb && !covered) {
+                        const int c = __ffs(pb) - 1;
+                        pb &= pb - 1;
+                        const int32_t t2 = __shfl_sync(0xffffffffu, tt[u], c);
+                        covered = warp_subset(srt, a, k, starts[t2], lane); // equal sizes: equal sets
+                    }
+                }
+                // sizes only fall along the list: a round that is not all of
+                // S's size reached the end of the copies
+                if (__ballot_sync(0xffffffffu, same[MAX_ROUND - 1]) != 0xffffffffu) break;
             }
         }
         if (covered) continue;
