@@ -10,7 +10,7 @@
 //   3. inverted index: the incidences radix-sorted by vertex and, within a
 //      vertex, by set size descending, give every vertex its posting list
 //      with the largest sets first;
-//   4. one warp per distinct set S: scan the posting list of S's rarest
+//   4. one warp per set S: scan the posting list of S's rarest
 //      vertex while its sets are larger than S, 128 candidates a round, and
 //      test each by its 256-bit signature (a bit per hashed id, written in
 //      step 1): a candidate whose signature lacks one of S's bits cannot
@@ -19,9 +19,11 @@
 //      set follow the larger sets in the same list: the copy of the smallest
 //      index is kept (copies that a larger set contains need no check);
 //   5. each maximal set is appended to the output at a slot reserved with an
-//      atomic add, with an entry (key of its first two ids, offset); a merge
-//      sort of the entries with a lexicographic comparison gives the order the
-//      reference's prefix tree writes, and the host gathers the sets in it.
+//      atomic add, with an entry (key of its first two ids, offset).  The
+//      entries are put in the order the reference's prefix tree writes
+//      (lexicographic): by 256-bit vectors over the survivors' ranked ids when
+//      there are at most 256 distinct ids, else by a merge sort comparing the
+//      sets; the host gathers the sets in that order.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 #include <cub/device/device_merge_sort.cuh>
