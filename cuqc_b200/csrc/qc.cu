@@ -25,6 +25,7 @@
 
 #include "../../include/qc.h"
 #include "expand_kernel.cuh"
+#include "level0_kernel.cuh"
 #include "filter.h"
 #include "host.h"
 
@@ -311,120 +312,6 @@ __global__ void root_rows_kernel(const int64_t* off, const int32_t* adj, const i
             int p = pos[adj2[e]];
             if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
         }
-    }
-}
-
-// Level 0 on the device for graphs of at most kLevel0DeviceMax vertices
-// (initialize_tasks, main.cu:846-998; the host form is build_root in
-// host.cpp): one block keeps the vertices with deg >= need and
-// |N2| >= min_size-1, peels to the subgraph where every vertex keeps >= need
-// neighbours (the k-core of the kept vertices is unique, so removing the
-// vertices in rounds instead of the reference's order keeps the same ones),
-// marks the cover vertex (largest exdeg, smallest id on ties) and its
-// surviving neighbours, and writes the survivors in Q order: covered,
-// candidates, cover, then exdeg, 2-hop size and id, all descending.
-// info = {root size, covered count}.
-constexpr int kLevel0DeviceMax = 65536;
-__global__ void __launch_bounds__(1024) level0_kernel(const int64_t* off, const int32_t* adj,
-                                                      const int64_t* off2, int n, int need,
-                                                      int min_size, int32_t* exdeg, int32_t* label,
-                                                      int32_t* l2, unsigned long long* keys,
-                                                      int32_t* ids, int32_t* info)
-{
-    __shared__ int changed, cnt, ncov;
-    __shared__ unsigned long long best;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int v = tid; v < n; v += nt) {
-        const int d = (int)(off[v + 1] - off[v]);
-        const int d2 = (int)(off2[v + 1] - off2[v]);
-        l2[v] = d2;
-        label[v] = (d >= need && d2 >= min_size - 1) ? 0 : -1;
-    }
-    __syncthreads();
-    for (int v = tid; v < n; v += nt) {
-        if (label[v] != 0) continue;
-        int c = 0;
-        for (int64_t e = off[v]; e < off[v + 1]; e++) c += label[adj[e]] == 0;
-        exdeg[v] = c;
-    }
-    __syncthreads();
-    for (;;) {
-        if (tid == 0) changed = 0;
-        __syncthreads();
-        for (int v = tid; v < n; v += nt)
-            if (label[v] == 0 && exdeg[v] < need) {
-                label[v] = -2;
-                changed = 1;
-            }
-        __syncthreads();
-        if (!changed) break;
-        for (int v = tid; v < n; v += nt)
-            if (label[v] == -2)
-                for (int64_t e = off[v]; e < off[v + 1]; e++) {
-                    const int w = adj[e];
-                    if (label[w] == 0) atomicSub(&exdeg[w], 1);
-                }
-        __syncthreads();
-        for (int v = tid; v < n; v += nt)
-            if (label[v] == -2) label[v] = -1;
-        __syncthreads();
-    }
-    if (tid == 0) {
-        best = 0;
-        cnt = 0;
-        ncov = 0;
-    }
-    __syncthreads();
-    for (int v = tid; v < n; v += nt)
-        if (label[v] == 0 && exdeg[v] > 0)
-            atomicMax(&best, ((unsigned long long)(unsigned)exdeg[v] << 32) |
-                                 (unsigned long long)(0xffffffffu - (unsigned)v));
-    __syncthreads();
-    if (best) {
-        const int bv = (int)(0xffffffffu - (unsigned)(best & 0xffffffffull));
-        for (int64_t e = off[bv] + tid; e < off[bv + 1]; e += nt) {
-            const int w = adj[e];
-            if (label[w] == 0) label[w] = 2;
-        }
-        __syncthreads();
-        if (tid == 0) label[bv] = 3;
-    }
-    __syncthreads();
-    for (int v = tid; v < n; v += nt) {
-        const int lb = label[v];
-        if (lb < 0) continue;
-        const unsigned long long rank = lb == 2 ? 0ull : (lb == 0 ? 1ull : 2ull);
-        const unsigned long long key = (rank << 51) |
-                                       ((unsigned long long)(0x1ffff - exdeg[v]) << 34) |
-                                       ((unsigned long long)(0x1ffff - l2[v]) << 17) |
-                                       (unsigned long long)(0x1ffff - v);
-        keys[atomicAdd(&cnt, 1)] = key;
-        if (lb == 2) atomicAdd(&ncov, 1);
-    }
-    __syncthreads();
-    const int t = cnt;
-    int N = 1;
-    while (N < t) N <<= 1;
-    for (int i = t + tid; i < N; i += nt) keys[i] = ~0ull;
-    __syncthreads();
-    for (int k = 2; k <= N; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = tid; i < N; i += nt) {
-                const int p = i ^ j;
-                if (p > i) {
-                    const unsigned long long x = keys[i], y = keys[p];
-                    if ((x > y) == ((i & k) == 0)) {
-                        keys[i] = y;
-                        keys[p] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    for (int i = tid; i < t; i += nt) ids[i] = 0x1ffff - (int)(keys[i] & 0x1ffffull);
-    if (tid == 0) {
-        info[0] = t;
-        info[1] = ncov;
     }
 }
 

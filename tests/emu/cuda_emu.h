@@ -22,6 +22,10 @@
 #define __global__
 #define __host__
 #define __forceinline__ inline
+#define __launch_bounds__(...)
+// block-shared variables of a kernel: one copy per process, so an emulated
+// kernel that declares them runs as a single block, one launch at a time
+#define __shared__ static
 
 struct emu_dim3 {
     unsigned x = 0, y = 0, z = 0;
@@ -34,10 +38,11 @@ inline thread_local emu_dim3 threadIdx, blockIdx, blockDim, gridDim;
 struct EmuBarrier {
     std::atomic<int> count{0};
     std::atomic<int> phase{0};
+    int parties = 32;
     void arrive_and_wait()
     {
         int ph = phase.load(std::memory_order_acquire);
-        if (count.fetch_add(1, std::memory_order_acq_rel) == 31) {
+        if (count.fetch_add(1, std::memory_order_acq_rel) == parties - 1) {
             count.store(0, std::memory_order_relaxed);
             phase.store(ph + 1, std::memory_order_release);
             return;
@@ -52,6 +57,7 @@ struct EmuWarp {
     uint64_t slot[32];
 };
 inline thread_local EmuWarp* emu_w = nullptr;
+inline thread_local EmuBarrier* emu_blk = nullptr; // every thread of this block
 inline thread_local int emu_lane = 0;
 inline thread_local unsigned char* emu_smem = nullptr; // this block's dynamic shared memory
 inline unsigned char* emu_dyn_smem() { return emu_smem; }
@@ -105,6 +111,12 @@ inline unsigned __ballot_sync(unsigned, int pred)
 inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0; }
 inline int __all_sync(unsigned m, int pred) { return __ballot_sync(m, pred) == 0xffffffffu; }
 inline void __syncwarp(unsigned = 0xffffffffu) { emu_w->bar.arrive_and_wait(); }
+inline void __syncthreads()
+{
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    emu_blk->arrive_and_wait();
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+}
 inline int __popc(unsigned x) { return __builtin_popcount(x); }
 template <class T> inline T __ldcg(const T* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 template <class T> inline T __ldg(const T* p) { return *p; }
@@ -175,14 +187,18 @@ inline void emu_launch(int blocks, int threads, const std::function<void()>& fn,
     std::vector<std::thread> th;
     std::vector<std::vector<unsigned char>> smem((size_t)blocks,
                                                  std::vector<unsigned char>(smem_bytes + 16));
+    std::vector<EmuBarrier> blk((size_t)blocks);
+    for (auto& bb : blk) bb.parties = threads;
     for (int b = 0; b < blocks; b++)
         for (int w = 0; w < nwarps_per_block; w++) {
             EmuWarp* ew = new EmuWarp();
             warps.push_back(ew);
             unsigned char* sb = smem[(size_t)b].data();
+            EmuBarrier* bbar = &blk[(size_t)b];
             for (int l = 0; l < 32; l++) {
                 th.emplace_back([=, &fn] {
                     emu_w = ew;
+                    emu_blk = bbar;
                     emu_lane = l;
                     emu_smem = sb;
                     threadIdx.x = w * 32 + l;

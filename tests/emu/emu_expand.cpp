@@ -7,6 +7,7 @@
 
 #include "../../cuqc_b200/csrc/expand_kernel.cuh"
 #include "../../cuqc_b200/csrc/host.h"
+#include "../../cuqc_b200/csrc/level0_kernel.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -277,4 +278,24 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     *out_nints = k;
     *out_buf = out;
     return ctl.status;
+}
+
+// The product's device level 0 (level0_kernel.cuh) as one emulated block of
+// `threads` threads; ids_out receives the root in Q order, info = {size,
+// covered count}.
+extern "C" int emu_level0(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
+                          double gamma, int min_size, int threads, int32_t* ids_out,
+                          int32_t* info)
+{
+    std::vector<int32_t> md, ubt;
+    gamma_tables(gamma, n, min_size, md, ubt);
+    int P = 1;
+    while (P < n) P <<= 1;
+    std::vector<int32_t> exdeg((size_t)n), label((size_t)n), l2((size_t)n);
+    std::vector<unsigned long long> keys((size_t)P);
+    emu_launch(1, threads, [&] {
+        level0_kernel(off, adj, off2, n, md[(size_t)min_size], min_size, exdeg.data(),
+                      label.data(), l2.data(), keys.data(), ids_out, info);
+    });
+    return 0;
 }

@@ -52,3 +52,20 @@ def test_emulated_batch_matches_oracle_per_instance():
     for g, gm, ms, got in zip(gs, gms, mss, per):
         want, _ = oracle.mine(g, gm, ms, "clean")
         assert canon(got) == canon(want)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_emulated_device_level0_matches_oracle_root(seed):
+    """The product's device level 0 (one emulated block of 64 threads) gives the
+    oracle's root: same vertices in the same Q order, same covered count."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(20, 200))
+    g = graphs.random_small(n, float(rng.uniform(0.03, 0.3)), 500 + seed,
+                            planted=int(rng.integers(0, 4)), size=int(rng.integers(5, 16)),
+                            density=float(rng.uniform(0.8, 1.0)))
+    gamma = [0.5, 0.6, 0.7, 0.8, 0.9, 1.0][seed % 6]
+    ms = int(rng.integers(3, 9))
+    want_ids, want_lab, _ = oracle.root(g, gamma, ms)
+    ids, cov = emu.level0(g, gamma, ms)
+    assert ids.tolist() == want_ids.tolist()
+    assert cov == int((want_lab == 2).sum())
