@@ -405,6 +405,17 @@ def run_serving(args):
     print(json.dumps(line))
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """The largest of every rank's `x` (each rank passes its own; with no
+    process group, x itself).  Every rank takes this step, in the same order."""
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
 
@@ -458,10 +469,7 @@ def run_ours(args):
             assert res.sets == ref_sets
         barrier()
     launches = res.stats["kernel_launches"] - launches0
-    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(t.item())
+    elapsed_max = max_over_ranks(elapsed, dist, dev)
     value = world * args.steps / (elapsed_max / 1000.0)
 
     # e2e: from host CSR arrays through the C ABI, result read back
@@ -476,10 +484,7 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - e2e_t0
     assert all(r2.sets == ref_sets for r2 in outs)
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / float(te.item())
+    e2e_value = world * args.steps / max_over_ranks(e2e_s, dist, dev)
     h2d = 8 * (g.n + 1) * 2 + 4 * g.m + 4 * g.m2
     d2h = 4 * sum(1 + len(s) for s in ref_sets)
 
