@@ -25,7 +25,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libqc_oracle.so")
 REFCPU_PATH = os.path.join(HERE, "_ref", "libqc_refcpu.so")
 ADJTOSER_PATH = os.path.join(HERE, "_ref", "adjToSer")
-REFBIN_PATH = os.path.join(HERE, "_ref", "cuQC_ref")
 
 MODE_HOST, MODE_BINARY, MODE_CLEAN = 0, 1, 2
 _MODES = {"host": MODE_HOST, "binary": MODE_BINARY, "clean": MODE_CLEAN}

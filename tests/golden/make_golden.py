@@ -6,9 +6,11 @@ serialized format plus result files the REFERENCE produced for it:
                         initialize_tasks, h_expand_level and RemoveNonMax,
                         compiled from the reference sources by oracle/Makefile
                         into oracle/_ref/libqc_refcpu.so), made by this script;
-  <name>.refbin.result  the reference binary (oracle/_ref/cuQC_ref, built from
-                        main.cu for sm_100a) run on a B200 by
-                        tests/golden/run_refbin.sh.  Large graphs are not stored: their generator
+  <name>.refbin.result  the reference binary (built from main.cu for sm_100a)
+                        run once on a B200; these and its temp.txt files
+                        (*.refbin.temp) and logs (refbin_logs/) are frozen
+                        records -- the binary is not built or run again
+                        (it faulted on small inputs).  Large graphs are not stored: their generator
 parameters and a digest of the serialized text are, so the tests regenerate
 them and check the digest first.
 
