@@ -1290,7 +1290,8 @@ std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
 
 std::string qcb_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
                                int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
-                               int64_t* total_out, cudaStream_t s, int* too_large, int* too_small);
+                               int64_t* total_out, cudaStream_t s, int* too_large, int* too_small,
+                               int* bad_csr);
 
 extern "C" qc_status qc_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
                                        int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
@@ -1301,11 +1302,12 @@ extern "C" qc_status qc_twohop_noalloc(int32_t n, const int64_t* d_off, const in
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(QC_ERR_NO_DEVICE, "no CUDA device visible");
-    int too_large = 0, too_small = 0;
+    int too_large = 0, too_small = 0, bad_csr = 0;
     std::string e = qcb_twohop_noalloc(n, d_off, d_adj, d_off2, d_adj2, adj2_cap, total_out,
-                                       (cudaStream_t)stream, &too_large, &too_small);
+                                       (cudaStream_t)stream, &too_large, &too_small, &bad_csr);
     if (e.empty()) return QC_OK;
     if (too_large) return fail(QC_ERR_TOO_LARGE, e);
+    if (bad_csr) return fail(QC_ERR_FORMAT, e);
     if (too_small) return fail(QC_ERR_RESULT_OVERFLOW, e);
     return fail(QC_ERR_CUDA, e);
 }

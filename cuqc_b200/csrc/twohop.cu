@@ -28,10 +28,17 @@ namespace {
 
 constexpr int kTwohopWarpsPerBlock = 8;
 
-__device__ void mark_row(const int64_t* off, const int32_t* adj, int v, uint32_t* bm,
-                         int32_t* touched, int* ntouched, int lane)
+// Marks N(v) u N(N(v)) minus {v} in the warp's bitmap.  With `err` set (the
+// no-allocation form, whose CSR was not checked on the host) an id outside
+// [0, n) is skipped and recorded instead of being used as an index.
+__device__ void mark_row(int n, const int64_t* off, const int32_t* adj, int v, uint32_t* bm,
+                         int32_t* touched, int* ntouched, int lane, int* err)
 {
     auto mark = [&](int w) {
+        if (err && (unsigned)w >= (unsigned)n) {
+            atomicOr(err, 2);
+            return;
+        }
         uint32_t b = 1u << (w & 31);
         uint32_t old = atomicOr(&bm[w >> 5], b);
         if (old == 0) {
@@ -42,6 +49,7 @@ __device__ void mark_row(const int64_t* off, const int32_t* adj, int v, uint32_t
     for (int64_t e = off[v] + lane; e < off[v + 1]; e += 32) mark(adj[e]);
     for (int64_t e = off[v]; e < off[v + 1]; e++) {
         int u = adj[e];
+        if (err && (unsigned)u >= (unsigned)n) continue; // recorded by mark(u) above
         for (int64_t f = off[u] + lane; f < off[u + 1]; f += 32) {
             int w = adj[f];
             if (w != v) mark(w);
@@ -54,8 +62,9 @@ __device__ void mark_row(const int64_t* off, const int32_t* adj, int v, uint32_t
 __global__ void twohop_kernel(int n, const int64_t* off, const int32_t* adj, uint32_t* bitmaps,
                               int64_t bm_words, int32_t* touched_all, int64_t touched_cap,
                               int* ntouched_all, int64_t* count_out, const int64_t* off2,
-                              int32_t* adj2)
+                              int32_t* adj2, int* err)
 {
+    if (err && *(volatile int*)err) return; // the CSR check failed: write nothing
     int lane = threadIdx.x & 31;
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int nw = (gridDim.x * blockDim.x) >> 5;
@@ -65,7 +74,7 @@ __global__ void twohop_kernel(int n, const int64_t* off, const int32_t* adj, uin
     for (int v = warp; v < n; v += nw) {
         if (lane == 0) *nt = 0;
         __syncwarp();
-        mark_row(off, adj, v, bm, touched, nt, lane);
+        mark_row(n, off, adj, v, bm, touched, nt, lane, err);
         // a self loop in N(v) keeps v (as the reference keeps it); v is never
         // added through N(N(v))
         int k = *(volatile int*)nt;
@@ -169,7 +178,8 @@ std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
     if (!h.adj.empty())
         TCK(cudaMemcpy(d_adj, h.adj.data(), sizeof(int32_t) * h.adj.size(), cudaMemcpyHostToDevice));
     twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32>>>(n, d_off, d_adj, d_bm, bm_words, d_touched,
-                                                         touched_cap, d_nt, d_cnt, nullptr, nullptr);
+                                                         touched_cap, d_nt, d_cnt, nullptr, nullptr,
+                                                         nullptr);
     TCK(cudaGetLastError());
     cnt.resize((size_t)n);
     TCK(cudaMemcpy(cnt.data(), d_cnt, sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
@@ -179,7 +189,8 @@ std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
     TCK(cudaMalloc(&d_adj2, sizeof(int32_t) * std::max<size_t>(adj2.size(), 1)));
     TCK(cudaMemcpy(d_off2, off2.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
     twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32>>>(n, d_off, d_adj, d_bm, bm_words, d_touched,
-                                                         touched_cap, d_nt, nullptr, d_off2, d_adj2);
+                                                         touched_cap, d_nt, nullptr, d_off2, d_adj2,
+                                                         nullptr);
     TCK(cudaGetLastError());
     if (!adj2.empty())
         TCK(cudaMemcpy(adj2.data(), d_adj2, sizeof(int32_t) * adj2.size(), cudaMemcpyDeviceToHost));
@@ -201,23 +212,39 @@ done:
 // For callers that cannot call cudaMalloc: an application whose device
 // memory is owned by its own pool or fixed memory plan, or that must not
 // allocate while it is serving requests.  Inputs and outputs are the
-// caller's device buffers; the per-warp working memory (a bitmap of n bits
-// and a list of touched bitmap words per warp) lives in one file-scope
+// caller's device buffers; the working memory lives in one file-scope
 // __device__ array that every GPU which loads this library holds until the
-// process exits.
+// process exits:
+//   [0, 256)        status: the two-hop entry count and the CSR-check flags
+//   [256, ...)      per-warp bitmaps of n bits, touched-word lists, counters
+// The caller's CSR is in device memory, so it is checked on the device
+// (csr_check_kernel) before any of it is used as an index.
 // ------------------------------------------------------------------
 
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 16u << 20;  // 16 MiB per device
+constexpr size_t kNoAllocHeaderBytes = 256;          // status words ahead of the warps' memory
 constexpr int kNoAllocMinWarps = 32;                 // fewest warps a call may run on
 constexpr int kNoAllocMaxDevices = 64;
+
+// CSR-check flags (NoAllocStatus::err)
+constexpr int kErrOffsets = 1;   // off[0] != 0 or off[v] > off[v+1]
+constexpr int kErrIds = 2;       // a neighbour id outside [0, n)
+constexpr int kErrNullAdj = 4;   // entries but no adjacency array
+
+struct NoAllocStatus {
+    int64_t total; // two-hop entries (off2[n]) after the scan
+    int32_t err;   // CSR-check flags
+};
 
 __device__ __align__(256) unsigned char g_twohop_scratch[kNoAllocScratchBytes];
 
 // Device address of g_twohop_scratch, looked up once per device (the host
 // symbol is only a stand-in: a kernel handed it would fault or read the
-// wrong memory).
+// wrong memory).  The cached address belongs to the device's primary
+// context, which is assumed to live as long as the process: after a
+// cudaDeviceReset on that device the cache is stale.
 struct ScratchAddr {
     std::mutex mu;
     void* ptr[kNoAllocMaxDevices] = {};
@@ -238,12 +265,41 @@ cudaError_t scratch_for_device(int dev, unsigned char** out)
     return cudaSuccess;
 }
 
-// In-place scan of off2[1..n] (per-vertex counts) into CSR offsets, off2[0] = 0.
-// One block walks the array in chunks of its size, carrying the running total.
-__global__ void twohop_scan_kernel(int64_t* off2, int n)
+// Checks the caller's device CSR before the two-hop passes read it: off[0] =
+// 0, offsets non-decreasing, off[n] >= 0, an adjacency array when off[n] > 0,
+// and every neighbour id in [0, n).  Only off[0..n] and adj[0..off[n]) are
+// read -- the extents the caller's contract gives.  Failures are or-ed into
+// st->err, which the two-hop passes read first.
+__global__ void csr_check_kernel(int n, const int64_t* off, const int32_t* adj, NoAllocStatus* st)
+{
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int bad = 0;
+    const int64_t m = off[n];
+    if (tid == 0 && (off[0] != 0 || m < 0)) bad |= kErrOffsets;
+    for (int64_t v = tid; v < n; v += stride)
+        if (off[v] > off[v + 1]) bad |= kErrOffsets;
+    if (m > 0 && !adj) {
+        bad |= kErrNullAdj;
+    } else {
+        for (int64_t e = tid; e < m; e += stride)
+            if ((unsigned)adj[e] >= (unsigned)n) bad |= kErrIds;
+    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (bad && (threadIdx.x & 31) == 0) atomicOr(&st->err, bad);
+}
+
+// In-place scan of off2[1..n] (per-vertex counts) into CSR offsets, off2[0] = 0;
+// the total goes to st->total.  One block walks the array in chunks of its
+// size, carrying the running total.  Skipped (total 0) when the CSR check failed.
+__global__ void twohop_scan_kernel(int64_t* off2, int n, NoAllocStatus* st)
 {
     __shared__ int64_t warp_tot[32];
     __shared__ int64_t carry;
+    if (*(volatile int32_t*)&st->err) {
+        if (threadIdx.x == 0) st->total = 0;
+        return;
+    }
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (tid == 0) {
         carry = 0;
@@ -275,16 +331,41 @@ __global__ void twohop_scan_kernel(int64_t* off2, int n)
         if (tid == blockDim.x - 1) carry = before + x;
         __syncthreads();
     }
+    if (tid == 0) st->total = carry;
 }
+
+std::string csr_error_text(int err)
+{
+    std::string t;
+    if (err & kErrOffsets) t += "offsets do not start at 0 or decrease";
+    if (err & kErrIds) t += std::string(t.empty() ? "" : "; ") + "a neighbour id is outside [0, n)";
+    if (err & kErrNullAdj) t += std::string(t.empty() ? "" : "; ") + "d_adj is NULL but off[n] > 0";
+    return "malformed device CSR: " + t;
+}
+
+// Per-warp working memory for n vertices: bitmap words, touched-word list
+// (padded to a power of two for the warp sort), touched counter.
+int64_t noalloc_bytes_per_warp(int64_t n, int64_t* bm_words, int64_t* touched_cap)
+{
+    int64_t w = (n + 31) / 32, tc = 1;
+    while (tc < w) tc <<= 1;
+    if (bm_words) *bm_words = w;
+    if (touched_cap) *touched_cap = tc;
+    return 4 * w + 4 * tc + 4;
+}
+
+constexpr int64_t kNoAllocWarpBytes = (int64_t)(kNoAllocScratchBytes - kNoAllocHeaderBytes);
 
 } // namespace
 
 std::string qcb_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
                                int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
-                               int64_t* total_out, cudaStream_t s, int* too_large, int* too_small)
+                               int64_t* total_out, cudaStream_t s, int* too_large, int* too_small,
+                               int* bad_csr)
 {
     *too_large = 0;
     *too_small = 0;
+    *bad_csr = 0;
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return std::string("cudaGetDevice: ") + cudaGetErrorString(e);
@@ -297,13 +378,9 @@ std::string qcb_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d
         if (total_out) *total_out = 0;
         return e == cudaSuccess ? "" : std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
     }
-    // per-warp working memory: bitmap words, touched-word list (padded to a
-    // power of two for the warp sort), touched counter
-    const int64_t bm_words = ((int64_t)n + 31) / 32;
-    int64_t touched_cap = 1;
-    while (touched_cap < bm_words) touched_cap <<= 1;
-    const int64_t per_warp = 4 * bm_words + 4 * touched_cap + 4;
-    int64_t fit = (int64_t)kNoAllocScratchBytes / per_warp;
+    int64_t bm_words = 0, touched_cap = 0;
+    const int64_t per_warp = noalloc_bytes_per_warp(n, &bm_words, &touched_cap);
+    const int64_t fit = kNoAllocWarpBytes / per_warp;
     if (fit < kNoAllocMinWarps) {
         *too_large = 1;
         return "graph has " + std::to_string(n) + " vertices; qc_twohop_noalloc supports at most " +
@@ -314,32 +391,42 @@ std::string qcb_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d
     int64_t nwarps = std::min<int64_t>(fit, (int64_t)sms * 2 * kTwohopWarpsPerBlock);
     nwarps -= nwarps % kTwohopWarpsPerBlock;
     const int blocks = (int)(nwarps / kTwohopWarpsPerBlock);
-    uint32_t* bm = (uint32_t*)scratch;
-    int32_t* touched = (int32_t*)(scratch + 4 * bm_words * nwarps);
-    int* nt = (int*)(scratch + 4 * bm_words * nwarps + 4 * touched_cap * nwarps);
-    // the array keeps the last call's contents: the bitmaps must start empty
-    e = cudaMemsetAsync(bm, 0, sizeof(uint32_t) * bm_words * nwarps, s);
+    NoAllocStatus* st = (NoAllocStatus*)scratch;
+    unsigned char* warp_mem = scratch + kNoAllocHeaderBytes;
+    uint32_t* bm = (uint32_t*)warp_mem;
+    int32_t* touched = (int32_t*)(warp_mem + 4 * bm_words * nwarps);
+    int* nt = (int*)(warp_mem + 4 * bm_words * nwarps + 4 * touched_cap * nwarps);
+    // the array keeps the last call's contents: the status words and the
+    // bitmaps (contiguous) must start at zero
+    e = cudaMemsetAsync(scratch, 0, kNoAllocHeaderBytes + sizeof(uint32_t) * bm_words * nwarps, s);
     if (e != cudaSuccess) return std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+    csr_check_kernel<<<sms * 4, 256, 0, s>>>(n, d_off, d_adj, st);
     // pass 1: per-vertex counts into off2[1..n], then the scan
     twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32, 0, s>>>(
-        n, d_off, d_adj, bm, bm_words, touched, touched_cap, nt, d_off2 + 1, nullptr, nullptr);
-    twohop_scan_kernel<<<1, 1024, 0, s>>>(d_off2, n);
+        n, d_off, d_adj, bm, bm_words, touched, touched_cap, nt, d_off2 + 1, nullptr, nullptr,
+        &st->err);
+    twohop_scan_kernel<<<1, 1024, 0, s>>>(d_off2, n, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return std::string("launch: ") + cudaGetErrorString(e);
-    int64_t total = 0;
-    e = cudaMemcpyAsync(&total, d_off2 + n, sizeof(total), cudaMemcpyDeviceToHost, s);
+    NoAllocStatus hs{};
+    e = cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return std::string("two-hop count: ") + cudaGetErrorString(e);
-    if (total_out) *total_out = total;
+    if (hs.err) {
+        *bad_csr = 1;
+        return csr_error_text(hs.err);
+    }
+    if (total_out) *total_out = hs.total;
     if (!d_adj2) return ""; // size query
-    if (total > adj2_cap) {
+    if (hs.total > adj2_cap) {
         *too_small = 1;
         return "adj2 holds " + std::to_string(adj2_cap) + " entries; the two-hop lists need " +
-               std::to_string(total);
+               std::to_string(hs.total);
     }
     // pass 2: sorted rows
     twohop_kernel<<<blocks, kTwohopWarpsPerBlock * 32, 0, s>>>(
-        n, d_off, d_adj, bm, bm_words, touched, touched_cap, nt, nullptr, d_off2, d_adj2);
+        n, d_off, d_adj, bm, bm_words, touched, touched_cap, nt, nullptr, d_off2, d_adj2,
+        &st->err);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return std::string("two-hop rows: ") + cudaGetErrorString(e);
@@ -351,9 +438,7 @@ extern "C" int32_t qc_twohop_noalloc_max_vertices(void)
     // largest n (a multiple of 32) whose per-warp working memory still leaves
     // room for kNoAllocMinWarps warps; the need grows with n
     auto fits = [](int64_t n) {
-        int64_t w = (n + 31) / 32, tc = 1;
-        while (tc < w) tc <<= 1;
-        return (int64_t)kNoAllocScratchBytes / (4 * w + 4 * tc + 4) >= kNoAllocMinWarps;
+        return kNoAllocWarpBytes / noalloc_bytes_per_warp(n, nullptr, nullptr) >= kNoAllocMinWarps;
     };
     int64_t lo = 32, hi = (int64_t)1 << 30; // fits(lo), !fits(hi)
     while (hi - lo > 32) {

@@ -77,15 +77,21 @@ qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int32_t* adj, q
  * the rows need more than adj2_cap entries the call returns
  * QC_ERR_RESULT_OVERFLOW with *total_out set to the size needed.
  *
+ * The CSR is checked on the device before it is used as an index: offsets
+ * starting at 0 and non-decreasing, every neighbour id in [0, n), and d_adj
+ * not NULL when d_off[n] > 0; a failed check returns QC_ERR_FORMAT and
+ * writes no rows.  Only d_off[0..n] and d_adj[0..d_off[n]) are read.
+ *
  * Working memory is one 16 MiB array in device memory that every GPU which
  * loads the library holds until the process exits; graphs above
  * qc_twohop_noalloc_max_vertices() vertices are rejected with
  * QC_ERR_TOO_LARGE.  The first call on a device looks up that array's device
- * address, so make it before any stream capture.  All calls share the array:
- * calls whose work overlaps on the GPU (other threads, other streams) race
- * and must be serialised by the caller.  The call runs on `stream` (a
- * cudaStream_t; NULL = the default stream) and returns when the lists are
- * written. */
+ * address (and keeps it for the life of the device's primary context), so
+ * make it before any stream capture.  All calls share the array: calls whose
+ * work overlaps on the GPU (other threads, other streams) race and must be
+ * serialised by the caller.  The call runs on `stream` (a cudaStream_t;
+ * NULL = the default stream) and is synchronous: it waits on that stream
+ * and returns when the lists are written. */
 qc_status qc_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_adj,
                             int64_t* d_off2, int32_t* d_adj2, int64_t adj2_cap,
                             int64_t* total_out, void* stream);
