@@ -405,6 +405,86 @@ def run_serving(args):
     print(json.dumps(line))
 
 
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _golden_graph(case, workdir):
+    """Path of a golden case's serialized graph (stored, or regenerated from
+    its recorded generator parameters and checked against its digest)."""
+    import hashlib
+
+    if case["stored_graph"]:
+        return os.path.join(GOLDEN, case["name"] + ".graph")
+    g = getattr(graphs, case["generator"])(**case["kwargs"])
+    path = os.path.join(workdir, case["name"] + ".graph")
+    graphs.write_serialized(g, path)
+    with open(path, "rb") as f:
+        if hashlib.sha256(f.read()).hexdigest() != case["graph_sha256"]:
+            raise SystemExit("generator output drifted for " + case["name"])
+    return path
+
+
+def _stdout_ms(text, key):
+    for line in text.splitlines():
+        if line.startswith("--->:%s: " % key):
+            return float(line.split(":")[2].split()[0])
+    return None
+
+
+def run_refbin_compare(args):
+    """The drop-in CLI on every golden graph the reference binary completed on a
+    B200 (its stdout is frozen in tests/golden/refbin_logs/), run the same way
+    here: one process per graph, each in its own directory.  Prints both
+    programs' ENUMERATION and TOTAL lines, this build's expansion-kernel time,
+    and whether the result files are identical.  The reference binary is not
+    run; its numbers come from its logs."""
+    import cuqc_b200 as Q
+
+    with open(os.path.join(GOLDEN, "manifest.json")) as f:
+        cases = [c for c in json.load(f) if c.get("refbin") == "ok"]
+    work = tempfile.mkdtemp(prefix="refbin_cmp_")
+    rows = []
+    for c in cases:
+        path = _golden_graph(c, work)
+        with open(os.path.join(GOLDEN, "refbin_logs", c["name"] + ".refbin.log")) as f:
+            ref_log = f.read()
+        d = os.path.join(work, c["name"])
+        os.makedirs(d, exist_ok=True)
+        enum, kern, total = [], [], []
+        same = True
+        for _ in range(max(1, args.steps)):
+            out = os.path.join(d, "out.txt")
+            rc, text = Q.cli(path, c["gamma"], c["min_size"], out, 0, cwd=d)
+            if rc != 0:
+                raise SystemExit("cuQC failed on %s: %s" % (c["name"], text[-400:]))
+            enum.append(_stdout_ms(text, "ENUMERATION TIME"))
+            kern.append(_stdout_ms(text, "EXPANSION KERNEL TIME"))
+            total.append(_stdout_ms(text, "TOTAL TIME"))
+            with open(out) as f1, open(os.path.join(GOLDEN, c["name"] + ".refbin.result")) as f2:
+                same = same and f1.read() == f2.read()
+        rows.append({"graph": c["name"], "gamma": c["gamma"], "min_size": c["min_size"],
+                     "ref_enumeration_ms": _stdout_ms(ref_log, "ENUMERATION TIME"),
+                     "ref_total_ms": _stdout_ms(ref_log, "TOTAL TIME"),
+                     "enumeration_ms": statistics.median(enum),
+                     "expansion_kernel_ms": statistics.median(kern),
+                     "total_ms": statistics.median(total),
+                     "result_identical": same})
+    ratios = [r["ref_enumeration_ms"] / max(r["enumeration_ms"], 1.0) for r in rows]
+    line = {
+        "metric": "ENUMERATION TIME line of the drop-in CLI vs the reference binary's (ms)",
+        "value": statistics.median(r["enumeration_ms"] for r in rows), "unit": "ms",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": 0,
+        "dtype": "int32", "data": "golden graphs the reference binary completed on a B200",
+        "config": {"workload": "refbin-goldens", "graphs": len(rows),
+                   "reference": "frozen stdout of the reference binary (main.cu built for "
+                                "sm_100a, one run per graph on a B200 of this pool)"},
+        "graphs": rows,
+        "all_results_identical": all(r["result_identical"] for r in rows),
+        "min_ratio_at_1ms_floor": min(ratios),
+    }
+    print(json.dumps(line))
+
+
 def max_over_ranks(x, dist=None, device=None):
     """The largest of every rank's `x` (each rank passes its own; with no
     process group, x itself).  Every rank takes this step, in the same order."""
@@ -556,7 +636,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
-                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + ["cfg5"])
+                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + ["cfg5", "refbin-goldens"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-instances", type=int, default=8)
     ap.add_argument("--instances", type=int, default=256, help="batched workload size")
@@ -571,6 +651,8 @@ def main():
         run_reference(args)
     elif args.workload == "cfg5":
         run_serving(args)
+    elif args.workload == "refbin-goldens":
+        run_refbin_compare(args)
     elif args.workload in BATCH_WORKLOADS:
         run_batch(args)
     else:

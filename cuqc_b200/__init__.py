@@ -38,6 +38,7 @@ EXPORTS = [
     "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
     "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune", "qc_maximal_sets",
+    "qc_context_last_stats",
 ]
 
 
@@ -125,6 +126,7 @@ def lib():
         L.qc_twohop_noalloc.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int64, P64, vp]
         L.qc_twohop_noalloc_max_vertices.restype = C.c_int32
         L.qc_maximal_sets.argtypes = [vp, P32, C.c_int64, C.c_int32, C.POINTER(vp)]
+        L.qc_context_last_stats.argtypes = [vp, C.POINTER(Stats)]
         _lib = L
     return _lib
 
@@ -272,6 +274,25 @@ class Context:
         r = C.c_void_p()
         _check(lib().qc_mine(self.h, dg.h, float(gamma), int(min_size), int(sched), C.byref(r)))
         return self._result(r)
+
+    def last_stats(self):
+        """Counters of the most recent expansion on this context (dict), also
+        of a run that stopped at cfg.time_limit_ms."""
+        st = Stats()
+        _check(lib().qc_context_last_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def mine_budgeted(self, g, gamma, min_size):
+        """Mine with the context's time limit; returns (result or None,
+        counters, finished).  A run that hits the limit gives no sets, only
+        the counts of the work done until it stopped."""
+        try:
+            r = self.mine(g, gamma, min_size)
+            return r, r.stats, True
+        except QCError as e:
+            if e.status != 8:
+                raise
+            return None, self.last_stats(), False
 
     def tune(self, g, gamma, min_size, repeats=2):
         """Pick the fastest launch shape for this device on (g, gamma,

@@ -159,6 +159,7 @@ struct qc_context {
     uint64_t use_clock = 0;
     int64_t arena_bytes = 0, stack_slots = 0, result_ints = 0;
     int64_t launches = 0;
+    qc_stats last{}; // counters of the most recent expansion, also of one that stopped
 };
 
 extern "C" void qc_config_default(qc_config* c)
@@ -482,6 +483,27 @@ static qc_status make_resident(qc_context* c, const qc_graph* g,
     return QC_OK;
 }
 
+// The work counters of the launch that just ended, kept in the context so a
+// caller can read them after a run that stopped at its time limit.
+static void record_last(qc_context* c, const Control& ctl, float kms, int root_size)
+{
+    qc_stats& l = c->last;
+    l = qc_stats{};
+    l.tasks = (int64_t)ctl.tasks;
+    l.branches = (int64_t)ctl.branches;
+    l.children = (int64_t)ctl.children;
+    l.emitted = (int64_t)ctl.emitted;
+    l.emitted_ints = (int64_t)ctl.result_top;
+    l.root_size = root_size;
+    l.max_task = ctl.max_task;
+    l.arena_peak = (int64_t)std::min(ctl.arena_top, ctl.arena_cap);
+    l.kernel_launches = c->launches;
+    l.kernel_ms = kms;
+    l.parent_vertices = (int64_t)ctl.parent_vertices;
+    l.p_rows = (int64_t)ctl.p_rows;
+    l.child_vertices = (int64_t)ctl.child_vertices;
+}
+
 static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
                           qc_result* r)
 {
@@ -665,6 +687,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaStreamSynchronize(s));
         float kms = 0;
         cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
+        record_last(c, ctl, kms, t);
 
         if (ctl.status & ST_TASK_OVERFLOW) {
             if (ctl.arena_top > ctl.arena_cap) c->arena_bytes *= 4;
@@ -798,6 +821,13 @@ extern "C" qc_status qc_context_upload(qc_context* c, const qc_graph* g)
 }
 
 extern "C" void* qc_context_stream(qc_context* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" qc_status qc_context_last_stats(const qc_context* c, qc_stats* out)
+{
+    if (!c || !out) return fail(QC_ERR_ARGS, "NULL argument");
+    *out = c->last;
+    return QC_OK;
+}
 
 extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
                              int32_t sched, qc_result** out)
@@ -1151,6 +1181,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         CK(cudaMemcpyAsync(&ctl, c->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
+        record_last(c, ctl, kms, 0);
         if (ctl.status & ST_TASK_OVERFLOW) {
             if (ctl.arena_top > ctl.arena_cap) c->arena_bytes *= 4;
             const bool stack_full = max_top(ctl) >= ctl.stack_cap;

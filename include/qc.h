@@ -181,6 +181,15 @@ typedef struct {
 
 typedef struct qc_result qc_result;
 
+/* Work counters of the context's most recent expansion kernel (tasks,
+ * branches, emitted sets, kernel_ms, the byte-model counters), also when
+ * that run stopped early: after qc_mine returns QC_ERR_ITER_LIMIT because
+ * cfg.time_limit_ms ran out, these are the counts of the work done until
+ * then (a budgeted measurement of a search too large to finish).  The
+ * reference prints its progress only through its DEBUG_TOGGLE size tracker
+ * (main.cu:626-660); this takes the place of that read-out. */
+qc_status qc_context_last_stats(const qc_context* ctx, qc_stats* out);
+
 /* Enumerate the maximal gamma-quasi-cliques of size >= min_size.
  * gamma in [0.5, 1], min_size > 1 (main.cu:437-446).  sched is accepted for
  * CLI compatibility (0 dynamic / 1 static, main.cu:447-453); the device work

@@ -237,6 +237,32 @@ def refcpu_run(graph_path, gamma_str, min_size, workdir=None, caps=None, times=N
     return text, np.asarray(flat, np.int32)
 
 
+def refcpu_budget(graph_path, gamma_str, min_size, budget_ms, workdir=None, caps=None):
+    """The reference's serial CPU enumeration under a wall-clock budget
+    (checked between its levels).  Returns a dict: tasks expanded, sets
+    emitted, levels, finished (bool), elapsed_ms."""
+    L = C.CDLL(REFCPU_PATH)
+    L.refcpu_budget.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_double,
+                                C.c_longlong, C.c_longlong, C.c_longlong, C.c_longlong,
+                                C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
+    L.refcpu_budget.restype = C.c_int
+    caps = caps or (1 << 26, 1 << 28, 1 << 24, 1 << 26)
+    wd = workdir or tempfile.mkdtemp(prefix="refcpu_")
+    temp = os.path.join(wd, "temp.txt")
+    out = (C.c_longlong * 4)()
+    el = C.c_double()
+    rc = L.refcpu_budget(graph_path.encode(), str(gamma_str).encode(), int(min_size),
+                         temp.encode(), float(budget_ms), *caps, out, C.byref(el))
+    if rc < 0:
+        raise RuntimeError("reference CPU path could not read %s" % graph_path)
+    try:
+        os.remove(temp)
+    except OSError:
+        pass
+    return {"tasks": int(out[0]), "emitted": int(out[1]), "levels": int(out[2]),
+            "finished": bool(out[3]), "elapsed_ms": float(el.value)}
+
+
 def adjtoser(adjlist_path, out_path):
     """The reference's adjacency-list -> serialized converter (adjToSer.cpp)."""
     subprocess.check_call([ADJTOSER_PATH, adjlist_path, out_path])

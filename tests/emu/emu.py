@@ -56,7 +56,7 @@ def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20, small_path=
     off2, adj2 = np.ascontiguousarray(g.off2, np.int64), np.ascontiguousarray(g.adj2, np.int32)
     ni = C.c_int64()
     buf = C.POINTER(C.c_int32)()
-    cnt = np.zeros(8, np.int64)
+    cnt = np.zeros(11, np.int64)
     st = L.emu_mine(int(g.n), off.ctypes.data_as(P64 := C.POINTER(C.c_int64)),
                     adj.ctypes.data_as(C.POINTER(C.c_int32)), off2.ctypes.data_as(P64),
                     adj2.ctypes.data_as(C.POINTER(C.c_int32)), float(gamma), int(min_size),
@@ -68,7 +68,7 @@ def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20, small_path=
         flat = np.ctypeslib.as_array(buf, shape=(ni.value,)).copy()
         L.emu_free(C.cast(buf, C.c_void_p))
     keys = ["tasks", "branches", "children", "emitted", "lookahead_hits", "status", "max_task",
-            "arena_bytes"]
+            "arena_bytes", "parent_vertices", "p_rows", "child_vertices"]
     return flat, dict(zip(keys, (int(x) for x in cnt))), st
 
 

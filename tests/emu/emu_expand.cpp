@@ -52,7 +52,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     build_root(g, md.data(), min_size, ids, cov);
     *out_nints = 0;
     *out_buf = nullptr;
-    for (int i = 0; i < 8; i++) counters[i] = 0;
+    for (int i = 0; i < 11; i++) counters[i] = 0;
     if (ids.empty()) return 0;
     int t = (int)ids.size();
     int W = words_for(t);
@@ -142,6 +142,9 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     counters[5] = ctl.status;
     counters[6] = ctl.max_task;
     counters[7] = (int64_t)std::min(ctl.arena_top, ctl.arena_cap);
+    counters[8] = (int64_t)ctl.parent_vertices;
+    counters[9] = (int64_t)ctl.p_rows;
+    counters[10] = (int64_t)ctl.child_vertices;
     int64_t k = std::min<int64_t>((int64_t)ctl.result_top, (int64_t)ctl.result_cap);
     if (ctl.status) k = 0;
     int32_t* out = (int32_t*)malloc(sizeof(int32_t) * (size_t)(k > 0 ? k : 1));

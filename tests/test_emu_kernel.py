@@ -37,6 +37,9 @@ def test_emulated_kernel_matches_oracle(case, small_path):
     assert cnt["tasks"] == st["tasks"]
     assert cnt["branches"] == st["branches"]
     assert cnt["children"] == st["children"]
+    # the byte-model counters of the bench's roofline numerator
+    for k in ("parent_vertices", "p_rows", "child_vertices"):
+        assert cnt[k] == st[k], k
 
 
 def test_emulated_batch_matches_oracle_per_instance():
