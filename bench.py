@@ -183,6 +183,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "source": "nvidia-smi -lms 200"}
 
 
+def arm_config(w):
+    """The workload as both arms report it (the same dict, so the two lines
+    can be matched): name, generator description, gamma and min_size."""
+    spec = WORKLOADS[w]
+    return {"workload": w, "desc": spec["desc"], "gamma": spec["gamma"],
+            "min_size": spec["min_size"], "seed": spec["kw"]["seed"]}
+
+
 def make_graph(w):
     spec = WORKLOADS[w]
     return getattr(graphs, spec["gen"])(**spec["kw"]), spec
@@ -245,7 +253,8 @@ def run_reference(args):
         "value": value, "unit": "instances/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": w, "desc": spec["desc"], "parallelism": "one instance per core"},
+        "config": arm_config(w),
+        "parallelism": "one instance per host core",
         "cpu_baseline": {"value": value, "unit": "instances/s", "cores": procs,
                          "kind": "reference",
                          "sample": "%d full instances per step, one per core; time = the "
@@ -345,6 +354,44 @@ def run_batch(args, standalone=True):
             "batched": out,
         }
         print(json.dumps(line))
+    return out
+
+
+def run_budgeted(args, w="cfg2"):
+    """A workload whose search does not finish in minutes (config 2: its planted
+    groups of up to 60 vertices at density 0.85 make an astronomically large
+    enumeration tree), measured under a fixed time budget: the expansion kernel
+    stops after `budget_ms` and reports the tasks and branches it expanded
+    (qc_context_last_stats); the reference's own CPU path runs on the same graph
+    under a wall-clock budget checked between its levels."""
+    import cuqc_b200 as Q
+
+    g, spec = make_graph(w)
+    gamma, ms = float(spec["gamma"]), spec["min_size"]
+    budget = args.budget_ms
+    out = {"workload": "%s: %s" % (w, spec["desc"]), "budget_ms": budget}
+    with Q.Context(device=0, time_limit_ms=budget) as ctx:
+        dg = ctx.upload(g)
+        ctx.mine_budgeted(dg, gamma, ms)  # sizes the buffers
+        runs = [ctx.mine_budgeted(dg, gamma, ms) for _ in range(2)]
+    st = runs[-1][1]
+    sec = st["kernel_ms"] / 1000.0
+    out["ours"] = {"finished": runs[-1][2], "kernel_ms": st["kernel_ms"], "tasks": st["tasks"],
+                   "branches": st["branches"], "emitted": st["emitted"],
+                   "root_size": st["root_size"], "max_task": st["max_task"],
+                   "tasks_per_s": st["tasks"] / sec, "branches_per_s": st["branches"] / sec,
+                   "arena_peak_bytes": st["arena_peak"]}
+    from oracle import oracle
+    if args.cpu_baseline and oracle.refcpu_available():
+        d = tempfile.mkdtemp()
+        path = os.path.join(d, "g.txt")
+        graphs.write_serialized(g, path)
+        r = oracle.refcpu_budget(path, spec["gamma"], ms, budget, workdir=d)
+        sec_r = r["elapsed_ms"] / 1000.0
+        out["reference_cpu"] = dict(r, cores=1, tasks_per_s=r["tasks"] / sec_r if sec_r else None,
+                                    note="the reference's own CPU path; its budget is checked "
+                                         "between levels, so a level that starts before the "
+                                         "budget ends runs to completion")
     return out
 
 
@@ -496,6 +543,53 @@ def max_over_ranks(x, dist=None, device=None):
     return float(t.item())
 
 
+def replica_rate(warmup, steps, step, ok, barrier, dist=None, device=None):
+    """The timed loop every rank runs on its own replica of the instance
+    (instances are independent: no data-path collective).  `step()` mines once
+    and returns (result, device ms); `ok(result)` checks it against this rank's
+    expected result.  After `warmup` untimed steps and a barrier, `steps` timed
+    steps; the job's time is the slowest rank's (max over ranks) and the rate
+    counts every rank's steps.  Returns (rate per second, slowest total ms,
+    the timed results)."""
+    for _ in range(warmup):
+        step()
+    barrier()
+    elapsed = 0.0
+    outs = []
+    for _ in range(steps):
+        r, ms = step()
+        if not ok(r):
+            raise SystemExit("a replica's result differs from its expected result")
+        elapsed += ms
+        outs.append(r)
+    barrier()
+    slowest = max_over_ranks(elapsed, dist, device)
+    world = dist.get_world_size() if dist else 1
+    return world * steps / (slowest / 1000.0), slowest, outs
+
+
+def replica_device():
+    """The GPU of this rank: one process per GPU, rank i of a node on GPU
+    LOCAL_RANK (torchrun sets it)."""
+    return int(os.environ.get("LOCAL_RANK", os.environ.get("RANK", "0")))
+
+
+def spawn_ranks(args):
+    """`bench.py --gpus N` started without a launcher: run the same command
+    under torch.distributed.run with N ranks on this node (127.0.0.1
+    rendezvous) and return its exit code; rank 0 prints the JSON line."""
+    import socket
+
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(args.gpus), "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def run_ours(args):
     import torch
 
@@ -503,7 +597,7 @@ def run_ours(args):
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    local = replica_device()
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -526,31 +620,29 @@ def run_ours(args):
         if dist:
             dist.barrier()
 
-    for _ in range(args.warmup):
+    def step():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
         res = ctx.mine(dg, gamma, ms)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        launch_log.append(res.stats["kernel_launches"])
+        return res, e0.elapsed_time(e1)
+
+    res = ctx.mine(dg, gamma, ms)
     ref_sets = res.sets
-    stats = []
-    barrier()
-    launches0 = res.stats["kernel_launches"]
-    with ClockSampler(local) as clocks:
-        elapsed = 0.0
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1)
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            res = ctx.mine(dg, gamma, ms)
-            with torch.cuda.stream(stream):
-                e1.record(stream)
-            e1.synchronize()
-            elapsed += e0.elapsed_time(e1)
-            stats.append(res.stats)
-            assert res.sets == ref_sets
-        barrier()
-    launches = res.stats["kernel_launches"] - launches0
-    elapsed_max = max_over_ranks(elapsed, dist, dev)
-    value = world * args.steps / (elapsed_max / 1000.0)
+    launch_log = [res.stats["kernel_launches"]]  # the context's cumulative launch count
+    for _ in range(args.warmup):
+        step()
+    with ClockSampler(local) as clocks:  # sampled over the timed steps only
+        value, elapsed_max, outs = replica_rate(
+            0, args.steps, step, lambda r: r.sets == ref_sets, barrier, dist, dev)
+    stats = [r.stats for r in outs]
+    launches = launch_log[-1] - launch_log[args.warmup]  # the timed steps' own launches
 
     # e2e: from host CSR arrays through the C ABI, result read back
     barrier()
@@ -584,9 +676,9 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": elapsed_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator: %s)" % spec["desc"],
-            "config": {"workload": w, "n": g.n, "gamma": spec["gamma"], "min_size": ms,
-                       "l2": "flushed before every step (256 MiB write, untimed)",
-                       "parallelism": "replicas (one instance per GPU per step)"},
+            "config": arm_config(w),
+            "l2": "flushed before every step (256 MiB write, untimed)",
+            "parallelism": "replicas (one instance per GPU per step)",
             "enum_ms": statistics.mean(s["enum_ms"] for s in stats),
             "kernel_ms": kernel_ms,
             "filter_ms": statistics.mean(s["filter_ms"] for s in stats),
@@ -608,6 +700,11 @@ def run_ours(args):
             ctx.close()
             ctx = None
             line["batched"] = run_batch(args, standalone=False)
+        if args.budget_ms > 0 and world == 1:
+            if ctx is not None:
+                ctx.close()
+                ctx = None
+            line["cfg2_budgeted"] = run_budgeted(args)
         if args.cpu_baseline and world == 1:
             from oracle import oracle
             if oracle.refcpu_available():
@@ -642,17 +739,31 @@ def main():
     ap.add_argument("--instances", type=int, default=256, help="batched workload size")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the batched-vs-plain comparison in the default run")
+    ap.add_argument("--budget-ms", type=int, default=500,
+                    help="time budget of the config-2 measurement in the default run (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-warps", type=int, default=8, help="warps per block of each slot")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10, 30, 100, 300, 1000])
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "cfg5":
         run_serving(args)
     elif args.workload == "refbin-goldens":
         run_refbin_compare(args)
+    elif args.workload == "cfg2":
+        b = run_budgeted(args, "cfg2")
+        o = b["ours"]
+        print(json.dumps({
+            "metric": "tasks expanded/s under a %d ms time budget (the search does not finish)"
+                      % args.budget_ms,
+            "value": o["tasks_per_s"], "unit": "tasks/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": {"workload": "cfg2", "budget_ms": args.budget_ms},
+            "cfg2_budgeted": b}))
     elif args.workload in BATCH_WORKLOADS:
         run_batch(args)
     else:

@@ -509,36 +509,42 @@ __device__ void filter_valid(const ExpandParams& P, const Rules& R, Ws& ws, cons
 // iterative degree pruning (main.cu:1735-1855)
 // Entry: indeg/exdeg valid for M u Call with exdeg relative to Call.
 // D = diameter survivors (label 0).  On success R holds the candidates.
-// Returns true on invalid bounds or a non-extendable member.
+// Returns 1 on invalid bounds or a non-extendable member, 0 when the
+// fixpoint is reached, and, with may_switch, 2 when a further round is due
+// and the members and remaining candidates Rm number at most 32: the caller
+// then runs the rest of the branch on the register path.
 // ------------------------------------------------------------------
 
-__device__ bool degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
-                             int m, const uint32_t* Call, const uint32_t* D, uint32_t* Rm,
-                             Bounds& b)
+enum { DP_DONE = 0, DP_INVALID = 1, DP_SWITCH = 2 };
+
+__device__ int degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
+                            int m, const uint32_t* Call, const uint32_t* D, uint32_t* Rm,
+                            Bounds& b, bool may_switch)
 {
     const int t = T.t, W = T.W;
     uint32_t* X = ws.mk(MK_X);
     uint32_t* who = ws.mk(MK_U);
     Bounds dummy = {0, 0, 0};
     int nc = build_hist(P, R, ws, D, t, m, false, m, dummy);
-    if (lu_bounds(P, R, ws, M, t, m, nc, m, b)) return true;
-    if (!members_ok(P, R, ws, M, t, m, b)) return true;
+    if (lu_bounds(P, R, ws, M, t, m, nc, m, b)) return DP_INVALID;
+    if (!members_ok(P, R, ws, M, t, m, b)) return DP_INVALID;
     filter_valid(P, R, ws, D, t, W, m, b, Rm, nullptr);
     // X = Call \ Rm
     for (int w = lane_id(); w < W; w += 32) X[w] = Call[w] & ~Rm[w];
     __syncwarp();
     while (!bs_empty(Rm, W) && !bs_empty(X, W)) {
+        if (may_switch && m + bs_count(Rm, W) <= 32) return DP_SWITCH;
         for (int w = lane_id(); w < W; w += 32) who[w] = M[w] | Rm[w];
         __syncwarp();
         recount_exdeg(T, ws, who, Rm);
         int nv = build_hist(P, R, ws, Rm, t, m, true, m, b);
-        if (lu_bounds(P, R, ws, M, t, m, nv, m, b)) return true;
-        if (!members_ok(P, R, ws, M, t, m, b)) return true;
+        if (lu_bounds(P, R, ws, M, t, m, nv, m, b)) return DP_INVALID;
+        if (!members_ok(P, R, ws, M, t, m, b)) return DP_INVALID;
         // Rm' = valid(Rm), X = Rm \ Rm'
         filter_valid(P, R, ws, Rm, t, W, m, b, ws.mk(MK_T), X);
         bs_copy(Rm, ws.mk(MK_T), W);
     }
-    return false;
+    return DP_DONE;
 }
 
 // ------------------------------------------------------------------
@@ -758,7 +764,7 @@ __device__ int take_slot(const ExpandParams& P, int s, int idx, StackEntry& out)
 // shard at or after the warp's home shard.  Returns (in every lane) 1 with
 // the entry in lane 0's `out`, 0 when the stack is empty and no warp holds
 // work, -1 on error or abort.
-__device__ int pop_shared(const ExpandParams& P, StackEntry& out)
+__device__ int pop_shared(const ExpandParams& P, StackEntry& out, unsigned long long deadline)
 {
     const int lane = lane_id();
     const int home = home_shard();
@@ -770,7 +776,7 @@ __device__ int pop_shared(const ExpandParams& P, StackEntry& out)
         int act = 0;
         if (lane == 0) {
             if (*(volatile int*)&P.ctl->status) act = -1;
-            else if (P.deadline_ns && now_ns() > P.deadline_ns) {
+            else if (deadline && now_ns() > deadline) {
                 set_status(P, ST_DEADLINE);
                 act = -1;
             }
@@ -829,7 +835,7 @@ __device__ int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out)
     const int lane = lane_id();
     if (lane == 0) atomicAdd(&P.ctl->idle_warps, 1);
     StackEntry e;
-    int r = pop_shared(P, e);
+    int r = pop_shared(P, e, ws.sm->deadline);
     if (lane == 0) {
         atomicSub(&P.ctl->idle_warps, 1);
         if (r > 0) {
@@ -1194,6 +1200,9 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
 // one branch: add parent position q (main.cu:1086-1178)
 // ------------------------------------------------------------------
 
+__device__ void branch_rest_small(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws,
+                                  const uint32_t* M, int m1, const uint32_t* Rm, const Bounds& b);
+
 __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, int q)
 {
     const int t = T.t, W = T.W;
@@ -1236,8 +1245,13 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     }
 
     Bounds b = {0, 0, 0};
-    if (degree_prune(P, R, T, ws, M, m1, PRE, D, Rm, b)) {
+    const int dp = degree_prune(P, R, T, ws, M, m1, PRE, D, Rm, b, P.small_path != 0);
+    if (dp == DP_INVALID) {
         if (m1 >= R.min_size) check_clique(P, R, T, ws, M, m1);
+        return;
+    }
+    if (dp == DP_SWITCH) {
+        branch_rest_small(P, R, T, ws, M, m1, Rm, b);
         return;
     }
 
@@ -1306,7 +1320,7 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
     }
     uint32_t* R2 = ws.mk(MK_R);
     Bounds b2 = {0, 0, 0};
-    bool fail2 = degree_prune(P, R, T, ws, M, m2, C2, D2, R2, b2);
+    bool fail2 = degree_prune(P, R, T, ws, M, m2, C2, D2, R2, b2, false) == DP_INVALID;
     if (m2 >= R.min_size) check_clique(P, R, T, ws, M, m2);
     if (fail2) return;
     int nr = bs_count(R2, W);
@@ -1461,15 +1475,12 @@ __device__ bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int 
     return invalid;
 }
 
-// degree pruning fixpoint (main.cu:1735-1855) on words; `ex` is updated in place
-__device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, unsigned M, int m, unsigned Call,
-                            unsigned D, unsigned& Rm, int in, int& ex, Bounds& b)
+// the rounds of the degree pruning fixpoint after the first: entered with
+// the surviving candidates Rm and the removed set X (non-empty), both words
+__device__ bool prune_loop_small(const ExpandParams& P, const Rules& R, unsigned a1, unsigned M, int m,
+                                 unsigned& Rm, unsigned X, int in, int& ex, Bounds& b)
 {
     int lane = lane_id();
-    if (lu_small(P, R, M, m, D, in, ex, b)) return true;
-    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(R, in, ex, m, b))) return true;
-    Rm = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid(R, in, ex, m, b));
-    unsigned X = Call & ~Rm;
     while (Rm && X) {
         ex = __popc(a1 & Rm);
         unsigned V = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid(R, in, ex, m, b));
@@ -1480,6 +1491,17 @@ __device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, 
         Rm = R2;
     }
     return false;
+}
+
+// degree pruning fixpoint (main.cu:1735-1855) on words; `ex` is updated in place
+__device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, unsigned M, int m, unsigned Call,
+                            unsigned D, unsigned& Rm, int in, int& ex, Bounds& b)
+{
+    int lane = lane_id();
+    if (lu_small(P, R, M, m, D, in, ex, b)) return true;
+    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(R, in, ex, m, b))) return true;
+    Rm = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid(R, in, ex, m, b));
+    return prune_loop_small(P, R, a1, M, m, Rm, Call & ~Rm, in, ex, b);
 }
 
 // Whole warp: append the buffered sets to the result buffer under one
@@ -1607,6 +1629,9 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
     __syncwarp();
 }
 
+__device__ void branch_tail_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T,
+                                  unsigned M1, int m1, unsigned Rm, int in, int ex, const Bounds& b);
+
 __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T, int q)
 {
     int lane = lane_id();
@@ -1632,6 +1657,16 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
         if (m1 >= R.min_size) clique_small(P, R, ws, M1, m1, in, T.id);
         return;
     }
+    branch_tail_small(P, R, ws, T, M1, m1, Rm, in, ex, b);
+}
+
+// The rest of a branch once its first degree pruning has converged: members
+// M1 (m1 of them), candidates Rm, bounds b, degrees in/ex of this lane's
+// vertex.  Critical vertices, second pruning, clique check, child.
+__device__ void branch_tail_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T,
+                                  unsigned M1, int m1, unsigned Rm, int in, int ex, const Bounds& b)
+{
+    int lane = lane_id();
     // critical vertices (main.cu:1526-1707)
     int critv = md_at(R, m1 + b.L);
     unsigned K = __ballot_sync(QC_FULL, in_set(M1, lane) && in + ex == critv && ex > 0);
@@ -1659,8 +1694,83 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
     if (R2) child_small(P, R, ws, T, M2, m2, R2, in, ex);
 }
 
-// a fresh task of at most 32 vertices, processed whole by one warp
-__device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V)
+// A branch of a task over 32 vertices whose members M (m1 of them) and
+// remaining candidates Rm number at most 32 while its degree pruning has
+// rounds to go: the set S = M u Rm, in ascending positions, is compacted into
+// the register form (lane i holds the i-th vertex of S and its 1-hop and 2-hop
+// rows restricted to S) and the rest of the branch runs there.  Within S the
+// children's order keys need ranks: of the ids, and of the task's lookahead
+// 2-hop counts (which may exceed 31 in a large task).
+__device__ void branch_rest_small(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws,
+                                  const uint32_t* M, int m1, const uint32_t* Rm, const Bounds& b)
+{
+    const int lane = lane_id();
+    const int W = T.W;
+    uint32_t* S = ws.mk(MK_U);
+    for (int w = lane; w < W; w += 32) S[w] = M[w] | Rm[w];
+    __syncwarp();
+    const int n = compact(ws, S, T.t); // m1 + |Rm| <= 32
+    const bool act = lane < n;
+    const int pos = act ? ws.vlist()[lane] : 0;
+    SmallTask C;
+    C.t = n;
+    C.m = m1;
+    C.cov = 0;
+    C.inst = T.inst;
+    C.rows = 0;
+    C.id = act ? rec_ld(T.ids + pos) : -1;
+    const int l2v = act ? rec_ld(T.l2 + pos) : -1;
+    const uint32_t* r1 = T.A1 + (int64_t)pos * W;
+    const uint32_t* r2 = T.A2 + (int64_t)pos * W;
+    unsigned a1 = 0, a2 = 0;
+    for (int j = 0; j < n; j++) {
+        const int pj = __shfl_sync(QC_FULL, pos, j);
+        if (act) {
+            a1 |= ((rec_ld(r1 + (pj >> 5)) >> (pj & 31)) & 1u) << j;
+            a2 |= ((rec_ld(r2 + (pj >> 5)) >> (pj & 31)) & 1u) << j;
+        }
+    }
+    C.a1 = a1;
+    C.a2 = a2;
+    int idr = 0, l2r = 0;
+    for (int j = 0; j < 32; j++) {
+        const int oid = __shfl_sync(QC_FULL, C.id, j);
+        const int ol2 = __shfl_sync(QC_FULL, l2v, j);
+        if (j < n) {
+            idr += oid > C.id ? 1 : 0;
+            l2r += ol2 > l2v ? 1 : 0;
+        }
+    }
+    C.idr = idr;
+    C.l2 = 31 - l2r; // the child key orders by 31 - l2: the largest count first
+    const unsigned Mc = __ballot_sync(QC_FULL, act && bit(M, pos));
+    unsigned Rc = __ballot_sync(QC_FULL, act && bit(Rm, pos));
+    int in = __popc(a1 & Mc);
+    int ex = 0; // recounted by the next round
+    Bounds bb = b;
+    // the pending round: its removed set is non-empty (the big loop's test)
+    if (prune_loop_small(P, R, a1, Mc, m1, Rc, ~0u, in, ex, bb)) {
+        if (m1 >= R.min_size) clique_small(P, R, ws, Mc, m1, in, C.id);
+        return;
+    }
+    branch_tail_small(P, R, ws, C, Mc, m1, Rc, in, ex, bb);
+}
+
+// Branches of a small task handed to waiting warps: a fresh task with at
+// least this many branches is split when other warps wait for work.
+constexpr int kSmallSplitMin = 4;
+// at most this many branch ranges pushed by one task
+constexpr int kSmallSplitMax = 16;
+
+// A task of at most 32 vertices on the register path.  A fresh task
+// (q_lo < 0) runs its lookahead and finds its branch range; when other warps
+// wait for work it keeps the first part of its branches and pushes the rest
+// as branch ranges (the record's l2 counts are written back first, since the
+// children's order reads them).  A branch-range item (q_lo >= 0) of a split
+// task runs its branches only.  Returns true when this call pushed branch
+// ranges of the record, which is then shared.
+__device__ bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V,
+                              int q_lo, int q_hi)
 {
     int lane = lane_id();
     SmallTask T;
@@ -1675,57 +1785,91 @@ __device__ void process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
     T.l2 = act ? rec_ld(V.l2 + lane) : 0;
     if (__any_sync(QC_FULL, act && (T.id < 0 || T.id >= R.n))) {
         if (lane == 0) check_fail(P, 8, V.rec); // a vertex id outside the instance
-        return;
+        return false;
     }
     // issued now, first read by a branch after the lookahead has run
     T.rows = act ? (int)((R.off[T.id + 1] - R.off[T.id]) + (R.off2[T.id + 1] - R.off2[T.id])) : 0;
     const int t = T.t, m = T.m;
     unsigned Mm = low_mask(m), Cm = low_mask(t) & ~Mm;
     int in = __popc(T.a1 & Mm), ex = __popc(T.a1 & Cm);
-    if (lane == 0) {
-        ws.sm->cnt.tasks++;
-        if ((unsigned long long)t > ws.sm->cnt.max_task) ws.sm->cnt.max_task = t;
-    }
-    // lookahead (main.cu:1349-1405)
-    int need_t = md_at(R, t);
-    if (!__any_sync(QC_FULL, in_set(Mm, lane) && in + ex < need_t)) {
-        int nc = t - m;
-        if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
-        bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
-        if (!__any_sync(QC_FULL, bad)) {
-            if (lane == 0) ws.sm->cnt.lookahead_hits++;
-            emit_small(P, R, ws, low_mask(t), T.id);
-            return;
+    int qlo = q_lo, qhi = q_hi;
+    bool pushed = false;
+    if (q_lo < 0) {
+        if (lane == 0) {
+            ws.sm->cnt.tasks++;
+            if ((unsigned long long)t > ws.sm->cnt.max_task) ws.sm->cnt.max_task = t;
         }
-    }
-    // branches run until a member would fail on removal (main.cu:1092-1099)
-    int need = mindeg(R, m);
-    int pos = 0;
-    if (in_set(Mm, lane)) {
-        int k = need - in;
-        if (k > 0) {
-            unsigned x = T.a1 & Cm;
-            for (int s = 1; s < k; s++) x &= x - 1;
-            pos = x ? __ffs(x) - 1 : t - 1;
+        // lookahead (main.cu:1349-1405)
+        int need_t = md_at(R, t);
+        if (!__any_sync(QC_FULL, in_set(Mm, lane) && in + ex < need_t)) {
+            int nc = t - m;
+            if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
+            bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
+            if (!__any_sync(QC_FULL, bad)) {
+                if (lane == 0) ws.sm->cnt.lookahead_hits++;
+                emit_small(P, R, ws, low_mask(t), T.id);
+                return false;
+            }
         }
+        // branches run until a member would fail on removal (main.cu:1092-1099)
+        int need = mindeg(R, m);
+        int pos = 0;
+        if (in_set(Mm, lane)) {
+            int k = need - in;
+            if (k > 0) {
+                unsigned x = T.a1 & Cm;
+                for (int s = 1; s < k; s++) x &= x - 1;
+                pos = x ? __ffs(x) - 1 : t - 1;
+            }
+        }
+        qlo = rmax(pos);
+        qlo = qlo > m + T.cov ? qlo : m + T.cov;
+        if (qlo > t - 1) return false;
+        // run status as read when the previous item started (no round trip here)
+        if (ws.sm->stat) return false;
+        qhi = t - 1;
+        // hand branch ranges to waiting warps (the waiting count was read when
+        // this item started): nb branches in parts of `per`, this warp keeping
+        // the first part (the highest positions, branched first)
+        const int nb = qhi - qlo + 1;
+        const int hungry = ws.sm->hungry;
+        if (hungry > 0 && nb >= kSmallSplitMin) {
+            int parts = hungry + 1;
+            parts = parts > nb / 2 ? nb / 2 : parts;
+            parts = parts > kSmallSplitMax + 1 ? kSmallSplitMax + 1 : parts;
+            const int per = (nb + parts - 1) / parts;
+            const int extra = (nb - per + per - 1) / per;
+            if (extra > 0) {
+                // the l2 counts of this task's record as the lookahead left them
+                if (act) ((int32_t*)V.l2)[lane] = T.l2;
+                __syncwarp();
+                __threadfence();
+                if (lane == 0) atomicAdd(&((TaskHdr*)(P.arena + V.rec))->refs, extra);
+                __syncwarp();
+                push_ranges(P, V.rec, qlo, qhi - per, per, extra);
+                __syncwarp();
+                if (lane == 0) ws.sm->hungry = hungry > extra ? hungry - extra : 0;
+                __syncwarp();
+                qlo = qhi - per + 1;
+                pushed = true;
+            }
+        }
+    } else if (ws.sm->stat) {
+        return false;
     }
-    int qlo = rmax(pos);
-    qlo = qlo > m + T.cov ? qlo : m + T.cov;
-    if (qlo > t - 1) return;
-    // run status as read when the previous item started (no round trip here)
-    if (ws.sm->stat) return;
     // rank of each id among the task's, largest first (the children's order)
     T.idr = 0;
     for (int j = 0; j < 32; j++) {
         const int o = __shfl_sync(QC_FULL, T.id, j);
         T.idr += (j < t && o > T.id) ? 1 : 0;
     }
-    for (int q = t - 1; q >= qlo; q--) {
+    for (int q = qhi; q >= qlo; q--) {
         branch_small(P, R, ws, T, q);
         // children of this task can go to waiting warps before its last branch
         // when many warps wait (not for the odd one that will soon get work)
         if (q > qlo && ws.sm->hungry >= kEagerHungry) donate(P, ws);
     }
+    return pushed;
 }
 
 // ------------------------------------------------------------------
@@ -1762,7 +1906,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     R.md_s = ws.sm->md;
     R.ubt_s = ws.sm->ubt;
     bool shared = it.q_lo >= 0;
-    if (!(it.q_lo < 0 && t <= 32 && P.small_path)) { // the register path checks its own ids
+    if (!(t <= 32 && P.small_path)) { // the register path checks its own ids
         int bad = 0;
         for (int v = lane; v < t; v += 32) {
             int id = rec_ld(T.ids + v);
@@ -1778,8 +1922,8 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         return shared;
     }
     int q_lo = it.q_lo, q_hi = it.q_hi;
-    if (q_lo < 0 && t <= 32 && P.small_path) {
-        process_small(P, R, ws, T);
+    if (t <= 32 && P.small_path) {
+        if (process_small(P, R, ws, T, q_lo, q_hi)) shared = true;
         return shared;
     }
     if (q_lo < 0) {
@@ -1883,7 +2027,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         int stop = 0;
         if (lane == 0) stop = *(volatile int*)&P.ctl->status;
         if (__shfl_sync(QC_FULL, stop, 0)) break;
-        if (P.deadline_ns && now_ns() > P.deadline_ns) {
+        if (ws.sm->deadline && now_ns() > ws.sm->deadline) {
             if (lane == 0) set_status(P, ST_DEADLINE);
             break;
         }
@@ -1979,6 +2123,13 @@ __global__ void expand_kernel(ExpandParams P)
         sm->en = 0;
         sm->es = 0;
         sm->cnt = WarpCount{};
+        sm->deadline = 0;
+        if (P.time_limit_ns) {
+            // the launch's start: the first warp's clock, shared through t_start
+            const unsigned long long now = now_ns();
+            const unsigned long long prev = atomicCAS(&P.ctl->t_start, 0ull, now);
+            sm->deadline = (prev ? prev : now) + P.time_limit_ns;
+        }
     }
     for (int c = lane; c < kArenaClasses; c += 32) {
         sm->fhead[c] = 0;

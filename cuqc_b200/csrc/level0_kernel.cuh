@@ -15,11 +15,33 @@
 // candidates, cover, then exdeg, 2-hop size and id, all descending.
 // info = {root size, covered count}.
 constexpr int kLevel0DeviceMax = 65536;
-__global__ void __launch_bounds__(1024) level0_kernel(const int64_t* off, const int32_t* adj,
-                                                      const int64_t* off2, int n, int need,
-                                                      int min_size, int32_t* exdeg, int32_t* label,
-                                                      int32_t* l2, unsigned long long* keys,
-                                                      int32_t* ids, int32_t* info)
+
+// Scratch of one level-0 run over n vertices: int32 exdeg, label and 2-hop
+// size arrays, then the 64-bit sort keys (padded to a power of two); every
+// array starts 16-byte aligned.
+__host__ __device__ inline int64_t level0_array_bytes(int n) { return ((int64_t)n * 4 + 15) & ~(int64_t)15; }
+__host__ __device__ inline int64_t level0_scratch_bytes(int n)
+{
+    int64_t P = 1;
+    while (P < n) P <<= 1;
+    return 3 * level0_array_bytes(n) + 8 * P;
+}
+
+// One instance of a batched launch: its graph, rules and where its scratch
+// and root ids go.
+struct Level0Job {
+    const int64_t* off;
+    const int32_t* adj;
+    const int64_t* off2;
+    int32_t n, need, min_size, pad;
+    int64_t scratch_at; // byte offset of the instance's scratch
+    int64_t ids_at;     // first entry of its root ids in the shared id array
+};
+
+// The work of one block (all of its threads take part).
+__device__ void level0_block(const int64_t* off, const int32_t* adj, const int64_t* off2, int n,
+                             int need, int min_size, int32_t* exdeg, int32_t* label, int32_t* l2,
+                             unsigned long long* keys, int32_t* ids, int32_t* info)
 {
     __shared__ int changed, cnt, ncov;
     __shared__ unsigned long long best;
@@ -116,4 +138,26 @@ __global__ void __launch_bounds__(1024) level0_kernel(const int64_t* off, const 
         info[0] = t;
         info[1] = ncov;
     }
+}
+
+__global__ void __launch_bounds__(1024) level0_kernel(const int64_t* off, const int32_t* adj,
+                                                      const int64_t* off2, int n, int need,
+                                                      int min_size, int32_t* exdeg, int32_t* label,
+                                                      int32_t* l2, unsigned long long* keys,
+                                                      int32_t* ids, int32_t* info)
+{
+    level0_block(off, adj, off2, n, need, min_size, exdeg, label, l2, keys, ids, info);
+}
+
+// Level 0 of many instances at once, one block per instance (batched mining):
+// info[2i], info[2i+1] = root size and covered count of instance i.
+__global__ void __launch_bounds__(256) level0_batch_kernel(const Level0Job* jobs, char* scratch,
+                                                           int32_t* ids_all, int32_t* info)
+{
+    const Level0Job J = jobs[blockIdx.x];
+    char* z = scratch + J.scratch_at;
+    const int64_t nb = level0_array_bytes(J.n);
+    level0_block(J.off, J.adj, J.off2, J.n, J.need, J.min_size, (int32_t*)z, (int32_t*)(z + nb),
+                 (int32_t*)(z + 2 * nb), (unsigned long long*)(z + 3 * nb), ids_all + J.ids_at,
+                 info + 2 * (int64_t)blockIdx.x);
 }

@@ -125,10 +125,11 @@ struct DevBuf {
 } // namespace
 
 struct BatchBufs {
-    DevBuf md, ubt, rules, meta, ids, pos;
+    DevBuf md, ubt, rules, meta, ids, pos, jobs, l0scratch, l0info;
     void release()
     {
-        for (DevBuf* b : {&md, &ubt, &rules, &meta, &ids, &pos}) b->release();
+        for (DevBuf* b : {&md, &ubt, &rules, &meta, &ids, &pos, &jobs, &l0scratch, &l0info})
+            b->release();
     }
 };
 
@@ -314,25 +315,6 @@ __global__ void root_rows_kernel(const int64_t* off, const int32_t* adj, const i
             if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
         }
     }
-}
-
-__global__ void globaltimer_kernel(unsigned long long* out)
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    *out = t;
-}
-
-// the device's globaltimer, read through a scratch word of the control block
-static cudaError_t read_globaltimer(cudaStream_t s, Control* scratch, unsigned long long* out)
-{
-    unsigned long long* w = &scratch->wait_fail_where;
-    globaltimer_kernel<<<1, 1, 0, s>>>(w);
-    cudaError_t e = cudaMemcpyAsync(out, w, sizeof(*out), cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(w, 0, sizeof(*w), s);
-    if (e != cudaSuccess) return e;
-    return cudaStreamSynchronize(s);
 }
 
 // ------------------------------------------------------------------
@@ -671,13 +653,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
-        P.deadline_ns = 0;
-        if (c->cfg.time_limit_ms > 0) {
-            // device globaltimer is nanoseconds; read it once on the device
-            unsigned long long now = 0;
-            CK(read_globaltimer(s, c->ctl.as<Control>(), &now));
-            P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
-        }
+        P.time_limit_ns = c->cfg.time_limit_ms > 0
+                              ? (unsigned long long)c->cfg.time_limit_ms * 1000000ull : 0ull;
         CK(cudaEventRecord(c->ev[1], s));
         expand_kernel<<<blocks, wpb * 32, sh.smem_bytes, s>>>(P);
         CK(cudaGetLastError());
@@ -1004,7 +981,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     BatchBufs& B = c->batch; // reused across calls on this context
     // every instance's graph resident on the device (uploaded on first use);
     // the rules of instance i point at its own arrays, nothing is concatenated
-    std::vector<int32_t> h_md, h_ubt, h_ids;
+    std::vector<int32_t> h_md, h_ubt;
     std::vector<Rules> rules(count);
     std::vector<int64_t> md_at_(count);
     std::vector<RootMeta> meta;
@@ -1030,31 +1007,88 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     double load_ms = ms_since(t_load);
 
     auto t_enum = clk::now();
-    uint64_t arena_at = 0;
+    // level 0 of every instance: on the device, one block per instance, for
+    // instances of up to kLevel0DeviceMax vertices (their root ids land in the
+    // shared id array at the instance's vertex base); larger ones on the host
+    std::vector<Level0Job> jobs;
+    std::vector<int32_t> job_inst;
+    std::vector<std::vector<int32_t>> host_ids(count);
+    std::vector<int32_t> root_t(count, 0), root_cov(count, 0);
+    int64_t l0_bytes = 0;
     for (int i = 0; i < count; i++) {
         const HostGraph& h = graphs[i]->h;
-        std::vector<int32_t> md, ubt, ids;
+        std::vector<int32_t> md, ubt;
         gamma_tables(gammas[i], h.n, min_sizes[i], md, ubt);
         md_at_[i] = (int64_t)h_md.size();
         rules[i].mdlen = (int32_t)md.size();
         rules[i].min_size = min_sizes[i];
         h_md.insert(h_md.end(), md.begin(), md.end());
         h_ubt.insert(h_ubt.end(), ubt.begin(), ubt.end());
-        int cov = 0;
-        build_root(h, md.data(), min_sizes[i], ids, cov);
-        if (ids.empty()) continue;
+        if (h.n == 0) continue;
+        if (h.n <= kLevel0DeviceMax) {
+            Level0Job J{};
+            J.off = rules[i].off;
+            J.adj = rules[i].adj;
+            J.off2 = rules[i].off2;
+            J.n = h.n;
+            J.need = md[(size_t)min_sizes[i]];
+            J.min_size = min_sizes[i];
+            J.scratch_at = l0_bytes;
+            J.ids_at = rules[i].vbase;
+            l0_bytes += level0_scratch_bytes(h.n);
+            jobs.push_back(J);
+            job_inst.push_back(i);
+        } else {
+            int cov = 0;
+            build_root(h, md.data(), min_sizes[i], host_ids[(size_t)i], cov);
+            root_t[(size_t)i] = (int32_t)host_ids[(size_t)i].size();
+            root_cov[(size_t)i] = cov;
+        }
+    }
+    CK(B.ids.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(vtotal, 4)));
+    for (int i = 0; i < count; i++)
+        if (!host_ids[(size_t)i].empty())
+            CK(cudaMemcpyAsync(B.ids.as<int32_t>() + rules[i].vbase, host_ids[(size_t)i].data(),
+                               sizeof(int32_t) * host_ids[(size_t)i].size(), cudaMemcpyHostToDevice,
+                               s));
+    if (!jobs.empty()) {
+        CK(upload(B.jobs, jobs, s));
+        CK(B.l0scratch.ensure((size_t)std::max<int64_t>(l0_bytes, 16)));
+        CK(B.l0info.ensure(sizeof(int32_t) * 2 * jobs.size()));
+        level0_batch_kernel<<<(unsigned)jobs.size(), 256, 0, s>>>(
+            B.jobs.as<Level0Job>(), B.l0scratch.as<char>(), B.ids.as<int32_t>(),
+            B.l0info.as<int32_t>());
+        CK(cudaGetLastError());
+        c->launches += 1;
+        std::vector<int32_t> info(2 * jobs.size());
+        CK(cudaMemcpyAsync(info.data(), B.l0info.p, sizeof(int32_t) * info.size(),
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (size_t j = 0; j < jobs.size(); j++) {
+            const int i = job_inst[j];
+            const int32_t t = info[2 * j], cov = info[2 * j + 1];
+            if (t < 0 || t > graphs[i]->h.n || cov < 0 || cov > t)
+                return fail(QC_ERR_CUDA, "level 0 size out of range");
+            root_t[(size_t)i] = t;
+            root_cov[(size_t)i] = cov;
+        }
+    }
+    uint64_t arena_at = 0;
+    int64_t rows_at = 0;
+    for (int i = 0; i < count; i++) {
+        if (root_t[(size_t)i] == 0) continue;
         RootMeta M{};
-        M.t = (int32_t)ids.size();
+        M.t = root_t[(size_t)i];
         M.W = words_for(M.t);
-        M.cov = cov;
+        M.cov = root_cov[(size_t)i];
         M.inst = i;
         M.cls = arena_class(rec_bytes(M.t, M.W));
         M.vbase = rules[i].vbase;
         M.rec = arena_at;
-        M.id_at = (int64_t)h_ids.size();
-        M.row_at = M.id_at;
+        M.id_at = rules[i].vbase;
+        M.row_at = rows_at;
+        rows_at += M.t;
         arena_at += arena_class_bytes(M.cls);
-        h_ids.insert(h_ids.end(), ids.begin(), ids.end());
         max_t = std::max(max_t, M.t);
         meta.push_back(M);
     }
@@ -1066,7 +1100,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     }
     CK(upload(B.rules, rules, s));
     const int nroots = (int)meta.size();
-    const int64_t total_rows = (int64_t)h_ids.size();
+    const int64_t total_rows = rows_at;
 
     Shape sh;
     {
@@ -1080,7 +1114,6 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
     CK(c->ctl.ensure(sizeof(Control)));
     if (nroots > 0) {
         CK(upload(B.meta, meta, s));
-        CK(upload(B.ids, h_ids, s));
         if (B.pos.n < sizeof(int32_t) * (size_t)std::max<int64_t>(vtotal, 1)) {
             CK(B.pos.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(vtotal, 1)));
             CK(cudaMemsetAsync(B.pos.p, 0xff, B.pos.n, s));
@@ -1167,12 +1200,8 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
-        P.deadline_ns = 0;
-        if (c->cfg.time_limit_ms > 0) {
-            unsigned long long now = 0;
-            CK(read_globaltimer(s, c->ctl.as<Control>(), &now));
-            P.deadline_ns = now + (unsigned long long)c->cfg.time_limit_ms * 1000000ull;
-        }
+        P.time_limit_ns = c->cfg.time_limit_ms > 0
+                              ? (unsigned long long)c->cfg.time_limit_ms * 1000000ull : 0ull;
         CK(cudaEventRecord(c->ev[1], s));
         expand_kernel<<<blocks, wpb * 32, sh.smem_bytes, s>>>(P);
         CK(cudaGetLastError());

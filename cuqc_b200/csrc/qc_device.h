@@ -62,6 +62,7 @@ struct Control {
     unsigned long long parent_vertices, p_rows, child_vertices;
     int max_task;
     int active_warps;              // warps still inside the work loop
+    unsigned long long t_start;    // globaltimer at the launch's start (0 until a warp sets it)
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
     unsigned long long check_site;      // first failed self-check: site id
     unsigned long long check_value;     //   ... and the offending value
@@ -169,7 +170,9 @@ struct ExpandParams {
     int32_t split;       // branches per work item before splitting
     int32_t small_path;  // 1: tasks of <= 32 vertices use the register path
     int64_t wait_ns;     // give up a wait after this long without progress
-    unsigned long long deadline_ns; // globaltimer value to stop at (0: none)
+    unsigned long long time_limit_ns; // stop this long after the launch began (0: none); the
+                                      // start is the first warp's globaltimer read, kept in
+                                      // Control::t_start, so a replayed launch times itself
 };
 
 // Work counters a warp accumulates privately and adds to the control block
@@ -220,6 +223,7 @@ struct WarpSmem {
     int32_t ebuf[kEmitInts];       // buffered sets, [k, ids..] each
     int32_t eset[kEmitSets];       // start of each buffered set in ebuf
     int32_t en, es;                // ints and sets buffered
+    unsigned long long deadline;   // globaltimer value to stop at (0: none)
 };
 
 // Per-warp workspace (global memory) for the bit-matrix path, tasks of up

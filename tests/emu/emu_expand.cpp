@@ -28,9 +28,9 @@ static StackEntry one_entry(unsigned long long rec)
     e.q_hi = -1;
     return e;
 }
-static unsigned long long emu_deadline()
+static unsigned long long emu_time_limit_ns()
 {
-    return g_emu_time_limit_ms > 0 ? emu_globaltimer() + (unsigned long long)g_emu_time_limit_ms * 1000000ull : 0ull;
+    return g_emu_time_limit_ms > 0 ? (unsigned long long)g_emu_time_limit_ms * 1000000ull : 0ull;
 }
 
 extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
@@ -128,7 +128,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     P.split = split;
     P.small_path = small_path;
     P.wait_ns = 20000000000ll;
-    P.deadline_ns = emu_deadline();
+    P.time_limit_ns = emu_time_limit_ns();
     // stage tasks of up to 96 vertices in (emulated) shared memory, as the
     // library does with its per-SM budget, so both task paths run here
     P.smem_t = t > 32 ? std::min(t, 96) : 0;
@@ -268,7 +268,7 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     P.split = split;
     P.small_path = 1;
     P.wait_ns = 20000000000ll;
-    P.deadline_ns = emu_deadline();
+    P.time_limit_ns = emu_time_limit_ns();
     P.smem_t = max_t > 32 ? std::min(max_t, 96) : 0;
     if (!items.empty())
         emu_launch(1, warps * 32, [&] { expand_kernel(P); }, expand_smem_bytes(warps, P.smem_t));

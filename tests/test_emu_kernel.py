@@ -21,6 +21,11 @@ CASES = [  # (n, p, seed, planted, size, gamma, min_size, warps, split); n > 32 
     (26, 0.3, 6, 1, 10, 0.75, 6, 2, 4),
     (44, 0.18, 7, 2, 12, 0.8, 6, 2, 3),
     (40, 0.22, 8, 1, 14, 0.9, 7, 2, 4),
+    # roots of 35-47 vertices: branches of tasks over 32 vertices that shrink
+    # to 32 or fewer members and candidates finish on the register path
+    (60, 0.12, 21, 2, 20, 0.9, 10, 3, 1),
+    (90, 0.08, 24, 3, 16, 0.9, 8, 2, 2),
+    (64, 0.2, 25, 1, 24, 0.95, 12, 2, 1),
 ]
 
 

@@ -69,3 +69,74 @@ def test_reference_arm_works_on_rank_zero_only(monkeypatch, capsys):
 
     assert bench.run_reference(Args()) is None
     assert capsys.readouterr().out == ""
+
+
+def _replica_rank(rank, world, port, q):
+    """One rank of the replica job with the GPU call replaced by a host stub:
+    each rank mines its own copy of the instance on its own device index."""
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      LOCAL_RANK=str(rank), WORLD_SIZE=str(world))
+    import torch.distributed as dist
+
+    import bench as b
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    dev = b.replica_device()
+    calls = []
+
+    def step():  # stand-in for one qc_mine on GPU `dev`: result and device ms
+        calls.append(dev)
+        return ("sets of instance", dev), 2.0 + rank  # rank 1 is slower
+
+    rate, slowest, outs = b.replica_rate(3, 5, step, lambda r: r == ("sets of instance", dev),
+                                         dist.barrier, dist, None)
+    bad = None
+    try:
+        b.replica_rate(0, 1, lambda: (("other", dev), 1.0), lambda r: r[0] == "sets of instance",
+                       dist.barrier, dist, None)
+    except SystemExit as e:
+        bad = str(e)
+    q.put((rank, dev, len(calls), rate, slowest, len(outs), bad))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_dispatch_on_two_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_replica_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, dev, ncalls, rate, slowest, nout, bad in out:
+        assert dev == rank                       # rank i mines on GPU i
+        assert ncalls == 3 + 5 and nout == 5     # warm-up steps untimed, 5 timed
+        assert slowest == 5 * 3.0                # the slower rank's 5 steps of 3 ms
+        assert abs(rate - 2 * 5 / 0.015) < 1e-9  # both ranks' steps over that time
+        assert bad is not None and "differs" in bad
+
+
+def test_gpus_flag_without_launcher_spawns_ranks(monkeypatch):
+    seen = {}
+
+    def fake_call(cmd):
+        seen["cmd"] = cmd
+        return 0
+
+    monkeypatch.setattr(bench.subprocess, "call", fake_call)
+    monkeypatch.setattr(bench.sys, "argv", ["bench.py", "--gpus", "4", "--steps", "2"])
+
+    class Args:
+        gpus = 4
+
+    assert bench.spawn_ranks(Args()) == 0
+    cmd = seen["cmd"]
+    assert cmd[1:4] == ["-m", "torch.distributed.run", "--nnodes=1"]
+    assert cmd[cmd.index("--nproc-per-node") + 1] == "4"
+    assert cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
+    assert cmd[-4:] == ["--gpus", "4", "--steps", "2"]
