@@ -38,7 +38,7 @@ EXPORTS = [
     "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
     "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune", "qc_maximal_sets",
-    "qc_context_last_stats",
+    "qc_context_last_stats", "qc_root", "qc_mine_shard",
 ]
 
 
@@ -63,7 +63,7 @@ class Stats(C.Structure):
                     "tasks", "branches", "children", "emitted", "emitted_ints", "maximal",
                     "root_size", "max_task", "arena_peak", "kernel_launches")] + [
                     ("kernel_ms", C.c_double)] + [(k, C.c_int64) for k in (
-                    "parent_vertices", "p_rows", "child_vertices")]
+                    "parent_vertices", "p_rows", "child_vertices", "level0_on_device")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -127,6 +127,9 @@ def lib():
         L.qc_twohop_noalloc_max_vertices.restype = C.c_int32
         L.qc_maximal_sets.argtypes = [vp, P32, C.c_int64, C.c_int32, C.POINTER(vp)]
         L.qc_context_last_stats.argtypes = [vp, C.POINTER(Stats)]
+        L.qc_root.argtypes = [vp, vp, C.c_double, C.c_int32, P32, C.c_int64, P32, P32]
+        L.qc_mine_shard.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                    C.POINTER(vp)]
         _lib = L
     return _lib
 
@@ -293,6 +296,28 @@ class Context:
             if e.status != 8:
                 raise
             return None, self.last_stats(), False
+
+    def root(self, g, gamma, min_size):
+        """Level 0 alone (qc_root): the root task's vertex ids in branching
+        order and the number of them the cover vertex covers."""
+        dg = g if isinstance(g, DeviceGraph) else DeviceGraph.from_graph(g)
+        t, cov = C.c_int32(), C.c_int32()
+        L = lib()
+        _check(L.qc_root(self.h, dg.h, float(gamma), int(min_size), None, 0, C.byref(t),
+                         C.byref(cov)))
+        ids = np.zeros(max(t.value, 1), np.int32)
+        _check(L.qc_root(self.h, dg.h, float(gamma), int(min_size), _p32(ids), len(ids),
+                         C.byref(t), C.byref(cov)))
+        return ids[: t.value].copy(), cov.value
+
+    def mine_shard(self, g, gamma, min_size, shard, nshards):
+        """Shard `shard` of `nshards` of a search split by the root's branches
+        (qc_mine_shard): the maximal sets among the sets its branches emit."""
+        dg = g if isinstance(g, DeviceGraph) else DeviceGraph.from_graph(g)
+        r = C.c_void_p()
+        _check(lib().qc_mine_shard(self.h, dg.h, float(gamma), int(min_size), int(shard),
+                                   int(nshards), C.byref(r)))
+        return self._result(r)
 
     def tune(self, g, gamma, min_size, repeats=2):
         """Pick the fastest launch shape for this device on (g, gamma,

@@ -54,7 +54,7 @@ int main(int argc, char* argv[])
     auto t_load = clk::now();
     std::cout << ">:PRE-PROCESSING" << std::endl;
     qc_graph* g = nullptr;
-    qc_status st = qc_graph_read_serialized(argv[1], &g);
+    qc_status st = qc_graph_read(argv[1], &g); // serialized text, or binary CSR
     if (st != QC_OK) {
         std::cout << qc_status_str(st) << ": " << qc_last_error() << std::endl;
         return st == QC_ERR_IO ? 1 : -1;

@@ -1147,6 +1147,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
         h->refs = 1;
         h->cls = cls;
         h->inst = T.inst;
+        h->shard_root = 0;
     }
     int32_t* cid = (int32_t*)(rec + rec_ids_off());
     int32_t* cl2 = (int32_t*)(rec + rec_l2_off(tc));
@@ -1613,6 +1614,7 @@ __device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const
         h->refs = 1;
         h->cls = cls;
         h->inst = T.inst;
+        h->shard_root = 0;
     }
     if (lane < tc) {
         ((int32_t*)(rec + rec_ids_off()))[lane] = sid;
@@ -1770,7 +1772,7 @@ constexpr int kSmallSplitMax = 16;
 // task runs its branches only.  Returns true when this call pushed branch
 // ranges of the record, which is then shared.
 __device__ bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V,
-                              int q_lo, int q_hi)
+                              int q_lo, int q_hi, bool sroot)
 {
     int lane = lane_id();
     SmallTask T;
@@ -1807,7 +1809,7 @@ __device__ bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
             bool bad = in_set(Cm, lane) && (T.l2 < nc - 1 || in + ex < need_t);
             if (!__any_sync(QC_FULL, bad)) {
                 if (lane == 0) ws.sm->cnt.lookahead_hits++;
-                emit_small(P, R, ws, low_mask(t), T.id);
+                if (!sroot || P.shard == 0) emit_small(P, R, ws, low_mask(t), T.id);
                 return false;
             }
         }
@@ -1864,6 +1866,8 @@ __device__ bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
         T.idr += (j < t && o > T.id) ? 1 : 0;
     }
     for (int q = qhi; q >= qlo; q--) {
+        // a sharded search's root: only this shard's branches
+        if (sroot && (t - 1 - q) % P.nshards != P.shard) continue;
         branch_small(P, R, ws, T, q);
         // children of this task can go to waiting warps before its last branch
         // when many warps wait (not for the odd one that will soon get work)
@@ -1922,8 +1926,11 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         return shared;
     }
     int q_lo = it.q_lo, q_hi = it.q_hi;
+    // the root of a search split by its branches: this launch expands only the
+    // branches of its own shard (and emits an accepted root in shard 0 only)
+    const bool sroot = hv.shard_root != 0 && P.nshards > 1;
     if (t <= 32 && P.small_path) {
-        if (process_small(P, R, ws, T, q_lo, q_hi)) shared = true;
+        if (process_small(P, R, ws, T, q_lo, q_hi, sroot)) shared = true;
         return shared;
     }
     if (q_lo < 0) {
@@ -1964,7 +1971,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
                 uint32_t* all = ws.mk(MK_T);
                 bs_range(all, W, 0, t);
                 if (lane == 0) ws.sm->cnt.lookahead_hits++;
-                emit_mask(P, R, T, all, t);
+                if (!sroot || P.shard == 0) emit_mask(P, R, T, all, t);
                 return shared;
             }
         }
@@ -2019,11 +2026,13 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     // here, summed after the branches
     long long rows = 0;
     for (int q = q_lo + lane; q <= q_hi; q += 32) {
+        if (sroot && (t - 1 - q) % P.nshards != P.shard) continue;
         const int pid = rec_ld(T.ids + q);
         if (pid >= 0 && pid < R.n)
             rows += (R.off[pid + 1] - R.off[pid]) + (R.off2[pid + 1] - R.off2[pid]);
     }
     for (int q = q_hi; q >= q_lo; q--) {
+        if (sroot && (t - 1 - q) % P.nshards != P.shard) continue;
         int stop = 0;
         if (lane == 0) stop = *(volatile int*)&P.ctl->status;
         if (__shfl_sync(QC_FULL, stop, 0)) break;
@@ -2059,6 +2068,7 @@ __device__ bool item_ok(const ExpandParams& P, const WorkItem& it, TaskHdr& hv)
         hv.W = W;
         hv.m = m;
         hv.inst = inst;
+        hv.shard_root = h->shard_root;
         hv.cov = cov;
         hv.cls = cls;
         hv.refs = refs;
@@ -2176,6 +2186,7 @@ __global__ void expand_kernel(ExpandParams P)
         hv.cov = __shfl_sync(QC_FULL, hv.cov, 0);
         hv.W = __shfl_sync(QC_FULL, hv.W, 0);
         hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
+        hv.shard_root = __shfl_sync(QC_FULL, hv.shard_root, 0);
         // idle warps and run status, read now and looked at while the next
         // item is taken and run, so the reads overlap this item's work
         int idle_now = 0, stat_now = 0;

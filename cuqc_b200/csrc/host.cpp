@@ -121,6 +121,85 @@ std::string write_serialized(const HostGraph& g, const char* path)
     return "";
 }
 
+bool is_binary_graph(const char* path)
+{
+    FILE* f = fopen(path, "rb");
+    if (!f) return false;
+    char m[8] = {0};
+    const bool ok = fread(m, 1, 8, f) == 8 && memcmp(m, kBinaryMagic, 8) == 0;
+    fclose(f);
+    return ok;
+}
+
+std::string read_binary(const char* path, HostGraph& g, bool& has_twohop)
+{
+    FILE* f = fopen(path, "rb");
+    if (!f) return std::string("cannot open graph file ") + path;
+    fseek(f, 0, SEEK_END);
+    const int64_t size = (int64_t)ftell(f);
+    fseek(f, 0, SEEK_SET);
+    char m[8];
+    int64_t hdr[3];
+    if (fread(m, 1, 8, f) != 8 || memcmp(m, kBinaryMagic, 8) != 0 || fread(hdr, 8, 3, f) != 3) {
+        fclose(f);
+        return "not a binary CSR graph file";
+    }
+    const int64_t n = hdr[0], nnz = hdr[1], nnz2 = hdr[2];
+    if (n < 0 || n > INT32_MAX || nnz < 0 || nnz2 < -1) {
+        fclose(f);
+        return "bad header values";
+    }
+    const int64_t pad = (8 - (nnz * 4) % 8) % 8;
+    const int64_t want = 32 + 8 * (n + 1) + 4 * nnz + pad +
+                         (nnz2 >= 0 ? 8 * (n + 1) + 4 * nnz2 : 0);
+    if (size != want) {
+        fclose(f);
+        return "file size " + std::to_string(size) + " does not match its header (" +
+               std::to_string(want) + " bytes expected)";
+    }
+    g.n = (int32_t)n;
+    g.off.resize((size_t)n + 1);
+    g.adj.resize((size_t)nnz);
+    bool ok = fread(g.off.data(), 8, (size_t)n + 1, f) == (size_t)n + 1 &&
+              fread(g.adj.data(), 4, (size_t)nnz, f) == (size_t)nnz;
+    if (ok && pad) {
+        char z[8];
+        ok = fread(z, 1, (size_t)pad, f) == (size_t)pad;
+    }
+    has_twohop = nnz2 >= 0;
+    g.off2.clear();
+    g.adj2.clear();
+    if (ok && has_twohop) {
+        g.off2.resize((size_t)n + 1);
+        g.adj2.resize((size_t)nnz2);
+        ok = fread(g.off2.data(), 8, (size_t)n + 1, f) == (size_t)n + 1 &&
+             fread(g.adj2.data(), 4, (size_t)nnz2, f) == (size_t)nnz2;
+    }
+    fclose(f);
+    if (!ok) return "short read on graph file";
+    return "";
+}
+
+std::string write_binary(const HostGraph& g, const char* path)
+{
+    FILE* f = fopen(path, "wb");
+    if (!f) return std::string("cannot open ") + path + " for writing";
+    const bool two = g.off2.size() == g.off.size();
+    const int64_t hdr[3] = {(int64_t)g.n, (int64_t)g.adj.size(),
+                            two ? (int64_t)g.adj2.size() : -1};
+    const int64_t pad = (8 - ((int64_t)g.adj.size() * 4) % 8) % 8;
+    const char z[8] = {0};
+    bool ok = fwrite(kBinaryMagic, 1, 8, f) == 8 && fwrite(hdr, 8, 3, f) == 3 &&
+              fwrite(g.off.data(), 8, g.off.size(), f) == g.off.size() &&
+              fwrite(g.adj.data(), 4, g.adj.size(), f) == g.adj.size() &&
+              (pad == 0 || fwrite(z, 1, (size_t)pad, f) == (size_t)pad);
+    if (ok && two)
+        ok = fwrite(g.off2.data(), 8, g.off2.size(), f) == g.off2.size() &&
+             fwrite(g.adj2.data(), 4, g.adj2.size(), f) == g.adj2.size();
+    ok = (fclose(f) == 0) && ok;
+    return ok ? "" : std::string("short write on ") + path;
+}
+
 // Rows of ids: every row strictly ascending (sorted, no duplicates) with its
 // ids in [0, n), checked with branch-free passes the compiler vectorises (a
 // row's ids are in range when its first and last are); the exact message is

@@ -20,6 +20,16 @@ struct HostGraph {
 // success, else a message.
 std::string read_serialized(const char* path, HostGraph& g);
 std::string write_serialized(const HostGraph& g, const char* path);
+
+// Binary CSR file, for graphs too large for the text format to load quickly:
+// 8 bytes "QCSRBIN1", then little-endian int64 n, nnz (= 2|E|) and nnz2 (the
+// two-hop entries; -1 when the file holds no two-hop lists), then int64
+// off[n+1], int32 adj[nnz], zero padding to a multiple of 8 bytes, and, when
+// nnz2 >= 0, int64 off2[n+1] and int32 adj2[nnz2].
+constexpr char kBinaryMagic[8] = {'Q', 'C', 'S', 'R', 'B', 'I', 'N', '1'};
+bool is_binary_graph(const char* path);
+std::string read_binary(const char* path, HostGraph& g, bool& has_twohop);
+std::string write_binary(const HostGraph& g, const char* path);
 // Structural checks the kernels rely on: offsets monotone, ids in range,
 // rows sorted and duplicate-free, no self loops, symmetric 1-hop rows.
 std::string validate(const HostGraph& g, bool need_twohop);

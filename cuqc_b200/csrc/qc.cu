@@ -26,6 +26,7 @@
 #include "../../include/qc.h"
 #include "expand_kernel.cuh"
 #include "level0_kernel.cuh"
+#include "level0_grid.cuh"
 #include "filter.h"
 #include "host.h"
 
@@ -170,6 +171,8 @@ extern "C" void qc_config_default(qc_config* c)
     c->wait_limit_ms = 10000;
 }
 
+static qc_status warm_kernels(qc_context* c);
+
 extern "C" qc_status qc_context_create(const qc_config* cfg, qc_context** out)
 {
     if (!out) return fail(QC_ERR_ARGS, "out is NULL");
@@ -192,6 +195,8 @@ extern "C" qc_status qc_context_create(const qc_config* cfg, qc_context** out)
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
     c->res_budget = total_b / 4;
+    qc_status ws = warm_kernels(c.get());
+    if (ws != QC_OK) return ws;
     *out = c.release();
     return QC_OK;
 }
@@ -257,6 +262,46 @@ extern "C" qc_status qc_graph_from_csr2(int32_t n, const int64_t* off, const int
     if (!e.empty()) return fail(QC_ERR_FORMAT, e);
     *out = g.release();
     return QC_OK;
+}
+
+std::string qcb_twohop_device(const HostGraph& h, std::vector<int64_t>& off2,
+                              std::vector<int32_t>& adj2);
+
+extern "C" qc_status qc_graph_read_binary(const char* path, qc_graph** out)
+{
+    if (!path || !out) return fail(QC_ERR_ARGS, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<qc_graph> g(new qc_graph());
+    bool two = false;
+    std::string e = read_binary(path, g->h, two);
+    if (!e.empty()) {
+        if (e.rfind("cannot open", 0) == 0) return fail(QC_ERR_IO, e);
+        return fail(QC_ERR_FORMAT, e);
+    }
+    e = validate(g->h, two);
+    if (!e.empty()) return fail(QC_ERR_FORMAT, e);
+    if (!two) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return fail(QC_ERR_NO_DEVICE, "no CUDA device to build the two-hop lists");
+        e = qcb_twohop_device(g->h, g->h.off2, g->h.adj2);
+        if (!e.empty()) return fail(QC_ERR_CUDA, e);
+    }
+    *out = g.release();
+    return QC_OK;
+}
+
+extern "C" qc_status qc_graph_write_binary(const qc_graph* g, const char* path)
+{
+    if (!g || !path) return fail(QC_ERR_ARGS, "NULL argument");
+    std::string e = write_binary(g->h, path);
+    return e.empty() ? QC_OK : fail(QC_ERR_IO, e);
+}
+
+extern "C" qc_status qc_graph_read(const char* path, qc_graph** out)
+{
+    if (path && is_binary_graph(path)) return qc_graph_read_binary(path, out);
+    return qc_graph_read_serialized(path, out);
 }
 
 extern "C" qc_status qc_graph_write_serialized(const qc_graph* g, const char* path)
@@ -486,30 +531,21 @@ static void record_last(qc_context* c, const Control& ctl, float kms, int root_s
     l.child_vertices = (int64_t)ctl.child_vertices;
 }
 
-static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
-                          qc_result* r)
+// Level 0 of graph h (resident as rg): the root task's vertex ids in Q order
+// land in c->ids on the device; t = root size, cov = covered count.  On the
+// device for graphs of up to kLevel0DeviceMax vertices (one block) and up to
+// kLevel0GridMax (the whole grid, one cooperative launch); on the host above.
+// *on_device tells which.
+static qc_status compute_root(qc_context* c, const HostGraph& h, ResidentGraph* rg,
+                              const std::vector<int32_t>& md, int32_t min_size, int& t, int& cov,
+                              bool* on_device)
 {
-    auto t_all = clk::now();
-    const HostGraph& h = g->h;
     cudaStream_t s = c->stream;
-    CK(cudaSetDevice(c->cfg.device));
-
-    // graph -> device (timed as load; skipped when already resident)
-    auto t_load = clk::now();
-    ResidentGraph* rg = nullptr;
-    {
-        qc_status us = make_resident(c, g, nullptr, &rg);
-        if (us != QC_OK) return us;
-    }
-    r->st.load_ms = ms_since(t_load);
-
-    // enumeration: level 0 + device expansion
-    auto t_enum = clk::now();
-    std::vector<int32_t> md, ubt;
-    gamma_tables(gamma, h.n, min_size, md, ubt);
     std::vector<int32_t> ids;
-    int cov = 0, t = 0;
+    t = 0;
+    cov = 0;
     const bool l0_dev = h.n > 0 && h.n <= kLevel0DeviceMax;
+    const bool l0_grid = h.n > kLevel0DeviceMax && (int64_t)h.n <= kLevel0GridMax;
     if (l0_dev) {
         // root ids straight into c->ids; only the root size and the covered
         // count come back
@@ -535,10 +571,71 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         t = hinfo[0];
         cov = hinfo[1];
         if (t < 0 || t > h.n || cov < 0 || cov > t) return fail(QC_ERR_CUDA, "level 0 size out of range");
+    } else if (l0_grid) {
+        // above one block's reach: the whole grid in one cooperative launch
+        const size_t sb = (size_t)level0_grid_scratch_bytes(h.n);
+        CK(c->lvl0.ensure(sb + 16));
+        CK(c->ids.ensure(std::max<size_t>((size_t)h.n * 4, 16)));
+        char* z = c->lvl0.as<char>();
+        int32_t* info = (int32_t*)(z + sb);
+        CK(cudaMemsetAsync(z + sb - 64, 0, 64, s)); // round flags, cover key, counts
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level0_grid_kernel, 256, 0));
+        if (per_sm < 1) return fail(QC_ERR_CUDA, "level 0 grid kernel cannot be resident");
+        const int64_t* a_off = rg->off.as<int64_t>();
+        const int32_t* a_adj = rg->adj.as<int32_t>();
+        const int64_t* a_off2 = rg->off2.as<int64_t>();
+        int64_t a_n = h.n;
+        int a_need = md[(size_t)min_size], a_ms = min_size;
+        int32_t* a_ids = c->ids.as<int32_t>();
+        void* args[] = {(void*)&a_off, (void*)&a_adj, (void*)&a_off2, (void*)&a_n, (void*)&a_need,
+                        (void*)&a_ms, (void*)&z, (void*)&a_ids, (void*)&info};
+        CK(cudaLaunchCooperativeKernel((const void*)level0_grid_kernel, dim3(c->sms * per_sm),
+                                       dim3(256), args, 0, s));
+        c->launches += 1;
+        int32_t hinfo[2] = {0, 0};
+        CK(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        t = hinfo[0];
+        cov = hinfo[1];
+        if (t < 0 || t > h.n || cov < 0 || cov > t) return fail(QC_ERR_CUDA, "level 0 size out of range");
     } else {
         build_root(h, md.data(), min_size, ids, cov);
         t = (int)ids.size();
     }
+    if (!l0_dev && !l0_grid) CK(upload(c->ids, ids, s));
+    if (on_device) *on_device = l0_dev || l0_grid;
+    return QC_OK;
+}
+
+static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
+                          qc_result* r, int32_t shard = 0, int32_t nshards = 1)
+{
+    auto t_all = clk::now();
+    const HostGraph& h = g->h;
+    cudaStream_t s = c->stream;
+    CK(cudaSetDevice(c->cfg.device));
+
+    // graph -> device (timed as load; skipped when already resident)
+    auto t_load = clk::now();
+    ResidentGraph* rg = nullptr;
+    {
+        qc_status us = make_resident(c, g, nullptr, &rg);
+        if (us != QC_OK) return us;
+    }
+    r->st.load_ms = ms_since(t_load);
+
+    // enumeration: level 0 + device expansion
+    auto t_enum = clk::now();
+    std::vector<int32_t> md, ubt;
+    gamma_tables(gamma, h.n, min_size, md, ubt);
+    int cov = 0, t = 0;
+    bool l0_on_device = false;
+    {
+        qc_status ls = compute_root(c, h, rg, md, min_size, t, cov, &l0_on_device);
+        if (ls != QC_OK) return ls;
+    }
+    r->st.level0_on_device = l0_on_device ? 1 : 0;
     r->st.root_size = (int64_t)t;
     if (t == 0) {
         r->st.enum_ms = ms_since(t_enum);
@@ -548,7 +645,6 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     const int W = words_for(t);
     CK(upload(c->md, md, s));
     CK(upload(c->ubt, ubt, s));
-    if (!l0_dev) CK(upload(c->ids, ids, s));
 
     Shape sh;
     {
@@ -591,6 +687,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         hd.refs = 1;
         hd.cls = root_cls;
         hd.inst = 0;
+        hd.shard_root = nshards > 1 ? 1 : 0;
         CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(rec + rec_ids_off(), c->ids.p, sizeof(int32_t) * t,
                            cudaMemcpyDeviceToDevice, s));
@@ -652,6 +749,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.smem_t = sh.smem_t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
+        P.shard = shard;
+        P.nshards = nshards;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
         P.time_limit_ns = c->cfg.time_limit_ms > 0
                               ? (unsigned long long)c->cfg.time_limit_ms * 1000000ull : 0ull;
@@ -806,6 +905,28 @@ extern "C" qc_status qc_context_last_stats(const qc_context* c, qc_stats* out)
     return QC_OK;
 }
 
+// Load the mining path's kernels now, at context creation, by mining a
+// 6-vertex clique once: with lazy module loading each kernel would otherwise
+// be loaded at its first launch, inside the first mining call.
+static qc_status warm_kernels(qc_context* c)
+{
+    qc_graph* g = new qc_graph();
+    const int n = 6;
+    g->h.n = n;
+    for (int v = 0; v <= n; v++) g->h.off.push_back((int64_t)v * (n - 1));
+    for (int v = 0; v < n; v++)
+        for (int w = 0; w < n; w++)
+            if (w != v) g->h.adj.push_back(w);
+    g->h.off2 = g->h.off;
+    g->h.adj2 = g->h.adj;
+    qc_result r;
+    const int64_t launches = c->launches;
+    qc_status st = mine_one(c, g, 0.9, 3, &r);
+    qc_graph_free(g); // its device copy's buffers go to the next graph
+    c->launches = launches;
+    return st;
+}
+
 extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
                              int32_t sched, qc_result** out)
 {
@@ -820,6 +941,58 @@ extern "C" qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, i
     qc_status st = mine_one(ctx, g, gamma, min_size, r.get());
     if (st != QC_OK) return st;
     *out = r.release();
+    return QC_OK;
+}
+
+static qc_status check_mine_args(const qc_graph* g, double gamma, int32_t min_size)
+{
+    if (!(gamma >= 0.5 && gamma <= 1.0))
+        return fail(QC_ERR_ARGS, "minimum degree ratio must be between .5 and 1 inclusive");
+    if (min_size <= 1) return fail(QC_ERR_ARGS, "minimum size must be greater than 1");
+    if (g->h.off2.size() != g->h.off.size()) return fail(QC_ERR_FORMAT, "graph has no 2-hop lists");
+    return QC_OK;
+}
+
+extern "C" qc_status qc_mine_shard(qc_context* ctx, const qc_graph* g, double gamma,
+                                   int32_t min_size, int32_t shard, int32_t nshards,
+                                   qc_result** out)
+{
+    if (!ctx || !g || !out) return fail(QC_ERR_ARGS, "NULL argument");
+    *out = nullptr;
+    if (nshards < 1 || shard < 0 || shard >= nshards) return fail(QC_ERR_ARGS, "bad shard");
+    qc_status st = check_mine_args(g, gamma, min_size);
+    if (st != QC_OK) return st;
+    std::unique_ptr<qc_result> r(new qc_result());
+    st = mine_one(ctx, g, gamma, min_size, r.get(), shard, nshards);
+    if (st != QC_OK) return st;
+    *out = r.release();
+    return QC_OK;
+}
+
+extern "C" qc_status qc_root(qc_context* c, const qc_graph* g, double gamma, int32_t min_size,
+                             int32_t* ids_out, int64_t cap, int32_t* t_out, int32_t* cov_out)
+{
+    if (!c || !g || !t_out || !cov_out || cap < 0 || (cap > 0 && !ids_out))
+        return fail(QC_ERR_ARGS, "bad arguments");
+    qc_status st = check_mine_args(g, gamma, min_size);
+    if (st != QC_OK) return st;
+    CK(cudaSetDevice(c->cfg.device));
+    ResidentGraph* rg = nullptr;
+    st = make_resident(c, g, nullptr, &rg);
+    if (st != QC_OK) return st;
+    std::vector<int32_t> md, ubt;
+    gamma_tables(gamma, g->h.n, min_size, md, ubt);
+    int t = 0, cov = 0;
+    st = compute_root(c, g->h, rg, md, min_size, t, cov, nullptr);
+    if (st != QC_OK) return st;
+    const int64_t k = std::min<int64_t>(cap, t);
+    if (k > 0) {
+        CK(cudaMemcpyAsync(ids_out, c->ids.p, sizeof(int32_t) * (size_t)k, cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    *t_out = t;
+    *cov_out = cov;
     return QC_OK;
 }
 
@@ -916,7 +1089,7 @@ __global__ void batch_root_fill_kernel(const RootMeta* meta, int nroots, const i
         h->refs = 1;
         h->cls = M.cls;
         h->inst = M.inst;
-        h->pad = 0;
+        h->shard_root = 0;
     }
 }
 

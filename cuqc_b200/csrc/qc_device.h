@@ -100,7 +100,7 @@ struct TaskHdr {
     int32_t refs; // work items that still reference this record
     int32_t cls;  // arena size class of the record's block
     int32_t inst; // instance (batched runs) whose rules apply
-    int32_t pad;
+    int32_t shard_root; // 1: the root of a search split by its branches (see ExpandParams)
 };
 
 // Arena blocks come in size classes: four steps per power of two from
@@ -170,6 +170,8 @@ struct ExpandParams {
     int32_t split;       // branches per work item before splitting
     int32_t small_path;  // 1: tasks of <= 32 vertices use the register path
     int64_t wait_ns;     // give up a wait after this long without progress
+    int32_t shard;       // a search split by the root's branches: branch i of the root
+    int32_t nshards;     //   (counted from the first branched) belongs to shard i % nshards
     unsigned long long time_limit_ns; // stop this long after the launch began (0: none); the
                                       // start is the first warp's globaltimer read, kept in
                                       // Control::t_start, so a replayed launch times itself

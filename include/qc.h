@@ -98,6 +98,22 @@ qc_status qc_twohop_noalloc(int32_t n, const int64_t* d_off, const int32_t* d_ad
 /* Largest vertex count qc_twohop_noalloc accepts. */
 int32_t qc_twohop_noalloc_max_vertices(void);
 
+/* Binary CSR graph file, for graphs whose text form is slow to parse (the
+ * reference reads only the text format, main.cu:96-121):
+ *   8 bytes "QCSRBIN1"; little-endian int64 n, nnz (= 2|E|), nnz2 (two-hop
+ *   entries, -1 when the file has no two-hop lists); int64 off[n+1];
+ *   int32 adj[nnz]; zero padding to a multiple of 8 bytes; and when nnz2 >= 0,
+ *   int64 off2[n+1] and int32 adj2[nnz2].
+ * The file is checked like a serialized one (sizes against the header, sorted
+ * symmetric rows, ids in range).  Without two-hop lists they are built on the
+ * GPU as qc_graph_from_csr does. */
+qc_status qc_graph_read_binary(const char* path, qc_graph** out);
+/* Write the graph (with its two-hop lists) in the binary CSR format. */
+qc_status qc_graph_write_binary(const qc_graph* g, const char* path);
+/* Read a graph file of either format: binary CSR when the file starts with
+ * "QCSRBIN1", else the serialized text format. */
+qc_status qc_graph_read(const char* path, qc_graph** out);
+
 /* Write the graph in the serialized format (adjToSer.cpp:159-204). */
 qc_status qc_graph_write_serialized(const qc_graph* g, const char* path);
 
@@ -177,9 +193,32 @@ typedef struct {
     int64_t parent_vertices; /* sum over branches of the parent task size    */
     int64_t p_rows;          /* sum over branches of deg(p) + |N2(p)|        */
     int64_t child_vertices;  /* sum of child task sizes written              */
+    int64_t level0_on_device; /* 1: level 0 ran on the device, 0: on the host  */
 } qc_stats;
 
 typedef struct qc_result qc_result;
+
+/* Level 0 alone: the root task of the search for (g, gamma, min_size) --
+ * the vertices that pass the degree and two-hop tests and the peeling, in the
+ * order the search branches them, and how many of them the cover vertex
+ * covers.  Replaces initialize_tasks (main.cu:846-998).  ids_out receives the
+ * first min(cap, root size) ids; *t_out the root size, *cov_out the covered
+ * count.  Runs on the device up to 2^30 vertices. */
+qc_status qc_root(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                  int32_t* ids_out, int64_t cap, int32_t* t_out, int32_t* cov_out);
+
+/* One shard of a search split by the root's branches, so that several GPUs
+ * (one context each) can mine one graph.  The root's branches are dealt to
+ * `nshards` shards round-robin in branching order (the i-th branch taken, i
+ * from 0, belongs to shard i mod nshards); this call expands the branches of
+ * shard `shard` and everything below them, and returns the maximal sets among
+ * the sets they emitted.  The maximal sets of the whole graph are the maximal
+ * sets of the union of every shard's result: qc_maximal_sets merges them.  A
+ * root that the lookahead accepts whole is emitted by shard 0 only; every
+ * shard counts the root in its task counter.  No counterpart in the reference,
+ * which mines on one GPU (search, main.cu:535-692). */
+qc_status qc_mine_shard(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                        int32_t shard, int32_t nshards, qc_result** out);
 
 /* Work counters of the context's most recent expansion kernel (tasks,
  * branches, emitted sets, kernel_ms, the byte-model counters), also when

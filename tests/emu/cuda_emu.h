@@ -141,6 +141,10 @@ inline unsigned long long atomicAdd(unsigned long long* a, unsigned long long v)
 inline int atomicSub(int* a, int v) { return __atomic_fetch_sub(a, v, __ATOMIC_SEQ_CST); }
 inline int atomicOr(int* a, int v) { return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST); }
 inline unsigned atomicOr(unsigned* a, unsigned v) { return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST); }
+inline unsigned long long atomicOr(unsigned long long* a, unsigned long long v)
+{
+    return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST);
+}
 inline int atomicExch(int* a, int v) { return __atomic_exchange_n(a, v, __ATOMIC_SEQ_CST); }
 inline int atomicCAS(int* a, int cmp, int v)
 {

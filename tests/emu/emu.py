@@ -16,6 +16,7 @@ SRCS = [os.path.join(HERE, "emu_expand.cpp"), os.path.join(ROOT, "cuqc_b200", "c
 DEPS = SRCS + [os.path.join(HERE, "cuda_emu.h"),
                os.path.join(ROOT, "cuqc_b200", "csrc", "expand_kernel.cuh"),
                os.path.join(ROOT, "cuqc_b200", "csrc", "level0_kernel.cuh"),
+               os.path.join(ROOT, "cuqc_b200", "csrc", "level0_grid.cuh"),
                os.path.join(ROOT, "cuqc_b200", "csrc", "qc_device.h"),
                os.path.join(ROOT, "cuqc_b200", "csrc", "host.h")]
 
@@ -44,6 +45,8 @@ def lib():
         L.emu_free.argtypes = [C.c_void_p]
         L.emu_level0.argtypes = [C.c_int, P64, P32, P64, C.c_double, C.c_int, C.c_int, P32, P32]
         L.emu_level0.restype = C.c_int
+        L.emu_level0_grid.argtypes = L.emu_level0.argtypes
+        L.emu_level0_grid.restype = C.c_int
         _lib = L
     return _lib
 
@@ -113,16 +116,18 @@ def mine_batch(gs, gammas, min_sizes, warps=3, split=2):
     return per, st
 
 
-def level0(g, gamma, min_size, threads=64):
+def level0(g, gamma, min_size, threads=64, grid=False):
     """Root ids (Q order) and covered count from the product's device level 0
-    (level0_kernel.cuh) run as one emulated block."""
+    run as one emulated block: the one-block form (level0_kernel.cuh) or, with
+    grid=True, the grid-wide form (level0_grid.cuh) as a grid of one block."""
     L = lib()
     P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
     off, adj = np.ascontiguousarray(g.off, np.int64), np.ascontiguousarray(g.adj, np.int32)
     off2 = np.ascontiguousarray(g.off2, np.int64)
     ids = np.zeros(max(int(g.n), 1), np.int32)
     info = np.zeros(2, np.int32)
-    L.emu_level0(int(g.n), off.ctypes.data_as(P64), adj.ctypes.data_as(P32),
+    fn = L.emu_level0_grid if grid else L.emu_level0
+    fn(int(g.n), off.ctypes.data_as(P64), adj.ctypes.data_as(P32),
                  off2.ctypes.data_as(P64), float(gamma), int(min_size), int(threads),
                  ids.ctypes.data_as(P32), info.ctypes.data_as(P32))
     return ids[: int(info[0])].copy(), int(info[1])

@@ -8,6 +8,7 @@
 #include "../../cuqc_b200/csrc/expand_kernel.cuh"
 #include "../../cuqc_b200/csrc/host.h"
 #include "../../cuqc_b200/csrc/level0_kernel.cuh"
+#include "../../cuqc_b200/csrc/level0_grid.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -299,6 +300,22 @@ extern "C" int emu_level0(int n, const int64_t* off, const int32_t* adj, const i
     emu_launch(1, threads, [&] {
         level0_kernel(off, adj, off2, n, md[(size_t)min_size], min_size, exdeg.data(),
                       label.data(), l2.data(), keys.data(), ids_out, info);
+    });
+    return 0;
+}
+
+// The product's grid-wide level 0 (level0_grid.cuh) as a grid of one emulated
+// block of `threads` threads (its grid barriers become block barriers).
+extern "C" int emu_level0_grid(int n, const int64_t* off, const int32_t* adj, const int64_t* off2,
+                               double gamma, int min_size, int threads, int32_t* ids_out,
+                               int32_t* info)
+{
+    std::vector<int32_t> md, ubt;
+    gamma_tables(gamma, n, min_size, md, ubt);
+    std::vector<char> scratch((size_t)level0_grid_scratch_bytes(n), 0);
+    emu_launch(1, threads, [&] {
+        level0_grid_kernel(off, adj, off2, (int64_t)n, md[(size_t)min_size], min_size,
+                           scratch.data(), ids_out, info);
     });
     return 0;
 }

@@ -62,10 +62,12 @@ def test_emulated_batch_matches_oracle_per_instance():
         assert canon(got) == canon(want)
 
 
+@pytest.mark.parametrize("grid", [False, True])
 @pytest.mark.parametrize("seed", range(12))
-def test_emulated_device_level0_matches_oracle_root(seed):
-    """The product's device level 0 (one emulated block of 64 threads) gives the
-    oracle's root: same vertices in the same Q order, same covered count."""
+def test_emulated_device_level0_matches_oracle_root(seed, grid):
+    """The product's device level 0 (one emulated block of 64 threads; the
+    one-block form and the grid-wide form) gives the oracle's root: same
+    vertices in the same Q order, same covered count."""
     rng = np.random.default_rng(seed)
     n = int(rng.integers(20, 200))
     g = graphs.random_small(n, float(rng.uniform(0.03, 0.3)), 500 + seed,
@@ -74,6 +76,6 @@ def test_emulated_device_level0_matches_oracle_root(seed):
     gamma = [0.5, 0.6, 0.7, 0.8, 0.9, 1.0][seed % 6]
     ms = int(rng.integers(3, 9))
     want_ids, want_lab, _ = oracle.root(g, gamma, ms)
-    ids, cov = emu.level0(g, gamma, ms)
+    ids, cov = emu.level0(g, gamma, ms, grid=grid)
     assert ids.tolist() == want_ids.tolist()
     assert cov == int((want_lab == 2).sum())

@@ -65,13 +65,13 @@ def test_random_graphs(ctx, seed):
         assert res.stats[k] == st[k], k
 
 
-def test_level0_on_the_host_above_the_device_limit(ctx):
-    # 70,000 vertices: level 0 runs on the host (the device form takes graphs
-    # of at most 65,536); sparse background, two planted groups survive
+@pytest.mark.parametrize("n", [70000, 200000])
+def test_level0_grid_above_the_block_limit(ctx, n):
+    # above 65,536 vertices level 0 runs over the whole grid (one cooperative
+    # launch, level0_grid.cuh); sparse background, planted groups survive
     rng = np.random.default_rng(21)
-    n = 70000
     src, dst = rng.integers(0, n, 3 * n), rng.integers(0, n, 3 * n)  # mean degree ~6
-    groups = [rng.choice(n, 15, replace=False) for _ in range(2)]
+    groups = [rng.choice(n, 15, replace=False) for _ in range(2 if n < 100000 else 6)]
     for grp in groups:
         iu, ju = np.triu_indices(15, 1)
         keep = rng.random(len(iu)) < 0.95

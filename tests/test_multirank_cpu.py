@@ -140,3 +140,62 @@ def test_gpus_flag_without_launcher_spawns_ranks(monkeypatch):
     assert cmd[cmd.index("--nproc-per-node") + 1] == "4"
     assert cmd[cmd.index("--master-addr") + 1] == "127.0.0.1"
     assert cmd[-4:] == ["--gpus", "4", "--steps", "2"]
+
+
+def _shard_rank(rank, world, port, q):
+    """One rank of a graph mined in shards, with the GPU calls replaced by host
+    stand-ins: a shard's result is its share of a known family of sets, the
+    merge is the oracle's maximal-set filter."""
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    import numpy as np
+    import torch.distributed as dist
+
+    from cuqc_b200 import shard
+    from oracle import oracle
+
+    fam = [(0, 1, 2), (0, 1), (3, 4, 5, 6), (1, 2), (4, 5), (7,), (0, 1, 2), (6, 7, 8)]
+
+    def pack(sets):
+        out = []
+        for s in sets:
+            out += [len(s)] + list(s)
+        return np.asarray(out, np.int32)
+
+    class FakeResult:
+        def __init__(self, flat):
+            self.flat = flat
+            self.sets = oracle.maximal(flat)
+
+    class FakeCtx:
+        def mine_shard(self, g, gamma, ms, s, n):
+            assert (s, n) == (rank, world)
+            return FakeResult(pack(fam[s::n]))
+
+        def maximal_sets(self, flat, nv):
+            return FakeResult(flat)
+
+    class G:
+        n = 9
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    r = shard.mine_sharded(FakeCtx(), G(), 0.9, 2, dist, None)
+    q.put((rank, r.sets, oracle.maximal(pack(fam))))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_merge_on_two_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, got, want in out:
+        assert got == want == [(0, 1, 2), (3, 4, 5, 6), (6, 7, 8)]
