@@ -38,7 +38,8 @@ EXPORTS = [
     "qc_context_create", "qc_context_free", "qc_context_upload", "qc_context_stream", "qc_mine", "qc_mine_batch", "qc_result_count",
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
     "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune", "qc_maximal_sets",
-    "qc_context_last_stats", "qc_root", "qc_mine_shard",
+    "qc_context_last_stats", "qc_root", "qc_mine_shard", "qc_graph_read_binary",
+    "qc_graph_write_binary", "qc_graph_read",
 ]
 
 
@@ -128,6 +129,9 @@ def lib():
         L.qc_maximal_sets.argtypes = [vp, P32, C.c_int64, C.c_int32, C.POINTER(vp)]
         L.qc_context_last_stats.argtypes = [vp, C.POINTER(Stats)]
         L.qc_root.argtypes = [vp, vp, C.c_double, C.c_int32, P32, C.c_int64, P32, P32]
+        L.qc_graph_read_binary.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.qc_graph_write_binary.argtypes = [vp, C.c_char_p]
+        L.qc_graph_read.argtypes = [C.c_char_p, C.POINTER(vp)]
         L.qc_mine_shard.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.c_int32,
                                     C.POINTER(vp)]
         _lib = L
@@ -170,9 +174,14 @@ class DeviceGraph:
 
     @classmethod
     def read(cls, path):
+        """A graph file of either format: binary CSR (starts with "QCSRBIN1")
+        or the serialized text."""
         h = C.c_void_p()
-        _check(lib().qc_graph_read_serialized(path.encode(), C.byref(h)))
+        _check(lib().qc_graph_read(path.encode(), C.byref(h)))
         return cls(h)
+
+    def write_binary(self, path):
+        _check(lib().qc_graph_write_binary(self.h, path.encode()))
 
     def to_graph(self) -> graphs.Graph:
         L = lib()

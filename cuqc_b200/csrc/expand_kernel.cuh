@@ -27,6 +27,16 @@ namespace qcb {
 
 #define QC_FULL 0xffffffffu
 
+// Inlining of the large-task path's and the register path's routines, left to
+// the compiler unless a build sets these (__noinline__ keeps one copy of a
+// routine that several call sites share, which shrinks the kernel's code).
+#ifndef QC_BIG_FN
+#define QC_BIG_FN
+#endif
+#ifndef QC_SMALL_FN
+#define QC_SMALL_FN
+#endif
+
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
 __device__ __forceinline__ int wsum(int x)
@@ -171,7 +181,7 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
 
 // Copy a record's body (ids, l2, A1, A2) into this warp's shared-memory
 // buffer with 16-byte loads through L2 and point the view there.
-__device__ void stage_record(const ExpandParams& P, TaskView& T, char* buf)
+__device__ QC_BIG_FN void stage_record(const ExpandParams& P, TaskView& T, char* buf)
 {
     const char* src = P.arena + T.rec + rec_ids_off();
     const uint64_t body = rec_bytes(T.t, T.W) - rec_ids_off(); // multiple of 16
@@ -240,11 +250,23 @@ struct Bounds {
 // gamma tables (main.cu:526-533, 2144-2151)
 // ------------------------------------------------------------------
 
-__device__ __forceinline__ int md_at(const Rules& R, int k)
+// The shared-memory copies hold entries [0, kTabCache), padded past the
+// table's end with its last entry, so an index in that range needs no clamp.
+__device__ __noinline__ int md_far(const Rules& R, int k)
 {
     k = k < 0 ? 0 : k;
     k = k >= R.mdlen ? R.mdlen - 1 : k;
-    return k < kTabCache ? R.md_s[k] : __ldg(R.md + k);
+    return __ldg(R.md + k);
+}
+__device__ __noinline__ int ubt_far(const Rules& R, int d)
+{
+    d = d < 0 ? 0 : d;
+    d = d >= R.mdlen ? R.mdlen - 1 : d;
+    return __ldg(R.ubt + d);
+}
+__device__ __forceinline__ int md_at(const Rules& R, int k)
+{
+    return (unsigned)k < (unsigned)kTabCache ? R.md_s[k] : md_far(R, k);
 }
 __device__ __forceinline__ int mindeg(const Rules& R, int k)
 {
@@ -252,9 +274,7 @@ __device__ __forceinline__ int mindeg(const Rules& R, int k)
 }
 __device__ __forceinline__ int ubt_at(const Rules& R, int d)
 {
-    d = d < 0 ? 0 : d;
-    d = d >= R.mdlen ? R.mdlen - 1 : d;
-    return d < kTabCache ? R.ubt_s[d] : __ldg(R.ubt + d);
+    return (unsigned)d < (unsigned)kTabCache ? R.ubt_s[d] : ubt_far(R, d);
 }
 
 // main.cu:2167-2178
@@ -291,7 +311,7 @@ __device__ __forceinline__ bool vert_extendable(const Rules& R, int in, int ex, 
 // only those passing validity under `b`), then prefix tables over bins in
 // descending value order: pcnt[j] = #values > vmax-j, psum[j] = their sum.
 // Values are bounded by vmax (members count).  Returns the number of values.
-__device__ int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* cm, int t, int vmax,
+__device__ QC_BIG_FN int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* cm, int t, int vmax,
                           bool filter_valid, int m, const Bounds& b)
 {
     int lane = lane_id();
@@ -300,14 +320,18 @@ __device__ int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const u
     int cnt = 0;
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
+        int j = -1;
         if (v < t && bit(cm, v)) {
             int in = ws.indeg()[v];
             if (!filter_valid || cand_valid(R, in, ws.exdeg()[v], m, b)) {
-                int j = vmax - (in > vmax ? vmax : (in < 0 ? 0 : in));
-                atomicAdd(&ws.hist()[j], 1);
+                j = vmax - (in > vmax ? vmax : (in < 0 ? 0 : in));
                 cnt++;
             }
         }
+        // one shared-memory add per distinct bin of the 32 lanes (many lanes
+        // share a degree, and their adds would otherwise queue on one word)
+        const unsigned peers = __match_any_sync(QC_FULL, j);
+        if (j >= 0 && (peers & ((1u << lane) - 1u)) == 0) atomicAdd(&ws.hist()[j], __popc(peers));
     }
     __syncwarp();
     // exclusive prefix over bins 0..vmax+1
@@ -349,7 +373,7 @@ __device__ __forceinline__ long long top_sum(const Ws& ws, int vmax, int k)
 // The candidate histogram must be built.  Returns true when invalid.
 // ------------------------------------------------------------------
 
-__device__ bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
+__device__ QC_BIG_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
                           int ncand, int vmax, Bounds& b)
 {
     int lane = lane_id();
@@ -442,7 +466,7 @@ __device__ bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const u
 }
 
 // every member extendable? (main.cu:1749-1753)
-__device__ bool members_ok(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
+__device__ QC_BIG_FN bool members_ok(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
                            const Bounds& b)
 {
     int lane = lane_id();
@@ -472,7 +496,7 @@ __device__ int compact(Ws& ws, const uint32_t* mask, int t)
 }
 
 // exdeg[v] = |N(v) & R| for v in mask `who`
-__device__ void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, const uint32_t* R)
+__device__ QC_BIG_FN void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, const uint32_t* R)
 {
     int n = compact(ws, who, T.t);
     for (int i = lane_id(); i < n; i += 32) {
@@ -483,7 +507,7 @@ __device__ void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, co
 }
 
 // out = {v in in_mask : cand_valid(v)} ; rem = in_mask \ out
-__device__ void filter_valid(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* in_mask, int t, int W,
+__device__ QC_BIG_FN void filter_valid(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* in_mask, int t, int W,
                              int m, const Bounds& b, uint32_t* out, uint32_t* rem)
 {
     int lane = lane_id();
@@ -517,7 +541,7 @@ __device__ void filter_valid(const ExpandParams& P, const Rules& R, Ws& ws, cons
 
 enum { DP_DONE = 0, DP_INVALID = 1, DP_SWITCH = 2 };
 
-__device__ int degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
+__device__ QC_BIG_FN int degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
                             int m, const uint32_t* Call, const uint32_t* D, uint32_t* Rm,
                             Bounds& b, bool may_switch)
 {
@@ -565,7 +589,7 @@ __device__ __forceinline__ void check_fail(const ExpandParams& P, unsigned long 
 }
 
 // write the ids of the vertices in mask `mm` (count k) as one set
-__device__ void emit_mask(const ExpandParams& P, const Rules& R, const TaskView& T, const uint32_t* mm, int k)
+__device__ QC_BIG_FN void emit_mask(const ExpandParams& P, const Rules& R, const TaskView& T, const uint32_t* mm, int k)
 {
     int lane = lane_id();
     unsigned long long at = 0;
@@ -596,7 +620,7 @@ __device__ void emit_mask(const ExpandParams& P, const Rules& R, const TaskView&
 }
 
 // clique check (main.cu:1974-1995): every member has indeg >= md[m]
-__device__ void check_clique(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* mm,
+__device__ QC_BIG_FN void check_clique(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* mm,
                              int m)
 {
     int lane = lane_id();
@@ -674,7 +698,7 @@ __device__ bool push_item(const ExpandParams& P, const WorkItem& it)
 // instead of queueing on one shard's top.  Every lane pushes a share.
 // Returns false when a shard is full (the run then stops with
 // ST_TASK_OVERFLOW) or a slot wait gave up.
-__device__ bool push_ranges(const ExpandParams& P, unsigned long long rec, int q_lo, int hi_first,
+__device__ QC_SMALL_FN bool push_ranges(const ExpandParams& P, unsigned long long rec, int q_lo, int hi_first,
                             int split, int count)
 {
     const int lane = lane_id();
@@ -830,7 +854,7 @@ __device__ int pop_shared(const ExpandParams& P, StackEntry& out, unsigned long 
 // busy warps read to decide whether to donate.  The first task of a popped
 // bundle becomes the warp's item (in lane 0), the others go on its own stack
 // (it holds no work when it pops, so they fit).
-__device__ int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out)
+__device__ QC_SMALL_FN int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out)
 {
     const int lane = lane_id();
     if (lane == 0) atomicAdd(&P.ctl->idle_warps, 1);
@@ -893,7 +917,7 @@ constexpr int kEagerHungry = 4;
 // task of this warp's own stack, oldest (shallowest, usually largest) first,
 // in bundles sized so each waiting warp can take one.  Lane b pushes bundle b
 // to shard (home + b), so the pushes' round trips overlap.
-__device__ void donate(const ExpandParams& P, Ws& ws)
+__device__ QC_SMALL_FN void donate(const ExpandParams& P, Ws& ws)
 {
     const int lane = lane_id();
     __syncwarp(); // lane 0's stack and counters written before the call
@@ -1067,7 +1091,7 @@ __device__ __forceinline__ bool key_less(unsigned long long ah, unsigned long lo
 }
 
 // Warp bitonic sort of n (key_hi, key_lo, sel) entries in the workspace.
-__device__ void sort_keys(Ws& ws, int n)
+__device__ QC_BIG_FN void sort_keys(Ws& ws, int n)
 {
     int lane = lane_id();
     int N = 1;
@@ -1099,7 +1123,7 @@ __device__ void sort_keys(Ws& ws, int n)
     }
 }
 
-__device__ void write_child(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
+__device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
                             int m, const uint32_t* Rm, int nr)
 {
     int lane = lane_id();
@@ -1204,7 +1228,7 @@ __device__ void write_child(const ExpandParams& P, const Rules& R, const TaskVie
 __device__ void branch_rest_small(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws,
                                   const uint32_t* M, int m1, const uint32_t* Rm, const Bounds& b);
 
-__device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, int q)
+__device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, int q)
 {
     const int t = T.t, W = T.W;
     int lane = lane_id();
@@ -1251,7 +1275,9 @@ __device__ void expand_branch(const ExpandParams& P, const Rules& R, const TaskV
         if (m1 >= R.min_size) check_clique(P, R, T, ws, M, m1);
         return;
     }
-    if (dp == DP_SWITCH) {
+    // the rest on the register path once members and candidates fit a warp
+    // (a converged pruning repeats one round there, which removes nothing)
+    if (dp == DP_SWITCH || (P.small_path && m1 + bs_count(Rm, W) <= 32)) {
         branch_rest_small(P, R, T, ws, M, m1, Rm, b);
         return;
     }
@@ -1410,7 +1436,7 @@ __device__ __forceinline__ int top_k_sum(unsigned cs, int in, int k)
 
 // LU bounds (main.cu:1857-1972) for members set M (m of them) and the
 // candidate indegree multiset given by lanes in `cs` with value `in`.
-__device__ bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int m, unsigned cs, int in, int ex,
+__device__ QC_SMALL_FN bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int m, unsigned cs, int in, int ex,
                          Bounds& b)
 {
     int lane = lane_id();
@@ -1478,7 +1504,7 @@ __device__ bool lu_small(const ExpandParams& P, const Rules& R, unsigned M, int 
 
 // the rounds of the degree pruning fixpoint after the first: entered with
 // the surviving candidates Rm and the removed set X (non-empty), both words
-__device__ bool prune_loop_small(const ExpandParams& P, const Rules& R, unsigned a1, unsigned M, int m,
+__device__ QC_SMALL_FN bool prune_loop_small(const ExpandParams& P, const Rules& R, unsigned a1, unsigned M, int m,
                                  unsigned& Rm, unsigned X, int in, int& ex, Bounds& b)
 {
     int lane = lane_id();
@@ -1507,7 +1533,7 @@ __device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, 
 
 // Whole warp: append the buffered sets to the result buffer under one
 // reservation of result ints and one of set indices.
-__device__ void emit_flush(const ExpandParams& P, Ws& ws)
+__device__ QC_SMALL_FN void emit_flush(const ExpandParams& P, Ws& ws)
 {
     const int lane = lane_id();
     __syncwarp();
@@ -1563,7 +1589,7 @@ __device__ __forceinline__ void clique_small(const ExpandParams& P, const Rules&
 }
 
 // child record of the vertices in M2 | R2, Q-sorted, matrices compacted
-__device__ void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T, unsigned M2, int m2,
+__device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T, unsigned M2, int m2,
                             unsigned R2, int in, int ex)
 {
     int lane = lane_id();
@@ -1665,7 +1691,7 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
 // The rest of a branch once its first degree pruning has converged: members
 // M1 (m1 of them), candidates Rm, bounds b, degrees in/ex of this lane's
 // vertex.  Critical vertices, second pruning, clique check, child.
-__device__ void branch_tail_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T,
+__device__ QC_SMALL_FN void branch_tail_small(const ExpandParams& P, const Rules& R, Ws& ws, const SmallTask& T,
                                   unsigned M1, int m1, unsigned Rm, int in, int ex, const Bounds& b)
 {
     int lane = lane_id();
@@ -1703,7 +1729,7 @@ __device__ void branch_tail_small(const ExpandParams& P, const Rules& R, Ws& ws,
 // rows restricted to S) and the rest of the branch runs there.  Within S the
 // children's order keys need ranks: of the ids, and of the task's lookahead
 // 2-hop counts (which may exceed 31 in a large task).
-__device__ void branch_rest_small(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws,
+__device__ QC_SMALL_FN void branch_rest_small(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws,
                                   const uint32_t* M, int m1, const uint32_t* Rm, const Bounds& b)
 {
     const int lane = lane_id();
@@ -1760,7 +1786,15 @@ __device__ void branch_rest_small(const ExpandParams& P, const Rules& R, const T
 
 // Branches of a small task handed to waiting warps: a fresh task with at
 // least this many branches is split when other warps wait for work.
-constexpr int kSmallSplitMin = 4;
+#ifndef QC_SMALL_SPLIT_MIN
+#define QC_SMALL_SPLIT_MIN 8
+#endif
+constexpr int kSmallSplitMin = QC_SMALL_SPLIT_MIN;
+// waiting warps needed before a small task splits
+#ifndef QC_SMALL_SPLIT_HUNGRY
+#define QC_SMALL_SPLIT_HUNGRY 2
+#endif
+constexpr int kSmallSplitHungry = QC_SMALL_SPLIT_HUNGRY;
 // at most this many branch ranges pushed by one task
 constexpr int kSmallSplitMax = 16;
 
@@ -1771,7 +1805,7 @@ constexpr int kSmallSplitMax = 16;
 // children's order reads them).  A branch-range item (q_lo >= 0) of a split
 // task runs its branches only.  Returns true when this call pushed branch
 // ranges of the record, which is then shared.
-__device__ bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V,
+__device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V,
                               int q_lo, int q_hi, bool sroot)
 {
     int lane = lane_id();
@@ -1835,9 +1869,9 @@ __device__ bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, con
         // the first part (the highest positions, branched first)
         const int nb = qhi - qlo + 1;
         const int hungry = ws.sm->hungry;
-        if (hungry > 0 && nb >= kSmallSplitMin) {
+        if (hungry >= kSmallSplitHungry && nb >= kSmallSplitMin) {
             int parts = hungry + 1;
-            parts = parts > nb / 2 ? nb / 2 : parts;
+            parts = parts > nb / 4 ? nb / 4 : parts; // ranges of at least 4 branches
             parts = parts > kSmallSplitMax + 1 ? kSmallSplitMax + 1 : parts;
             const int per = (nb + parts - 1) / parts;
             const int extra = (nb - per + per - 1) / per;

@@ -115,6 +115,24 @@ def read_serialized(path: str) -> Graph:
     return Graph(n=n, off=off, adj=adj, off2=off2, adj2=adj2)
 
 
+def write_binary(g: Graph, path: str, twohop: bool = True) -> None:
+    """The binary CSR file the library reads (qc_graph_read_binary): magic
+    "QCSRBIN1", int64 n, nnz, nnz2 (-1 without two-hop lists), int64 offsets,
+    int32 rows padded to 8 bytes, then the two-hop offsets and rows."""
+    off = np.asarray(g.off, "<i8")
+    adj = np.asarray(g.adj, "<i4")
+    two = twohop and g.off2 is not None
+    with open(path, "wb") as f:
+        f.write(b"QCSRBIN1")
+        f.write(np.asarray([g.n, len(adj), len(g.adj2) if two else -1], "<i8").tobytes())
+        f.write(off.tobytes())
+        f.write(adj.tobytes())
+        f.write(b"\0" * ((8 - (4 * len(adj)) % 8) % 8))
+        if two:
+            f.write(np.asarray(g.off2, "<i8").tobytes())
+            f.write(np.asarray(g.adj2, "<i4").tobytes())
+
+
 def write_adjlist(g: Graph, path: str) -> None:
     """Adjacency-list text (one line per vertex), the input of adjToSer."""
     with open(path, "w") as f:

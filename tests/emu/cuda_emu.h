@@ -22,6 +22,7 @@
 #define __global__
 #define __host__
 #define __forceinline__ inline
+#define __noinline__ __attribute__((noinline))
 #define __launch_bounds__(...)
 // block-shared variables of a kernel: one copy per process, so an emulated
 // kernel that declares them runs as a single block, one launch at a time
@@ -105,6 +106,17 @@ inline unsigned __ballot_sync(unsigned, int pred)
     unsigned r = 0;
     for (int i = 0; i < 32; i++)
         if (emu_w->slot[i]) r |= 1u << i;
+    emu_w->bar.arrive_and_wait();
+    return r;
+}
+// lanes whose value equals this lane's
+inline unsigned __match_any_sync(unsigned, int v)
+{
+    emu_w->slot[emu_lane] = (uint64_t)(uint32_t)v;
+    emu_w->bar.arrive_and_wait();
+    unsigned r = 0;
+    for (int i = 0; i < 32; i++)
+        if (emu_w->slot[i] == (uint64_t)(uint32_t)v) r |= 1u << i;
     emu_w->bar.arrive_and_wait();
     return r;
 }

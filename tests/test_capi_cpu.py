@@ -142,3 +142,26 @@ def test_mining_without_a_device_fails_loudly(has_gpu):
     with pytest.raises(Q.QCError) as e:
         Q.mine(g, 0.8, 4)
     assert e.value.status == 10
+
+
+def test_binary_round_trip_through_abi():
+    """Binary CSR file: write, read back (auto-detected), same arrays as the
+    serialized text gives; a file whose size disagrees with its header, or
+    with a bad magic, is refused."""
+    g = graphs.random_small(40, 0.2, 6, planted=2, size=8)
+    d = tempfile.mkdtemp()
+    txt, binp = os.path.join(d, "g.txt"), os.path.join(d, "g.bin")
+    graphs.write_serialized(g, txt)
+    Q.DeviceGraph.read(txt).write_binary(binp)
+    assert open(binp, "rb").read(8) == b"QCSRBIN1"
+    back = Q.DeviceGraph.read(binp).to_graph()
+    for a, b in ((back.off, g.off), (back.adj, g.adj), (back.off2, g.off2), (back.adj2, g.adj2)):
+        assert np.array_equal(a, b)
+    raw = open(binp, "rb").read()
+    bad = os.path.join(d, "bad.bin")
+    for blob, msg in ((raw[:-4], "does not match its header"), (b"QCSRBIN2" + raw[8:], "")):
+        open(bad, "wb").write(blob)
+        with pytest.raises(Q.QCError) as e:
+            h = Q.C.c_void_p()
+            Q._check(Q.lib().qc_graph_read_binary(bad.encode(), Q.C.byref(h)))
+        assert e.value.status == 3 and msg in str(e.value)

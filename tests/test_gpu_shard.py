@@ -60,3 +60,23 @@ def test_root_alone_matches_the_oracle(ctx, n):
     res = ctx.mine(dg, 0.9, 15)
     assert res.stats["level0_on_device"] == 1
     assert res.stats["root_size"] == len(want_ids)
+
+
+def test_binary_graph_file_without_twohop_lists(tmp_path):
+    """A binary CSR file holding only the 1-hop lists: the library builds the
+    two-hop lists on the GPU (equal to the oracle's), and the drop-in CLI gives
+    the same result file for it as for the serialized text of the graph."""
+    g = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
+    binp, txt = str(tmp_path / "g.bin"), str(tmp_path / "g.txt")
+    graphs.write_binary(g, binp, twohop=False)
+    graphs.write_serialized(g, txt)
+    back = Q.DeviceGraph.read(binp).to_graph()
+    off2, adj2 = oracle.twohop(g.n, g.off, g.adj)
+    assert np.array_equal(back.off2, off2) and np.array_equal(back.adj2, adj2)
+    outs = []
+    for path in (binp, txt):
+        out = str(tmp_path / (path.rsplit("/", 1)[1] + ".result"))
+        rc, text = Q.cli(path, "0.8", 10, out, 0, cwd=str(tmp_path))
+        assert rc == 0, text
+        outs.append(open(out).read())
+    assert outs[0] == outs[1] == oracle.result_text(oracle.solve(g, 0.8, 10)[0])
