@@ -395,7 +395,7 @@ def run_budgeted(args, w="cfg2"):
     return out
 
 
-def run_serving(args):
+def run_serving(args, standalone=True):
     """Serving: Poisson arrivals of mining queries, 90% drawn from the batched
     workload's instances and 10% config-1-sized graphs (ER n=1000 + 5 planted
     groups of 30, reseeded per query); latency p50/p99 and instances/s per rate,
@@ -449,7 +449,9 @@ def run_serving(args):
         "rates": rates_out,
         "serial": {"instances_per_s": n_req / serial_s, "form": "one qc_mine at a time"},
     }
-    print(json.dumps(line))
+    if standalone:
+        print(json.dumps(line))
+    return line
 
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
@@ -700,6 +702,16 @@ def run_ours(args):
             ctx.close()
             ctx = None
             line["batched"] = run_batch(args, standalone=False)
+        if args.serve_in_default and world == 1:
+            if ctx is not None:
+                ctx.close()
+                ctx = None
+            import copy
+            a2 = copy.copy(args)
+            a2.serve_requests, a2.serve_rates = 150, [30.0, 100.0]
+            sv = run_serving(a2, standalone=False)
+            line["serving"] = {"workload": "cfg5", "config": sv["config"], "rates": sv["rates"],
+                               "serial": sv["serial"]}
         if args.budget_ms > 0 and world == 1:
             if ctx is not None:
                 ctx.close()
@@ -741,6 +753,8 @@ def main():
                     help="skip the batched-vs-plain comparison in the default run")
     ap.add_argument("--budget-ms", type=int, default=500,
                     help="time budget of the config-2 measurement in the default run (0: skip)")
+    ap.add_argument("--no-serve", dest="serve_in_default", action="store_false",
+                    help="skip the short serving measurement in the default run")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--serve-warps", type=int, default=8, help="warps per block of each slot")

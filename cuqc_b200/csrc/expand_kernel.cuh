@@ -39,10 +39,16 @@ namespace qcb {
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+// warp reductions: one redux instruction on the device, shuffles in the
+// CPU emulator
 __device__ __forceinline__ int wsum(int x)
 {
+#ifdef QC_EMULATION
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(QC_FULL, x, o);
     return x;
+#else
+    return __reduce_add_sync(QC_FULL, x);
+#endif
 }
 __device__ __forceinline__ long long wsum64(long long x)
 {
@@ -51,19 +57,27 @@ __device__ __forceinline__ long long wsum64(long long x)
 }
 __device__ __forceinline__ int wmin(int x)
 {
+#ifdef QC_EMULATION
     for (int o = 16; o; o >>= 1) {
         int y = __shfl_xor_sync(QC_FULL, x, o);
         x = y < x ? y : x;
     }
     return x;
+#else
+    return __reduce_min_sync(QC_FULL, x);
+#endif
 }
 __device__ __forceinline__ int wmax(int x)
 {
+#ifdef QC_EMULATION
     for (int o = 16; o; o >>= 1) {
         int y = __shfl_xor_sync(QC_FULL, x, o);
         x = y > x ? y : x;
     }
     return x;
+#else
+    return __reduce_max_sync(QC_FULL, x);
+#endif
 }
 // inclusive prefix sum across lanes
 __device__ __forceinline__ int wscan(int x)
@@ -390,7 +404,8 @@ __device__ QC_BIG_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& w
     }
     int min_in = wmin(mi);
     int min_tot = wmin(mt);
-    long long sum_in = wsum64(si);
+    // a sum of at most t indegrees below t: 32 bits hold it below 46,341 vertices
+    long long sum_in = t < 46341 ? (long long)wsum((int)si) : wsum64(si);
     int me = 0x7fffffff;
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
@@ -911,7 +926,10 @@ __device__ void schedule_child(const ExpandParams& P, Ws& ws, unsigned long long
 
 // waiting warps from which a small task's children are donated between its
 // branches, not only between items
-constexpr int kEagerHungry = 4;
+#ifndef QC_EAGER_HUNGRY
+#define QC_EAGER_HUNGRY 4
+#endif
+constexpr int kEagerHungry = QC_EAGER_HUNGRY;
 
 // Whole warp: while other warps wait for work, hand them all but the newest
 // task of this warp's own stack, oldest (shallowest, usually largest) first,

@@ -226,6 +226,32 @@ def chung_lu_planted(n, beta, mean_degree, n_groups, size_range, density_range, 
     return from_edges(n, np.concatenate(ss), np.concatenate(dd))
 
 
+def chung_lu_sparse_planted(n, beta, mean_degree, n_groups, size_range, density_range, seed,
+                            with_twohop=False):
+    """Chung-Lu graph for large n in O(n + m): n * mean_degree / 2 edges whose
+    two endpoints are drawn independently in proportion to the expected
+    degrees w (chung_lu_weights), self loops dropped and repeats merged -- the
+    edge-sampling form of the expected-degree model (each pair appears with
+    probability about 1 - exp(-w_i w_j / sum w), close to min(1, w_i w_j /
+    sum w) for all but the heaviest pairs).  Planted groups as in
+    chung_lu_planted.  The two-hop lists are left to the GPU unless asked."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = chung_lu_weights(n, beta, mean_degree)
+    m = int(round(n * mean_degree / 2.0))
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    src = np.searchsorted(cdf, rng.random(m), side="right").clip(0, n - 1)
+    dst = np.searchsorted(cdf, rng.random(m), side="right").clip(0, n - 1)
+    ss, dd = [src], [dst]
+    for _ in range(n_groups):
+        s = int(rng.integers(size_range[0], size_range[1] + 1))
+        d = float(rng.uniform(density_range[0], density_range[1]))
+        members = rng.choice(n, size=min(s, n), replace=False)
+        a, b = _plant(rng, members, d)
+        ss.append(a); dd.append(b)
+    return from_edges(n, np.concatenate(ss), np.concatenate(dd), with_twohop=with_twohop)
+
+
 def random_small(n, p, seed, planted=0, size=0, density=1.0):
     """Small random graph for parity sweeps."""
     rng = np.random.Generator(np.random.PCG64(seed))
