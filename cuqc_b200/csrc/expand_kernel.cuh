@@ -114,7 +114,10 @@ __device__ __forceinline__ bool rec_bit(const uint32_t* a, int v) { return (rec_
 __device__ __forceinline__ int popc_and(const uint32_t* row, const uint32_t* mask, int W)
 {
     int s = 0;
-    for (int w = 0; w < W; w++) s += __popc(rec_ld(row + w) & mask[w]);
+    for (int w = 0; w < W; w++) {
+        const uint32_t mw = mask[w]; // the same in every lane: skipping a zero word never diverges
+        if (mw) s += __popc(rec_ld(row + w) & mw);
+    }
     return s;
 }
 
@@ -333,9 +336,11 @@ __device__ QC_BIG_FN int build_hist(const ExpandParams& P, const Rules& R, Ws& w
     __syncwarp();
     int cnt = 0;
     for (int base = 0; base < t; base += 32) {
+        const uint32_t cw = cm[base >> 5];
+        if (cw == 0) continue; // no vertex of this chunk (the word is the same in every lane)
         int v = base + lane;
         int j = -1;
-        if (v < t && bit(cm, v)) {
+        if (v < t && ((cw >> lane) & 1u)) {
             int in = ws.indeg()[v];
             if (!filter_valid || cand_valid(R, in, ws.exdeg()[v], m, b)) {
                 j = vmax - (in > vmax ? vmax : (in < 0 ? 0 : in));
@@ -356,7 +361,8 @@ __device__ QC_BIG_FN int build_hist(const ExpandParams& P, const Rules& R, Ws& w
         int c = (j <= vmax + 1) ? ws.hist()[j] : 0;
         long long s = (j <= vmax) ? (long long)c * (vmax - j) : 0;
         int ic = wscan(c);
-        long long is = wscan64(s);
+        // the sums stay below t * vmax: 32 bits hold them below 46,341 vertices
+        long long is = t < 46341 ? (long long)wscan((int)s) : wscan64(s);
         if (j <= vmax + 1) {
             ws.pcnt()[j] = carry + ic - c;
             ws.psum()[j] = carry_s + is - s;
@@ -391,13 +397,22 @@ __device__ QC_BIG_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& w
                           int ncand, int vmax, Bounds& b)
 {
     int lane = lane_id();
-    int mi = 0x7fffffff, mt = 0x7fffffff;
+    // one pass over the members: this lane's smallest indegree and, among
+    // its members with that indegree, the smallest exdegree
+    int mi = 0x7fffffff, mt = 0x7fffffff, me = 0x7fffffff;
     long long si = 0;
     for (int base = 0; base < t; base += 32) {
+        const uint32_t mw = mm[base >> 5];
+        if (mw == 0) continue;
         int v = base + lane;
-        if (v < t && bit(mm, v)) {
+        if (v < t && ((mw >> lane) & 1u)) {
             int in = ws.indeg()[v], ex = ws.exdeg()[v];
-            mi = in < mi ? in : mi;
+            if (in < mi) {
+                mi = in;
+                me = ex;
+            } else if (in == mi && ex < me) {
+                me = ex;
+            }
             mt = in + ex < mt ? in + ex : mt;
             si += in;
         }
@@ -406,15 +421,7 @@ __device__ QC_BIG_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& w
     int min_tot = wmin(mt);
     // a sum of at most t indegrees below t: 32 bits hold it below 46,341 vertices
     long long sum_in = t < 46341 ? (long long)wsum((int)si) : wsum64(si);
-    int me = 0x7fffffff;
-    for (int base = 0; base < t; base += 32) {
-        int v = base + lane;
-        if (v < t && bit(mm, v) && ws.indeg()[v] == min_in) {
-            int ex = ws.exdeg()[v];
-            me = ex < me ? ex : me;
-        }
-    }
-    int min_in_ex = wmin(me);
+    int min_in_ex = wmin(mi == min_in ? me : 0x7fffffff);
 
     bool invalid = false;
     b.med = mindeg(R, m + 1);
@@ -487,8 +494,10 @@ __device__ QC_BIG_FN bool members_ok(const ExpandParams& P, const Rules& R, Ws& 
     int lane = lane_id();
     int bad = 0;
     for (int base = 0; base < t; base += 32) {
+        const uint32_t mw = mm[base >> 5];
+        if (mw == 0) continue;
         int v = base + lane;
-        if (v < t && bit(mm, v) && !vert_extendable(R, ws.indeg()[v], ws.exdeg()[v], m, b)) bad = 1;
+        if (v < t && ((mw >> lane) & 1u) && !vert_extendable(R, ws.indeg()[v], ws.exdeg()[v], m, b)) bad = 1;
     }
     return !__any_sync(QC_FULL, bad);
 }
@@ -500,8 +509,10 @@ __device__ int compact(Ws& ws, const uint32_t* mask, int t)
     int lane = lane_id();
     int n = 0;
     for (int base = 0; base < t; base += 32) {
+        const uint32_t mw = mask[base >> 5];
+        if (mw == 0) continue;
         int v = base + lane;
-        bool in = v < t && bit(mask, v);
+        bool in = v < t && ((mw >> lane) & 1u);
         unsigned bal = __ballot_sync(QC_FULL, in);
         if (in) ws.vlist()[n + __popc(bal & ((1u << lane) - 1u))] = v;
         n += __popc(bal);
@@ -527,8 +538,16 @@ __device__ QC_BIG_FN void filter_valid(const ExpandParams& P, const Rules& R, Ws
 {
     int lane = lane_id();
     for (int base = 0; base < t; base += 32) {
+        const uint32_t iw = in_mask[base >> 5];
+        if (iw == 0) {
+            if (lane == 0) {
+                out[base >> 5] = 0;
+                if (rem) rem[base >> 5] = 0;
+            }
+            continue;
+        }
         int v = base + lane;
-        bool in = v < t && bit(in_mask, v);
+        bool in = v < t && ((iw >> lane) & 1u);
         bool ok = in && cand_valid(R, ws.indeg()[v], ws.exdeg()[v], m, b);
         unsigned bo = __ballot_sync(QC_FULL, ok);
         unsigned br = __ballot_sync(QC_FULL, in && !ok);
@@ -1274,11 +1293,21 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
         for (int w = lane; w < W; w += 32) MD[w] = M[w] | D[w];
         __syncwarp();
         int n = compact(ws, MD, t);
+        // members are positions [0, m) and q, the earlier candidates [m, q):
+        // both counts come from the row's words up to q's, read once
+        const int mt = T.m, qw = q >> 5;
         for (int i = lane; i < n; i += 32) {
             int v = ws.vlist()[i];
             const uint32_t* row = T.A1 + (int64_t)v * W;
-            ws.indeg()[v] = popc_and(row, M, W);
-            ws.exdeg()[v] = popc_and(row, PRE, W);
+            int in = 0, ex = 0;
+            for (int w = 0; w <= qw; w++) {
+                const uint32_t x = rec_ld(row + w);
+                in += __popc(x & range_word(w, 0, mt));
+                ex += __popc(x & range_word(w, mt, q));
+            }
+            in += (int)((rec_ld(row + qw) >> (q & 31)) & 1u);
+            ws.indeg()[v] = in;
+            ws.exdeg()[v] = ex;
         }
         __syncwarp();
     }
