@@ -3,27 +3,26 @@
 //
 // Input: the emitted sets in the device result buffer, [k, id_1..id_k] each,
 // and the start offset of every set (written by the expansion kernel).
-//   1. one warp per set: sort its ids ascending into the sorted buffer and
-//      build its 256-bit signature;
-//   2. each set writes its (vertex, set) incidences at once, to slots
-//      reserved with an atomic add (their order does not matter: 3 sorts);
-//   3. inverted index: the incidences radix-sorted by vertex and, within a
-//      vertex, by set size descending, give every vertex its posting list
-//      with the largest sets first;
-//   4. one warp per set S: scan the posting list of S's rarest
-//      vertex while its sets are larger than S, 128 candidates a round, and
-//      test each by its 256-bit signature (a bit per hashed id, written in
-//      step 1): a candidate whose signature lacks one of S's bits cannot
-//      contain S; the few that pass are checked exactly by the whole warp.
-//      S is maximal iff no such set contains it.  Exact copies of a maximal
-//      set follow the larger sets in the same list: the copy of the smallest
-//      index is kept (copies that a larger set contains need no check);
-//   5. each maximal set is appended to the output at a slot reserved with an
-//      atomic add, with an entry (key of its first two ids, offset).  The
-//      entries are put in the order the reference's prefix tree writes
-//      (lexicographic): by 256-bit vectors over the survivors' ranked ids when
-//      there are at most 256 distinct ids, else by a merge sort comparing the
-//      sets; the host gathers the sets in that order.
+//   1. one warp per set: sort its ids ascending into the sorted buffer, build
+//      its 256-bit signature and its order-free 64-bit hash (the sum of a
+//      mix of each id);
+//   2. the one-less pass: every set is entered in an open-addressing table
+//      by its hash; every set T looks up T minus each of its ids (hash
+//      H(T) - mix(x)) and marks the sets equal to it, and looks up its own
+//      hash for an exact copy of smaller index, which marks T;
+//   3. the residual -- the unmarked sets -- holds every maximal set (a set
+//      inside any emitted set is inside a maximal one, and a maximal set is
+//      never marked), so only the residual is tested for supersets, against
+//      itself: pairwise (signature first, then an exact warp check) when it
+//      has at most 4,096 sets, else through an inverted index (incidences
+//      radix-sorted by vertex and set size, one warp per set scanning the
+//      posting list of its rarest vertex for larger sets);
+//   4. each maximal set is appended to the output at a slot reserved with an
+//      atomic add, with an entry for the ordering.  The entries are put in the
+//      order the reference's prefix tree writes (lexicographic): by 256-bit
+//      vectors over the survivors' ranked ids when there are at most 256
+//      distinct ids (few survivors ranked by counting, many by a merge sort),
+//      else by a merge sort comparing the sets; the host only gathers.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 #include <cub/device/device_merge_sort.cuh>
@@ -529,32 +528,69 @@ __global__ void one_less_kernel(const int32_t* srt, const unsigned long long* st
         const int k = srt[a];
         const int32_t* T = srt + a + 1;
         const unsigned long long hT = hsh[s];
-        for (int i = lane; i < k; i += 32) {
-            const unsigned long long h = hT - id_mix(T[i]);
-            unsigned long long p = h & mask;
-            for (unsigned long long it = 0; it <= mask; it++) {
-                const int32_t c = table[p];
-                if (c < 0) break;
-                if (hsh[c] == h) {
-                    const unsigned long long b = starts[c];
-                    if (srt[b] == k - 1 && thread_subset(srt + b + 1, k - 1, T, k)) dead[c] = 1;
-                }
-                p = (p + 1) & mask;
-            }
-        }
-        if (lane == 0) {
-            unsigned long long p = hT & mask;
-            for (unsigned long long it = 0; it <= mask; it++) {
-                const int32_t c = table[p];
-                if (c < 0) break;
-                if (c < s && hsh[c] == hT) {
-                    const unsigned long long b = starts[c];
-                    if (srt[b] == k && thread_subset(srt + b + 1, k, T, k)) {
-                        dead[s] = 1;
-                        break;
+        if (k >= 32) {
+            // sets of 32 ids or more: each lane checks its own hits
+            for (int i = lane; i < k; i += 32) {
+                const unsigned long long h = hT - id_mix(T[i]);
+                unsigned long long p = h & mask;
+                for (unsigned long long it = 0; it <= mask; it++) {
+                    const int32_t c = table[p];
+                    if (c < 0) break;
+                    if (hsh[c] == h) {
+                        const unsigned long long b = starts[c];
+                        if (srt[b] == k - 1 && thread_subset(srt + b + 1, k - 1, T, k)) dead[c] = 1;
                     }
+                    p = (p + 1) & mask;
                 }
-                p = (p + 1) & mask;
+            }
+            if (lane == 0) {
+                unsigned long long p = hT & mask;
+                for (unsigned long long it = 0; it <= mask; it++) {
+                    const int32_t c = table[p];
+                    if (c < 0) break;
+                    if (c < s && hsh[c] == hT) {
+                        const unsigned long long b = starts[c];
+                        if (srt[b] == k && thread_subset(srt + b + 1, k, T, k)) {
+                            dead[s] = 1;
+                            break;
+                        }
+                    }
+                    p = (p + 1) & mask;
+                }
+            }
+            continue;
+        }
+        // sets of at most 31 ids: lane j holds T[j].  Lane i (< k) walks the
+        // probe sequence of T minus T[i] and lane k that of T itself (for an
+        // exact copy of smaller index); every hit -- a set of the right size
+        // and hash -- is checked by the whole warp at once: id j of the hit
+        // against T's id j (or j + 1 past the dropped one).
+        const int my = lane < k ? T[lane] : 0;
+        const bool prober = lane <= k;
+        const unsigned long long h = lane < k ? hT - id_mix(my) : hT;
+        const int want = lane < k ? k - 1 : k;
+        unsigned long long p = h & mask;
+        bool walking = prober;
+        for (unsigned long long it = 0; it <= mask && __any_sync(0xffffffffu, walking); it++) {
+            int32_t c = -1;
+            if (walking) {
+                c = table[p];
+                if (c < 0) walking = false;
+                else p = (p + 1) & mask;
+            }
+            const bool hit = c >= 0 && hsh[c] == h && (lane < k || c < s) &&
+                             srt[starts[c]] == want;
+            unsigned pend = __ballot_sync(0xffffffffu, hit);
+            while (pend) {
+                const int i = __ffs(pend) - 1;
+                pend &= pend - 1;
+                const int32_t cc = __shfl_sync(0xffffffffu, c, i);
+                const int n = i < k ? k - 1 : k; // ids of the hit
+                const unsigned long long b = starts[cc];
+                const int src = (i < k && lane >= i) ? lane + 1 : lane;
+                const int tv = __shfl_sync(0xffffffffu, my, src & 31);
+                const bool eq = lane >= n || srt[b + 1 + lane] == tv;
+                if (__all_sync(0xffffffffu, eq) && lane == 0) dead[i < k ? cc : s] = 1;
             }
         }
     }
@@ -624,39 +660,23 @@ __global__ void residual_pairs_kernel(const int32_t* srt, const unsigned long lo
     }
 }
 
-// Up to kBlockSortMax bit-vector entries ordered in one block (bitonic
-// network in shared memory), descending: the survivors' lexicographic order.
-constexpr int kBlockSortMax = 4096;
-__global__ void __launch_bounds__(1024) bit_sort_block_kernel(BitEnt* e, int n)
+// Up to kRankSortMax bit-vector entries put in descending order by rank:
+// one warp per entry counts the entries above it and writes it at that
+// position (the vectors are distinct: they stand for distinct maximal sets).
+// n^2 comparisons, spread over the whole grid.
+constexpr int kRankSortMax = 4096;
+__global__ void bit_rank_kernel(const BitEnt* in, int n, BitEnt* out)
 {
-    extern __shared__ __align__(16) unsigned char bsm[];
-    BitEnt* x = (BitEnt*)bsm;
-    int N = 1;
-    while (N < n) N <<= 1;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        if (i < n) x[i] = e[i];
-        else x[i] = BitEnt{{0ull, 0ull, 0ull, 0ull}, -1ll}; // below every real entry
-    }
-    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
     const BitMore more;
-    for (int k = 2; k <= N; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < N; i += blockDim.x) {
-                const int p = i ^ j;
-                if (p > i) {
-                    // blocks with bit k clear put the larger vectors first,
-                    // the others the smaller ones; the last stage all larger first
-                    const bool larger_first = (i & k) == 0;
-                    if (more(x[p], x[i]) == larger_first) {
-                        const BitEnt t = x[i];
-                        x[i] = x[p];
-                        x[p] = t;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) e[i] = x[i];
+    for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        const BitEnt x = in[i];
+        int c = 0;
+        for (int j = lane; j < n; j += 32) c += more(in[j], x) ? 1 : 0;
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) out[c] = x;
+    }
 }
 
 } // namespace
@@ -688,12 +708,12 @@ void FilterScratch::release()
     host = nullptr;
     host_n = 0;
     for (auto* pp : {&sorted, &sig, &poff, &post, &ctr, &ents, &bents, &temp, &ikey, &ikey2,
-                     &ival, &rsig, &hsh, &table, &dead, &rstarts, &ikey3}) {
+                     &ival, &rsig, &hsh, &table, &dead, &rstarts, &ikey3, &bents2}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
     sorted_n = sig_n = poff_n = post_n = ctr_n = ents_n = bents_n = temp_n = ikey_n = ikey2_n =
-        ival_n = rsig_n = hsh_n = table_n = dead_n = rstarts_n = ikey3_n = 0;
+        ival_n = rsig_n = hsh_n = table_n = dead_n = rstarts_n = ikey3_n = bents2_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -828,26 +848,19 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     // the universe is small (one block for a few thousand), else by comparing
     // the sets
     const bool bits = uni <= kBitUniverse && out_sets > 1;
+    void* sorted_bents = nullptr; // where the ordered bit-vector entries end up
     if (bits) {
         ENS(bents, bents_n, sizeof(BitEnt) * out_sets);
+        sorted_bents = F.bents;
         bit_key_kernel<<<blocks, 256, 0, s>>>(d_out, (const SetEnt*)F.ents, (long long)out_sets,
                                               bitmap, rank_base, (BitEnt*)F.bents);
         nlaunch += 1;
-        if (out_sets <= kBlockSortMax) {
-            int N = 1;
-            while (N < out_sets) N <<= 1;
-            const size_t smem = sizeof(BitEnt) * (size_t)N;
-            static bool raised[64] = {};
-            int dev = 0;
-            FCK(cudaGetDevice(&dev));
-            if (dev >= 0 && dev < 64 && !raised[dev]) {
-                FCK(cudaFuncSetAttribute(bit_sort_block_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(BitEnt) * kBlockSortMax)));
-                raised[dev] = true;
-            }
-            bit_sort_block_kernel<<<1, 1024, smem, s>>>((BitEnt*)F.bents, (int)out_sets);
+        if (out_sets <= kRankSortMax) {
+            ENS(bents2, bents2_n, sizeof(BitEnt) * out_sets);
+            bit_rank_kernel<<<blocks, 256, 0, s>>>((const BitEnt*)F.bents, (int)out_sets,
+                                                   (BitEnt*)F.bents2);
             nlaunch += 1;
+            sorted_bents = F.bents2;
         } else {
             size_t tbm = 0;
             FCK(cub::DeviceMergeSort::SortKeys(nullptr, tbm, (BitEnt*)F.bents, (int64_t)out_sets,
@@ -883,7 +896,8 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     if (out_ints) {
         FCK(cudaMemcpyAsync(F.host, d_out, sizeof(int32_t) * out_ints, cudaMemcpyDeviceToHost, s));
         if (bits)
-            FCK(cudaMemcpyAsync((void*)he, F.bents, sizeof(BitEnt) * out_sets, cudaMemcpyDeviceToHost, s));
+            FCK(cudaMemcpyAsync((void*)he, sorted_bents, sizeof(BitEnt) * out_sets,
+                                cudaMemcpyDeviceToHost, s));
         else
             FCK(cudaMemcpyAsync((void*)he, F.ents, sizeof(SetEnt) * out_sets, cudaMemcpyDeviceToHost, s));
         FCK(cudaStreamSynchronize(s));
