@@ -55,7 +55,7 @@ class Config(C.Structure):
                 ("stack_slots", C.c_int64), ("result_ints", C.c_int64),
                 ("keep_emitted", C.c_int32), ("wait_limit_ms", C.c_int32),
                 ("time_limit_ms", C.c_int32), ("split", C.c_int32), ("max_blocks", C.c_int32),
-                ("stage_max", C.c_int32)]
+                ("stage_max", C.c_int32), ("shared_order", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -685,17 +685,39 @@ __device__ __forceinline__ unsigned long long now_ns()
 // the shard a warp pushes to and starts its scans from
 __device__ __forceinline__ int home_shard() { return (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % kStackShards); }
 
+// Shared-stack shards.  Each shard is a stack (idle warps take the newest
+// entry: depth first, few live tasks) or, with P.shared_fifo, a ring whose
+// oldest entry is taken first (the shallowest donated tasks, which head the
+// largest subtrees, start first: better when many independent instances
+// keep every warp busy).  reserve_push returns the slot a new entry of shard
+// `shard` goes to, or -1 when the shard is full.
+__device__ __forceinline__ long long reserve_push(const ExpandParams& P, int shard)
+{
+    const int cap = P.ctl->stack_cap;
+    const int idx = atomicAdd(&P.ctl->stack_top[shard], 1);
+    if (P.shared_fifo) {
+        // indices count up for the whole run; cap is a power of two, so the
+        // slot (idx mod cap) stays right when the 32-bit count wraps.  Takers
+        // may have claimed this index and later ones already (they wait for
+        // the writes), so the distance to the bottom is taken as signed.
+        if ((int)((unsigned)idx - (unsigned)*(volatile int*)&P.ctl->stack_bot[shard]) >= cap)
+            return -1;
+        return (long long)shard * cap + ((unsigned)idx & (unsigned)(cap - 1));
+    }
+    if (idx >= cap) return -1;
+    return (long long)shard * cap + idx;
+}
+
 // lane-0 only: one entry onto shard `shard` of the shared stack
 __device__ bool push_entry(const ExpandParams& P, const StackEntry& e, int shard)
 {
     atomicAdd(&P.ctl->pending, 1);
-    int idx = atomicAdd(&P.ctl->stack_top[shard], 1);
-    if (idx >= P.ctl->stack_cap) {
+    const long long at = reserve_push(P, shard);
+    if (at < 0) {
         set_status(P, ST_TASK_OVERFLOW);
         atomicSub(&P.ctl->pending, 1);
         return false;
     }
-    long long at = (long long)shard * P.ctl->stack_cap + idx;
     unsigned long long t0 = now_ns();
     unsigned spins = 0;
     while (atomicCAS(&P.slot[at], 0, 2) != 0) {
@@ -742,14 +764,13 @@ __device__ QC_SMALL_FN bool push_ranges(const ExpandParams& P, unsigned long lon
     int ok = 1;
     for (int c = lane; c < count; c += 32) {
         const int shard = (home + c) % kStackShards;
-        const int idx = atomicAdd(&P.ctl->stack_top[shard], 1);
-        if (idx >= P.ctl->stack_cap) {
+        const long long at = reserve_push(P, shard);
+        if (at < 0) {
             set_status(P, ST_TASK_OVERFLOW);
             atomicSub(&P.ctl->pending, 1);
             ok = 0;
             continue;
         }
-        const long long at = (long long)shard * P.ctl->stack_cap + idx;
         unsigned long long t0 = now_ns();
         unsigned spins = 0;
         bool got = true;
@@ -782,16 +803,21 @@ __device__ QC_SMALL_FN bool push_ranges(const ExpandParams& P, unsigned long lon
     return __all_sync(QC_FULL, ok);
 }
 
-// lane 0: read the entry at position idx of shard s once its writer is done
+// lane 0: read the entry at index idx of shard s once its writer is done
 __device__ int take_slot(const ExpandParams& P, int s, int idx, StackEntry& out)
 {
-    // a failed push (shard full) leaves the top above the capacity; such an
-    // index has no slot behind it
-    if (idx >= P.ctl->stack_cap) {
-        set_status(P, ST_TASK_OVERFLOW);
-        return -1;
+    long long at;
+    if (P.shared_fifo) {
+        at = (long long)s * P.ctl->stack_cap + ((unsigned)idx & (unsigned)(P.ctl->stack_cap - 1));
+    } else {
+        // a failed push (shard full) leaves the top above the capacity; such
+        // an index has no slot behind it
+        if (idx >= P.ctl->stack_cap) {
+            set_status(P, ST_TASK_OVERFLOW);
+            return -1;
+        }
+        at = (long long)s * P.ctl->stack_cap + idx;
     }
-    long long at = (long long)s * P.ctl->stack_cap + idx;
     unsigned long long t1 = now_ns();
     unsigned s2 = 0;
     while (atomicCAS(&P.slot[at], 1, 3) != 1) {
@@ -841,14 +867,22 @@ __device__ int pop_shared(const ExpandParams& P, StackEntry& out, unsigned long 
         }
         if (__shfl_sync(QC_FULL, act, 0) < 0) return -1;
         int top = *(volatile int*)&P.ctl->stack_top[lane];
-        unsigned ne = __ballot_sync(QC_FULL, top > 0);
+        const int bot = P.shared_fifo ? *(volatile int*)&P.ctl->stack_bot[lane] : 0;
+        unsigned ne = __ballot_sync(QC_FULL, (int)((unsigned)top - (unsigned)bot) > 0);
         if (ne) {
             unsigned rot = home ? ((ne >> home) | (ne << (32 - home))) : ne;
             int s = (home + __ffs(rot) - 1) & 31;
-            int ts = __shfl_sync(QC_FULL, top, s);
             int got = 0;
-            if (lane == 0 && atomicCAS(&P.ctl->stack_top[s], ts, ts - 1) == ts)
-                got = take_slot(P, s, ts - 1, out);
+            if (P.shared_fifo) {
+                // the oldest entry of the shard
+                const int bs = __shfl_sync(QC_FULL, bot, s);
+                if (lane == 0 && atomicCAS(&P.ctl->stack_bot[s], bs, bs + 1) == bs)
+                    got = take_slot(P, s, bs, out);
+            } else {
+                const int ts = __shfl_sync(QC_FULL, top, s);
+                if (lane == 0 && atomicCAS(&P.ctl->stack_top[s], ts, ts - 1) == ts)
+                    got = take_slot(P, s, ts - 1, out);
+            }
             got = __shfl_sync(QC_FULL, got, 0);
             if (got != 0) return got;
             // lost the race for that top: wait a short, warp-dependent time so

@@ -384,11 +384,21 @@ template <class T> cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaSt
 
 } // namespace
 
+// stack slots rounded up so that every shard's capacity is a power of two
+// (the FIFO form of the shards indexes its ring by a wrapping count)
+static int64_t shard_slots(int64_t want)
+{
+    int64_t per = 2;
+    while (per * kStackShards < want) per <<= 1;
+    return per * kStackShards;
+}
+
 // entries on the fullest shard of the shared stack
 static int max_top(const Control& ctl)
 {
     int m = 0;
-    for (int i = 0; i < kStackShards; i++) m = std::max(m, ctl.stack_top[i]);
+    for (int i = 0; i < kStackShards; i++)
+        m = std::max(m, (int)((unsigned)ctl.stack_top[i] - (unsigned)ctl.stack_bot[i]));
     return m;
 }
 
@@ -660,7 +670,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     std::vector<int32_t> flat;
     for (int attempt = 0;; attempt++) {
         CK(c->arena.ensure((size_t)c->arena_bytes));
-        c->stack_slots = std::max<int64_t>(c->stack_slots, 2 * kStackShards);
+        c->stack_slots = shard_slots(std::max<int64_t>(c->stack_slots, 2 * kStackShards));
         CK(c->stack.ensure(sizeof(StackEntry) * (size_t)c->stack_slots));
         CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
         CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
@@ -751,6 +761,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.small_path = 1;
         P.shard = shard;
         P.nshards = nshards;
+        P.shared_fifo = c->cfg.shared_order == 2 ? 1 : 0;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
         P.time_limit_ns = c->cfg.time_limit_ms > 0
                               ? (unsigned long long)c->cfg.time_limit_ms * 1000000ull : 0ull;
@@ -1299,7 +1310,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         if ((int64_t)arena_at * 2 > c->arena_bytes) c->arena_bytes = (int64_t)arena_at * 2;
         c->stack_slots = std::max<int64_t>(c->stack_slots, (int64_t)nroots * 2 + 64 * kStackShards);
         CK(c->arena.ensure((size_t)c->arena_bytes));
-        c->stack_slots = std::max<int64_t>(c->stack_slots, 2 * kStackShards);
+        c->stack_slots = shard_slots(std::max<int64_t>(c->stack_slots, 2 * kStackShards));
         CK(c->stack.ensure(sizeof(StackEntry) * (size_t)c->stack_slots));
         CK(c->slot.ensure(sizeof(int32_t) * (size_t)c->stack_slots));
         CK(c->results.ensure(sizeof(int32_t) * (size_t)c->result_ints));
@@ -1372,6 +1383,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         P.smem_t = sh.smem_t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
+        P.shared_fifo = c->cfg.shared_order == 1 ? 0 : 1;
         P.wait_ns = (int64_t)c->cfg.wait_limit_ms * 1000000ll;
         P.time_limit_ns = c->cfg.time_limit_ms > 0
                               ? (unsigned long long)c->cfg.time_limit_ms * 1000000ull : 0ull;

@@ -50,7 +50,8 @@ struct Control {
     unsigned long long result_cap;
     unsigned long long set_cap;    // capacity of the set-start array
     int stack_cap;                 // slots per shard; shard s owns slots [s*cap, (s+1)*cap)
-    alignas(128) int stack_top[kStackShards]; // entries on each shard of the shared stack
+    alignas(128) int stack_top[kStackShards]; // entries pushed on each shard of the shared stack
+    alignas(128) int stack_bot[kStackShards]; // entries taken from the bottom (FIFO shards only)
     alignas(128) int pending;      // items on the shared stack + warps holding work
     alignas(128) int idle_warps;   // warps looking for work on the shared stack
     alignas(128) int status;
@@ -170,6 +171,7 @@ struct ExpandParams {
     int32_t split;       // branches per work item before splitting
     int32_t small_path;  // 1: tasks of <= 32 vertices use the register path
     int64_t wait_ns;     // give up a wait after this long without progress
+    int32_t shared_fifo; // 1: idle warps take the oldest shared-stack entry, 0: the newest
     int32_t shard;       // a search split by the root's branches: branch i of the root
     int32_t nshards;     //   (counted from the first branched) belongs to shard i % nshards
     unsigned long long time_limit_ns; // stop this long after the launch began (0: none); the

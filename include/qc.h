@@ -146,6 +146,11 @@ typedef struct {
                                     contexts running at once); 0: every resident block */
     int32_t stage_max;           /* largest task (vertices) worked on in shared memory;
                                     0: as large as the shared memory allows, -1: none */
+    int32_t shared_order;        /* which donated task an idle warp takes: 1 the newest
+                                    (depth first), 2 the oldest (the largest subtrees
+                                    first); 0: newest for qc_mine, oldest for
+                                    qc_mine_batch, whose many instances keep every
+                                    warp busy */
 } qc_config;
 
 /* Fill a config with defaults (device 0, everything autotuned). */

@@ -40,7 +40,7 @@ def lib():
         P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
         L.emu_mine.argtypes = [C.c_int, P64, P32, P64, P32, C.c_double, C.c_int, C.c_int, C.c_int,
                                C.c_int, C.c_longlong, P64, C.POINTER(P32), P64, C.c_int,
-                               C.c_longlong]
+                               C.c_longlong, C.c_int]
         L.emu_mine.restype = C.c_int
         L.emu_free.argtypes = [C.c_void_p]
         L.emu_level0.argtypes = [C.c_int, P64, P32, P64, C.c_double, C.c_int, C.c_int, P32, P32]
@@ -52,7 +52,7 @@ def lib():
 
 
 def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20, small_path=1, stack_cap=0,
-         result_cap=0):
+         result_cap=0, shared_fifo=0):
     """Emitted multiset (flat [k, ids..]) and counters of the emulated kernel."""
     L = lib()
     off, adj = np.ascontiguousarray(g.off, np.int64), np.ascontiguousarray(g.adj, np.int32)
@@ -65,7 +65,7 @@ def mine(g, gamma, min_size, warps=2, split=4, arena_bytes=64 << 20, small_path=
                     adj2.ctypes.data_as(C.POINTER(C.c_int32)), float(gamma), int(min_size),
                     int(warps), int(split), int(small_path), int(arena_bytes), C.byref(ni),
                     C.byref(buf),
-                    cnt.ctypes.data_as(P64), int(stack_cap), int(result_cap))
+                    cnt.ctypes.data_as(P64), int(stack_cap), int(result_cap), int(shared_fifo))
     flat = np.zeros(0, np.int32)
     if ni.value:
         flat = np.ctypeslib.as_array(buf, shape=(ni.value,)).copy()

@@ -38,7 +38,8 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
                         const int32_t* adj2, double gamma, int min_size, int warps, int split,
                         int small_path,
                         long long arena_bytes, int64_t* out_nints, int32_t** out_buf,
-                        int64_t* counters, int stack_cap, long long result_cap)
+                        int64_t* counters, int stack_cap, long long result_cap,
+                        int shared_fifo)
 {
     HostGraph g;
     g.n = n;
@@ -91,8 +92,11 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     ctl.arena_cap = (unsigned long long)arena_bytes;
     ctl.result_cap = result_cap > 0 ? (unsigned long long)result_cap : (1ull << 24);
     ctl.set_cap = ctl.result_cap / 2 + 1;
-    const int total_slots = std::max(stack_cap > 0 ? stack_cap : (1 << 20), 2 * kStackShards);
-    ctl.stack_cap = total_slots / kStackShards;
+    const int want_slots = std::max(stack_cap > 0 ? stack_cap : (1 << 20), 2 * kStackShards);
+    int per_shard = 2; // a power of two, as the library sizes it
+    while (per_shard * kStackShards < want_slots) per_shard <<= 1;
+    const int total_slots = per_shard * kStackShards;
+    ctl.stack_cap = per_shard;
     ctl.stack_top[0] = 1;
     ctl.pending = 1;
     std::vector<StackEntry> stack((size_t)total_slots);
@@ -128,6 +132,7 @@ extern "C" int emu_mine(int n, const int64_t* off, const int32_t* adj, const int
     P.max_t = t;
     P.split = split;
     P.small_path = small_path;
+    P.shared_fifo = shared_fifo;
     P.wait_ns = 20000000000ll;
     P.time_limit_ns = emu_time_limit_ns();
     // stage tasks of up to 96 vertices in (emulated) shared memory, as the
@@ -254,6 +259,7 @@ extern "C" int emu_mine_batch(int count, const int32_t* ns, const int64_t* off_a
     WsLayout L = ws_layout(max_t);
     std::vector<char> ws((size_t)(L.total * warps));
     ExpandParams P{};
+    P.shared_fifo = 1; // oldest donated task first, as batched launches run
     P.rules = rules.data();
     P.nrules = count;
     P.ctl = &ctl;

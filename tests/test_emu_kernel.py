@@ -29,14 +29,16 @@ CASES = [  # (n, p, seed, planted, size, gamma, min_size, warps, split); n > 32 
 ]
 
 
-@pytest.mark.parametrize("small_path", [1, 0])
+@pytest.mark.parametrize("small_path,fifo", [(1, 0), (0, 0), (1, 1)])
 @pytest.mark.parametrize("case", CASES)
-def test_emulated_kernel_matches_oracle(case, small_path):
+def test_emulated_kernel_matches_oracle(case, small_path, fifo):
+    """Both task paths, and the shared stack taken newest first or oldest first."""
     n, p, seed, planted, size, gamma, ms, warps, split = case
     g = graphs.random_small(n, p, seed, planted=planted, size=size, density=0.95)
     want, st = oracle.mine(g, gamma, ms, "clean")
     assert st["tasks"] < 2500, "keep emulated cases small"
-    got, cnt, status = emu.mine(g, gamma, ms, warps=warps, split=split, small_path=small_path)
+    got, cnt, status = emu.mine(g, gamma, ms, warps=warps, split=split, small_path=small_path,
+                                shared_fifo=fifo)
     assert status == 0
     assert canon(got) == canon(want)
     assert cnt["tasks"] == st["tasks"]
