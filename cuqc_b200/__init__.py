@@ -39,7 +39,7 @@ EXPORTS = [
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
     "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune", "qc_maximal_sets",
     "qc_context_last_stats", "qc_root", "qc_mine_shard", "qc_graph_read_binary",
-    "qc_graph_write_binary", "qc_graph_read",
+    "qc_graph_write_binary", "qc_graph_read", "qc_tune_batch",
 ]
 
 
@@ -124,6 +124,8 @@ def lib():
         L.qc_result_write.argtypes = [vp, C.c_char_p]
         L.qc_result_free.argtypes = [vp]
         L.qc_tune.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.POINTER(Config)]
+        L.qc_tune_batch.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_double), P32, C.c_int32,
+                                    C.c_int32, C.POINTER(Config)]
         L.qc_twohop_noalloc.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_int64, P64, vp]
         L.qc_twohop_noalloc_max_vertices.restype = C.c_int32
         L.qc_maximal_sets.argtypes = [vp, P32, C.c_int64, C.c_int32, C.POINTER(vp)]
@@ -336,8 +338,20 @@ class Context:
         _check(lib().qc_tune(self.h, dg.h, float(gamma), int(min_size), int(repeats),
                              C.byref(best)))
         self.cfg = best
-        return {"warps_per_block": best.warps_per_block, "blocks_per_sm": best.blocks_per_sm,
-                "split": best.split}
+        return _tuned(best)
+
+    def tune_batch(self, gs, gammas, min_sizes, repeats=1):
+        """qc_tune on a batched workload (qc_tune_batch); returns the settings."""
+        dgs = [g if isinstance(g, DeviceGraph) else DeviceGraph.from_graph(g) for g in gs]
+        k = len(dgs)
+        ga = (C.c_void_p * k)(*[d.h for d in dgs])
+        gm = np.ascontiguousarray(gammas, np.float64)
+        ms = np.ascontiguousarray(min_sizes, np.int32)
+        best = Config()
+        _check(lib().qc_tune_batch(self.h, ga, gm.ctypes.data_as(C.POINTER(C.c_double)), _p32(ms),
+                                   k, int(repeats), C.byref(best)))
+        self.cfg = best
+        return _tuned(best)
 
     def mine_batch(self, gs, gammas, min_sizes):
         L = lib()
@@ -369,6 +383,11 @@ class Context:
 
     def __exit__(self, *a):
         self.close()
+
+
+def _tuned(cfg):
+    return {k: getattr(cfg, k) for k in ("warps_per_block", "blocks_per_sm", "split",
+                                         "stage_max", "shared_order")}
 
 
 def mine(g, gamma, min_size, **kw):

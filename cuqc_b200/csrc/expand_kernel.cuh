@@ -196,22 +196,6 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
     return T;
 }
 
-// Copy a record's body (ids, l2, A1, A2) into this warp's shared-memory
-// buffer with 16-byte loads through L2 and point the view there.
-__device__ QC_BIG_FN void stage_record(const ExpandParams& P, TaskView& T, char* buf)
-{
-    const char* src = P.arena + T.rec + rec_ids_off();
-    const uint64_t body = rec_bytes(T.t, T.W) - rec_ids_off(); // multiple of 16
-    const uint4* s4 = (const uint4*)src;
-    uint4* d4 = (uint4*)buf;
-    for (uint64_t i = lane_id(); i < body / 16; i += 32) d4[i] = __ldcg(s4 + i);
-    __syncwarp();
-    char* b = buf - rec_ids_off(); // same offsets as in the record
-    T.ids = (const int32_t*)(b + rec_ids_off());
-    T.l2 = (int32_t*)(b + rec_l2_off(T.t));
-    T.A1 = (const uint32_t*)(b + rec_a1_off(T.t));
-    T.A2 = (const uint32_t*)(b + rec_a2_off(T.t, T.W));
-}
 
 // A warp's workspace: one base pointer and the byte offsets of its arrays
 // (laid out by ws_layout), so the whole view fits in a few registers.
@@ -1991,6 +1975,92 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
     return pushed;
 }
 
+#ifndef QC_EMULATION
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+// this warp's mbarrier for its bulk copies (one arrival: lane 0's)
+__device__ __forceinline__ void stage_bar_init(WarpSmem* sm)
+{
+    if (lane_id() == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&sm->stage_bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        sm->stage_phase = 0;
+    }
+    __syncwarp();
+}
+// has the bulk copy of the given parity landed?
+__device__ __forceinline__ bool stage_bar_done(WarpSmem* sm, int phase)
+{
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(&sm->stage_bar)), "r"(phase)
+                 : "memory");
+    return ok != 0;
+}
+#endif
+
+// Copy a record's body (ids, l2, A1, A2) into this warp's shared-memory
+// buffer and point the view there.  On the device one bulk copy by the TMA
+// unit (cp.async.bulk, global -> shared, completing on the warp's mbarrier;
+// the body and both addresses are 16-byte multiples); in the CPU emulator
+// 16-byte loads through L2.  Returns false if the copy did not land within
+// the run's wait limit (the run then stops).
+__device__ QC_BIG_FN bool stage_record(const ExpandParams& P, WarpSmem* sm, TaskView& T, char* buf)
+{
+    const char* src = P.arena + T.rec + rec_ids_off();
+    const uint64_t body = rec_bytes(T.t, T.W) - rec_ids_off(); // multiple of 16
+#ifndef QC_EMULATION
+    const int phase = sm->stage_phase;
+    if (lane_id() == 0) {
+        // earlier reads of the buffer (generic proxy) and the record's writes
+        // by other warps ordered before the copy (async proxy)
+        asm volatile("fence.proxy.async;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     ::"r"(smem_addr(&sm->stage_bar)), "r"((unsigned)body) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(smem_addr(buf)), "l"(src), "r"((unsigned)body), "r"(smem_addr(&sm->stage_bar))
+                     : "memory");
+    }
+    bool done = stage_bar_done(sm, phase);
+    if (!done) {
+        const unsigned long long t0 = now_ns();
+        while (!(done = stage_bar_done(sm, phase))) {
+            if (now_ns() - t0 > (unsigned long long)P.wait_ns) break;
+        }
+    }
+    if (!__all_sync(QC_FULL, done)) {
+        if (lane_id() == 0) {
+            set_status(P, ST_ITER_LIMIT);
+            P.ctl->wait_fail_where = 5;
+        }
+        // the copy may still land: wait for it once more, again bounded,
+        // before the buffer can be reused
+        const unsigned long long t1 = now_ns();
+        while (!stage_bar_done(sm, phase) && now_ns() - t1 <= (unsigned long long)P.wait_ns) {
+        }
+        return false;
+    }
+    __syncwarp();
+    if (lane_id() == 0) sm->stage_phase = phase ^ 1;
+    __syncwarp();
+#else
+    const uint4* s4 = (const uint4*)src;
+    uint4* d4 = (uint4*)buf;
+    for (uint64_t i = lane_id(); i < body / 16; i += 32) d4[i] = __ldcg(s4 + i);
+    __syncwarp();
+#endif
+    char* b = buf - rec_ids_off(); // same offsets as in the record
+    T.ids = (const int32_t*)(b + rec_ids_off());
+    T.l2 = (int32_t*)(b + rec_l2_off(T.t));
+    T.A1 = (const uint32_t*)(b + rec_a1_off(T.t));
+    T.A2 = (const uint32_t*)(b + rec_a2_off(T.t, T.W));
+    return true;
+}
+
 // ------------------------------------------------------------------
 // a work item: fresh task (lookahead, branch range) or a branch range
 // ------------------------------------------------------------------
@@ -2008,7 +2078,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     const int t = T.t, W = T.W, m = T.m;
     int lane = lane_id();
     const bool staged = stage != nullptr && t > 32 && t <= P.smem_t && t <= P.max_t;
-    if (staged) stage_record(P, T, stage);
+    if (staged && !stage_record(P, wss.sm, T, stage)) return it.q_lo >= 0; // the run is stopping
     Ws ws = staged ? wss : wsg;
     Rules R = P.rules[T.inst];
     if (ws.sm->tab_inst != T.inst) {
@@ -2261,6 +2331,9 @@ __global__ void expand_kernel(ExpandParams P)
         sm->fcount[c] = 0;
     }
     __syncwarp();
+#ifndef QC_EMULATION
+    if (stage) stage_bar_init(sm);
+#endif
     for (;;) {
         WorkItem it;
         TaskHdr hv{};

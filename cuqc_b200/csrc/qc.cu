@@ -1013,52 +1013,125 @@ extern "C" qc_status qc_root(qc_context* c, const qc_graph* g, double gamma, int
 // main.cu:21-55)
 // ------------------------------------------------------------------
 
-extern "C" qc_status qc_tune(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
-                             int32_t repeats, qc_config* best)
+// The search behind qc_tune and qc_tune_batch.  `run(kernel_ms, nsets)` mines
+// the sample workload once with ctx->cfg.  First the launch shape (warps per
+// block, blocks per SM, branches per work item of a large task), then, from
+// the best shape, the largest task staged in shared memory (beyond it task
+// records are read through L2) and the order idle warps take donated tasks
+// in, one knob at a time.  Every run must give the same number of sets.
+template <class Run>
+static qc_status tune_search(qc_context* ctx, int32_t repeats, Run run, qc_config* best)
 {
-    if (!ctx || !g) return fail(QC_ERR_ARGS, "NULL argument");
-    if (!(gamma >= 0.5 && gamma <= 1.0))
-        return fail(QC_ERR_ARGS, "minimum degree ratio must be between .5 and 1 inclusive");
-    if (min_size <= 1) return fail(QC_ERR_ARGS, "minimum size must be greater than 1");
-    if (g->h.off2.size() != g->h.off.size()) return fail(QC_ERR_FORMAT, "graph has no 2-hop lists");
     if (repeats < 1) repeats = 2;
-    static const int32_t kWpb[] = {2, 4, 8};
-    static const int32_t kBps[] = {1, 2};
-    static const int32_t kSplit[] = {1, 2, 4};
     const qc_config keep = ctx->cfg;
     qc_config chosen = keep;
     double best_ms = 1e300;
     int64_t want_sets = -1;
+    auto time_cfg = [&](const qc_config& cfg, double& t) -> qc_status {
+        ctx->cfg = cfg;
+        t = 1e300;
+        for (int32_t rep = 0; rep <= repeats; rep++) { // the first run warms up
+            double ms = 0;
+            int64_t nsets = 0;
+            qc_status st = run(ms, nsets);
+            if (st != QC_OK) return st;
+            if (want_sets < 0) want_sets = nsets;
+            if (nsets != want_sets) return fail(QC_ERR_CUDA, "tuning runs disagree on the result");
+            if (rep > 0) t = std::min(t, ms);
+        }
+        return QC_OK;
+    };
+    auto consider = [&](const qc_config& cfg) -> qc_status {
+        double t = 0;
+        qc_status st = time_cfg(cfg, t);
+        if (st != QC_OK) return st;
+        if (t < best_ms) {
+            best_ms = t;
+            chosen = cfg;
+        }
+        return QC_OK;
+    };
+    static const int32_t kWpb[] = {4, 8};
+    static const int32_t kBps[] = {1, 2};
+    static const int32_t kSplit[] = {2, 4};
     for (int32_t wpb : kWpb)
         for (int32_t bps : kBps)
             for (int32_t split : kSplit) {
-                ctx->cfg = keep;
-                ctx->cfg.warps_per_block = wpb;
-                ctx->cfg.blocks_per_sm = bps;
-                ctx->cfg.split = split;
-                double t = 1e300;
-                for (int32_t rep = 0; rep <= repeats; rep++) { // first run warms up
-                    qc_result r;
-                    qc_status st = mine_one(ctx, g, gamma, min_size, &r);
-                    if (st != QC_OK) {
-                        ctx->cfg = keep;
-                        return st;
-                    }
-                    if (want_sets < 0) want_sets = r.nsets;
-                    if (r.nsets != want_sets) {
-                        ctx->cfg = keep;
-                        return fail(QC_ERR_CUDA, "tuning runs disagree on the result");
-                    }
-                    if (rep > 0) t = std::min(t, r.st.kernel_ms);
-                }
-                if (t < best_ms) {
-                    best_ms = t;
-                    chosen = ctx->cfg;
+                qc_config cfg = keep;
+                cfg.warps_per_block = wpb;
+                cfg.blocks_per_sm = bps;
+                cfg.split = split;
+                qc_status st = consider(cfg);
+                if (st != QC_OK) {
+                    ctx->cfg = keep;
+                    return st;
                 }
             }
+    const qc_config shape = chosen;
+    for (int32_t stage : {64, -1}) {
+        qc_config cfg = shape;
+        cfg.stage_max = stage;
+        qc_status st = consider(cfg);
+        if (st != QC_OK) {
+            ctx->cfg = keep;
+            return st;
+        }
+    }
+    const qc_config staged = chosen;
+    for (int32_t order : {1, 2}) {
+        qc_config cfg = staged;
+        cfg.shared_order = order;
+        qc_status st = consider(cfg);
+        if (st != QC_OK) {
+            ctx->cfg = keep;
+            return st;
+        }
+    }
     ctx->cfg = chosen;
     if (best) *best = chosen;
     return QC_OK;
+}
+
+extern "C" qc_status qc_tune(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
+                             int32_t repeats, qc_config* best)
+{
+    if (!ctx || !g) return fail(QC_ERR_ARGS, "NULL argument");
+    qc_status st = check_mine_args(g, gamma, min_size);
+    if (st != QC_OK) return st;
+    return tune_search(ctx, repeats, [&](double& ms, int64_t& nsets) -> qc_status {
+        qc_result r;
+        qc_status s2 = mine_one(ctx, g, gamma, min_size, &r);
+        ms = r.st.kernel_ms;
+        nsets = r.nsets;
+        return s2;
+    }, best);
+}
+
+static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const double* gammas,
+                            const int32_t* min_sizes, int32_t count, std::vector<qc_result*>& res);
+
+extern "C" qc_status qc_tune_batch(qc_context* ctx, const qc_graph* const* graphs,
+                                   const double* gammas, const int32_t* min_sizes, int32_t count,
+                                   int32_t repeats, qc_config* best)
+{
+    if (!ctx || !graphs || !gammas || !min_sizes || count < 1) return fail(QC_ERR_ARGS, "bad arguments");
+    for (int32_t i = 0; i < count; i++) {
+        if (!graphs[i]) return fail(QC_ERR_ARGS, "NULL graph in batch");
+        qc_status st = check_mine_args(graphs[i], gammas[i], min_sizes[i]);
+        if (st != QC_OK) return st;
+    }
+    return tune_search(ctx, repeats, [&](double& ms, int64_t& nsets) -> qc_status {
+        std::vector<qc_result*> res;
+        qc_status s2 = mine_batch(ctx, graphs, gammas, min_sizes, count, res);
+        ms = 0;
+        nsets = 0;
+        if (s2 == QC_OK && !res.empty()) ms = res[0]->st.kernel_ms;
+        for (auto* r : res) {
+            if (r) nsets += r->nsets;
+            delete r;
+        }
+        return s2;
+    }, best);
 }
 
 // ------------------------------------------------------------------

@@ -228,6 +228,9 @@ struct WarpSmem {
     int32_t eset[kEmitSets];       // start of each buffered set in ebuf
     int32_t en, es;                // ints and sets buffered
     unsigned long long deadline;   // globaltimer value to stop at (0: none)
+    unsigned long long stage_bar;  // mbarrier of this warp's bulk copies into its stage buffer
+    int32_t stage_phase;           // parity of the next completion of stage_bar
+    int32_t pad_;
 };
 
 // Per-warp workspace (global memory) for the bit-matrix path, tasks of up

@@ -242,15 +242,26 @@ qc_status qc_context_last_stats(const qc_context* ctx, qc_stats* out);
 qc_status qc_mine(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
                   int32_t sched, qc_result** out);
 
-/* Pick the launch shape (warps per block, blocks per SM, branches per work
- * item) for this device and workload: mines (g, gamma, min_size) with every
- * candidate shape, `repeats` timed runs each after one warm-up, keeps the
- * fastest expansion kernel, stores it in the context's configuration and, if
- * `best` is not NULL, copies it there.  Every run must give the same result.
- * Replaces the reference's compile-time launch constants (BLOCK_SIZE,
+/* Pick the launch settings for this device and workload: mines (g, gamma,
+ * min_size) with every candidate launch shape (warps per block, blocks per
+ * SM, branches per work item of a task over 32 vertices), then, from the
+ * fastest, tries the largest task staged in shared memory (larger task
+ * records are read through L2: the spill threshold) and the order in which
+ * idle warps take donated tasks; `repeats` timed runs each after one
+ * warm-up, the fastest expansion kernel kept in the context's configuration
+ * and, if `best` is not NULL, copied there.  Every run must give the same
+ * result.  Replaces the reference's compile-time constants (BLOCK_SIZE,
  * NUM_OF_BLOCKS, TASKS_PER_WARP, EXPAND_THRESHOLD, main.cu:21-55). */
 qc_status qc_tune(qc_context* ctx, const qc_graph* g, double gamma, int32_t min_size,
                   int32_t repeats, qc_config* best);
+
+/* qc_tune on a sample of a batched workload: the same search, each candidate
+ * timed by one qc_mine_batch of the `count` instances (the batched launch's
+ * best shape differs from a single instance's: its many instances keep every
+ * warp busy, so throughput settings win over latency ones). */
+qc_status qc_tune_batch(qc_context* ctx, const qc_graph* const* graphs, const double* gammas,
+                        const int32_t* min_sizes, int32_t count, int32_t repeats,
+                        qc_config* best);
 
 /* Mine `count` independent instances in one persistent launch (each with
  * its own graph, gamma and min_size).  outs[i] receives instance i's result. */

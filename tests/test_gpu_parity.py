@@ -223,9 +223,23 @@ def test_tune_picks_a_shape_and_keeps_results():
     want = oracle.solve(g, 0.8, 10)[0]
     with Q.Context(device=0) as c:
         best = c.tune(g, 0.8, 10, repeats=1)
-        assert best["warps_per_block"] in (2, 4, 8) and best["blocks_per_sm"] in (1, 2)
-        assert best["split"] in (1, 2, 4)
+        assert best["warps_per_block"] in (4, 8) and best["blocks_per_sm"] in (1, 2)
+        assert best["split"] in (2, 4) and best["stage_max"] in (0, 64, -1)
+        assert best["shared_order"] in (0, 1, 2)
         assert c.mine(g, 0.8, 10).sets == want
+
+
+def test_tune_batch_picks_settings_and_keeps_results():
+    specs = _batch_specs(900, 12)
+    gs = [x[0] for x in specs]
+    gms = [x[1] for x in specs]
+    mss = [x[2] for x in specs]
+    with Q.Context(device=0) as c:
+        best = c.tune_batch(gs, gms, mss, repeats=1)
+        assert best["warps_per_block"] in (4, 8) and best["split"] in (2, 4)
+        res = c.mine_batch(gs, gms, mss)
+    for (g, gm, ms), r in zip(specs, res):
+        assert r.sets == oracle.solve(g, gm, ms)[0]
 
 
 def test_freed_graph_buffers_are_reused_correctly():
