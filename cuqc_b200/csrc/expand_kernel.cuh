@@ -36,6 +36,12 @@ namespace qcb {
 #ifndef QC_SMALL_FN
 #define QC_SMALL_FN
 #endif
+#ifndef QC_PRUNE_FN
+#define QC_PRUNE_FN QC_BIG_FN
+#endif
+#ifndef QC_BOUNDS_FN
+#define QC_BOUNDS_FN QC_BIG_FN
+#endif
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
@@ -312,7 +318,7 @@ __device__ __forceinline__ bool vert_extendable(const Rules& R, int in, int ex, 
 // only those passing validity under `b`), then prefix tables over bins in
 // descending value order: pcnt[j] = #values > vmax-j, psum[j] = their sum.
 // Values are bounded by vmax (members count).  Returns the number of values.
-__device__ QC_BIG_FN int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* cm, int t, int vmax,
+__device__ QC_BOUNDS_FN int build_hist(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* cm, int t, int vmax,
                           bool filter_valid, int m, const Bounds& b)
 {
     int lane = lane_id();
@@ -377,7 +383,7 @@ __device__ __forceinline__ long long top_sum(const Ws& ws, int vmax, int k)
 // The candidate histogram must be built.  Returns true when invalid.
 // ------------------------------------------------------------------
 
-__device__ QC_BIG_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
+__device__ QC_BOUNDS_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws& ws, const uint32_t* mm, int t, int m,
                           int ncand, int vmax, Bounds& b)
 {
     int lane = lane_id();
@@ -559,7 +565,7 @@ __device__ QC_BIG_FN void filter_valid(const ExpandParams& P, const Rules& R, Ws
 
 enum { DP_DONE = 0, DP_INVALID = 1, DP_SWITCH = 2 };
 
-__device__ QC_BIG_FN int degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
+__device__ QC_PRUNE_FN int degree_prune(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
                             int m, const uint32_t* Call, const uint32_t* D, uint32_t* Rm,
                             Bounds& b, bool may_switch)
 {
@@ -2013,7 +2019,7 @@ __device__ QC_BIG_FN bool stage_record(const ExpandParams& P, WarpSmem* sm, Task
 {
     const char* src = P.arena + T.rec + rec_ids_off();
     const uint64_t body = rec_bytes(T.t, T.W) - rec_ids_off(); // multiple of 16
-#ifndef QC_EMULATION
+#if !defined(QC_EMULATION) && !defined(QC_STAGE_LOOP)
     const int phase = sm->stage_phase;
     if (lane_id() == 0) {
         // earlier reads of the buffer (generic proxy) and the record's writes
