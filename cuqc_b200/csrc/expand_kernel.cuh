@@ -257,56 +257,67 @@ struct Bounds {
 // gamma tables (main.cu:526-533, 2144-2151)
 // ------------------------------------------------------------------
 
-// The shared-memory copies hold entries [0, kTabCache), padded past the
-// table's end with its last entry, so an index in that range needs no clamp.
-__device__ __noinline__ int md_far(const Rules& R, int k)
+// Each warp keeps shared-memory copies of entries [0, kTabCache) of md and
+// ubt, padded past the table's end with its last entry.  A lookup clamps the
+// index to the table and reads the copy or, past it, the global table; both
+// loads are plain predicated instructions (no call, no divergent branch).
+__device__ __forceinline__ int tab_far(const int32_t* tab_s, const int32_t* tab, int len, int k)
 {
-    k = k < 0 ? 0 : k;
-    k = k >= R.mdlen ? R.mdlen - 1 : k;
-    return __ldg(R.md + k);
+    k = k < 0 ? 0 : (k >= len ? len - 1 : k);
+    return k < kTabCache ? tab_s[k] : __ldg(tab + k);
 }
-__device__ __noinline__ int ubt_far(const Rules& R, int d)
+// `Near` lookups read the copy alone: on the register path members and
+// candidates number at most 32, so every index is below 96, and an index at
+// or below min_size goes through md_min.
+__device__ __forceinline__ int tab_near(const int32_t* tab, int k)
 {
-    d = d < 0 ? 0 : d;
-    d = d >= R.mdlen ? R.mdlen - 1 : d;
-    return __ldg(R.ubt + d);
+    k = k < 0 ? 0 : (k >= kTabCache ? kTabCache - 1 : k);
+    return tab[k];
 }
+template <bool Near = false>
 __device__ __forceinline__ int md_at(const Rules& R, int k)
 {
-    return (unsigned)k < (unsigned)kTabCache ? R.md_s[k] : md_far(R, k);
+    if (Near) return tab_near(R.md_s, k);
+    return tab_far(R.md_s, R.md, R.mdlen, k);
 }
+template <bool Near = false>
 __device__ __forceinline__ int mindeg(const Rules& R, int k)
 {
+    if (Near) return k < R.min_size ? R.md_min : tab_near(R.md_s, k);
     return md_at(R, k < R.min_size ? R.min_size : k);
 }
+template <bool Near = false>
 __device__ __forceinline__ int ubt_at(const Rules& R, int d)
 {
-    return (unsigned)d < (unsigned)kTabCache ? R.ubt_s[d] : ubt_far(R, d);
+    if (Near) return tab_near(R.ubt_s, d);
+    return tab_far(R.ubt_s, R.ubt, R.mdlen, d);
 }
 
 // main.cu:2167-2178
+template <bool Near = false>
 __device__ __forceinline__ bool cand_valid(const Rules& R, int in, int ex, int m,
                                            const Bounds& b)
 {
     int tot = in + ex;
-    if (tot < md_at(R, R.min_size)) return false;
-    if (tot < mindeg(R, m + ex + 1)) return false;
+    if (tot < R.md_min) return false;
+    if (tot < mindeg<Near>(R, m + ex + 1)) return false;
     if (tot < b.med) return false;
-    if (in + b.U - 1 < md_at(R, m + b.L)) return false;
-    if (tot < mindeg(R, m + b.L)) return false;
+    if (in + b.U - 1 < md_at<Near>(R, m + b.L)) return false;
+    if (tot < mindeg<Near>(R, m + b.L)) return false;
     return true;
 }
 // main.cu:2180-2198
+template <bool Near = false>
 __device__ __forceinline__ bool vert_extendable(const Rules& R, int in, int ex, int m,
                                                 const Bounds& b)
 {
     int tot = in + ex;
-    if (tot < md_at(R, R.min_size)) return false;
-    if (tot < mindeg(R, m + ex)) return false;
+    if (tot < R.md_min) return false;
+    if (tot < mindeg<Near>(R, m + ex)) return false;
     if (tot < b.med) return false;
-    if (ex == 0 && in < mindeg(R, m + ex)) return false;
-    if (in + b.U < md_at(R, m + b.U)) return false;
-    if (tot < mindeg(R, m + b.L)) return false;
+    if (ex == 0 && in < mindeg<Near>(R, m + ex)) return false;
+    if (in + b.U < md_at<Near>(R, m + b.U)) return false;
+    if (tot < mindeg<Near>(R, m + b.L)) return false;
     return true;
 }
 
@@ -973,20 +984,26 @@ __device__ void schedule_child(const ExpandParams& P, Ws& ws, unsigned long long
 #define QC_EAGER_HUNGRY 4
 #endif
 constexpr int kEagerHungry = QC_EAGER_HUNGRY;
+// tasks a warp keeps on its own stack when it donates between a small task's
+// branches (it has branches left to run, so it may give away all of them)
+#ifndef QC_EAGER_KEEP
+#define QC_EAGER_KEEP 1
+#endif
+constexpr int kEagerKeep = QC_EAGER_KEEP;
 
 // Whole warp: while other warps wait for work, hand them all but the newest
 // task of this warp's own stack, oldest (shallowest, usually largest) first,
 // in bundles sized so each waiting warp can take one.  Lane b pushes bundle b
 // to shard (home + b), so the pushes' round trips overlap.
-__device__ QC_SMALL_FN void donate(const ExpandParams& P, Ws& ws)
+__device__ QC_SMALL_FN void donate(const ExpandParams& P, Ws& ws, int keep = 1)
 {
     const int lane = lane_id();
     __syncwarp(); // lane 0's stack and counters written before the call
     const int n = ws.sm->lcount;
     // read when the previous item started (the read overlapped its work)
     const int hungry = ws.sm->hungry;
-    if (n < 2 || hungry <= 0) return;
-    const int give = n - 1;
+    if (n <= keep || hungry <= 0) return;
+    const int give = n - keep;
     int per = (give + hungry - 1) / hungry;
     per = per < 1 ? 1 : (per > kBundle ? kBundle : per);
     int nb = (give + per - 1) / per;
@@ -1029,6 +1046,9 @@ __device__ QC_SMALL_FN void donate(const ExpandParams& P, Ws& ws)
 
 constexpr unsigned long long kOffMask = (1ull << 40) - 1;
 
+// the size class of every record of at most 32 vertices (rec_block_bytes)
+__device__ __forceinline__ int small_class() { return arena_class(rec_bytes(32, 1)); }
+
 __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigned long long bytes, int& cls)
 {
     cls = arena_class(bytes);
@@ -1037,6 +1057,15 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigne
         return ~0ull;
     }
     unsigned long long size = arena_class_bytes(cls);
+    // small records: this warp's array of free blocks in shared memory
+    if (cls == small_class() && ws.sm->nsfree > 0) {
+        const unsigned long long off = ws.sm->sfree[--ws.sm->nsfree];
+        if ((off & 15ull) != 0 || off + size > P.arena_cap) {
+            check_fail(P, 13, off); // a free block outside the arena
+            return ~0ull;
+        }
+        return off;
+    }
     // this warp's own free list: blocks it freed itself, no other warp touches it
     if (ws.sm->fcount[cls] > 0) {
         unsigned long long off = (ws.sm->fhead[cls] - 1) * 16;
@@ -1098,6 +1127,11 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigne
 // kPrivateFreeCap blocks; beyond that, to the shared lock-free list.
 __device__ void arena_free(const ExpandParams& P, Ws& ws, unsigned long long off, int cls)
 {
+    if (cls == small_class() && ws.sm->nsfree < kSmallFree) {
+        ((TaskHdr*)(P.arena + off))->refs = kFreeMagic; // a stale item on it fails its check
+        ws.sm->sfree[ws.sm->nsfree++] = off;
+        return;
+    }
     if (ws.sm->fcount[cls] < kPrivateFreeCap) {
         *(unsigned long long*)(P.arena + off) = ws.sm->fhead[cls];
         ((TaskHdr*)(P.arena + off))->refs = kFreeMagic;
@@ -1216,7 +1250,7 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     __syncwarp();
     sort_keys(ws, tc);
     int Wc = words_for(tc);
-    unsigned long long bytes = rec_bytes(tc, Wc);
+    unsigned long long bytes = rec_block_bytes(tc, Wc);
     unsigned long long at = 0;
     int cls = 0;
     if (lane == 0) at = arena_alloc(P, ws, bytes, cls);
@@ -1518,23 +1552,23 @@ __device__ QC_SMALL_FN bool lu_small(const ExpandParams& P, const Rules& R, unsi
     int min_in_ex = rmin(mem && in == min_in ? ex : 0x7fffffff);
     int ncand = __popc(cs);
     bool invalid = false;
-    b.med = mindeg(R, m + 1);
-    if (min_in < md_at(R, m)) {
-        int lb = mindeg(R, m) - min_in;
+    b.med = mindeg<true>(R, m + 1);
+    if (min_in < md_at<true>(R, m)) {
+        int lb = mindeg<true>(R, m) - min_in;
         for (int base = lb;; base += 32) {
             int L = base + lane;
-            bool cont = (L <= min_in_ex) && (min_in + L < md_at(R, m + L));
+            bool cont = (L <= min_in_ex) && (min_in + L < md_at<true>(R, m + L));
             unsigned stop = __ballot_sync(QC_FULL, !cont);
             if (stop) {
                 lb = base + __ffs(stop) - 1;
                 break;
             }
         }
-        if (min_in + lb < md_at(R, m + lb)) {
+        if (min_in + lb < md_at<true>(R, m + lb)) {
             lb = ncand + 1;
             invalid = true;
         }
-        int ub = ubt_at(R, min_tot) + 1 - m;
+        int ub = ubt_at<true>(R, min_tot) + 1 - m;
         if (ub > ncand) ub = ncand;
         if (lb < ub) {
             // S(k) for k = lane: sum of the k largest candidate indegrees
@@ -1544,22 +1578,22 @@ __device__ QC_SMALL_FN bool lu_small(const ExpandParams& P, const Rules& R, unsi
             int k = lane;
             long long Sk = excl;
             bool g = (k >= lb && k <= ub) &&
-                     (k == ub || (long long)sum_in + Sk >= (long long)m * md_at(R, m + k));
+                     (k == ub || (long long)sum_in + Sk >= (long long)m * md_at<true>(R, m + k));
             unsigned bal = __ballot_sync(QC_FULL, g);
             int idx = bal ? __ffs(bal) - 1 : ub;
             // idx <= ub <= ncand < 32: a task of at most 32 vertices has a member
             long long Sidx = __shfl_sync(QC_FULL, excl, idx & 31);
-            if ((long long)sum_in + Sidx < (long long)m * md_at(R, m + idx)) {
+            if ((long long)sum_in + Sidx < (long long)m * md_at<true>(R, m + idx)) {
                 lb = ub + 1;
                 invalid = true;
             } else {
                 lb = idx;
                 bool g2 = (k > idx && k <= ub) &&
-                          ((long long)sum_in + Sk >= (long long)m * md_at(R, m + k));
+                          ((long long)sum_in + Sk >= (long long)m * md_at<true>(R, m + k));
                 unsigned b2 = __ballot_sync(QC_FULL, g2);
                 int tub = b2 ? 31 - __clz(b2) : idx;
                 if (ub > tub) ub = tub;
-                if (lb > 1) b.med = mindeg(R, m + lb);
+                if (lb > 1) b.med = mindeg<true>(R, m + lb);
             }
         }
         b.U = ub;
@@ -1581,10 +1615,10 @@ __device__ QC_SMALL_FN bool prune_loop_small(const ExpandParams& P, const Rules&
     int lane = lane_id();
     while (Rm && X) {
         ex = __popc(a1 & Rm);
-        unsigned V = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid(R, in, ex, m, b));
+        unsigned V = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid<true>(R, in, ex, m, b));
         if (lu_small(P, R, M, m, V, in, ex, b)) return true;
-        if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(R, in, ex, m, b))) return true;
-        unsigned R2 = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid(R, in, ex, m, b));
+        if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable<true>(R, in, ex, m, b))) return true;
+        unsigned R2 = __ballot_sync(QC_FULL, in_set(Rm, lane) && cand_valid<true>(R, in, ex, m, b));
         X = Rm & ~R2;
         Rm = R2;
     }
@@ -1597,8 +1631,8 @@ __device__ bool prune_small(const ExpandParams& P, const Rules& R, unsigned a1, 
 {
     int lane = lane_id();
     if (lu_small(P, R, M, m, D, in, ex, b)) return true;
-    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable(R, in, ex, m, b))) return true;
-    Rm = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid(R, in, ex, m, b));
+    if (__any_sync(QC_FULL, in_set(M, lane) && !vert_extendable<true>(R, in, ex, m, b))) return true;
+    Rm = __ballot_sync(QC_FULL, in_set(D, lane) && cand_valid<true>(R, in, ex, m, b));
     return prune_loop_small(P, R, a1, M, m, Rm, Call & ~Rm, in, ex, b);
 }
 
@@ -1655,7 +1689,7 @@ __device__ __forceinline__ void clique_small(const ExpandParams& P, const Rules&
                                              int id)
 {
     int lane = lane_id();
-    int need = md_at(R, m);
+    int need = md_at<true>(R, m);
     if (!__any_sync(QC_FULL, in_set(M, lane) && in < need)) emit_small(P, R, ws, M, id);
 }
 
@@ -1695,7 +1729,7 @@ __device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, W
         c1 |= ((sa1 >> pj) & 1u) << j;
         c2 |= ((sa2 >> pj) & 1u) << j;
     }
-    unsigned long long bytes = rec_bytes(tc, 1);
+    unsigned long long bytes = rec_block_bytes(tc, 1);
     unsigned long long at = 0;
     int cls = 0;
     if (lane == 0) at = arena_alloc(P, ws, bytes, cls);
@@ -1767,7 +1801,7 @@ __device__ QC_SMALL_FN void branch_tail_small(const ExpandParams& P, const Rules
 {
     int lane = lane_id();
     // critical vertices (main.cu:1526-1707)
-    int critv = md_at(R, m1 + b.L);
+    int critv = md_at<true>(R, m1 + b.L);
     unsigned K = __ballot_sync(QC_FULL, in_set(M1, lane) && in + ex == critv && ex > 0);
     unsigned CA = Rm & ror(in_set(K, lane) ? T.a1 : 0u);
     int nca = __popc(CA);
@@ -1868,6 +1902,11 @@ constexpr int kSmallSplitMin = QC_SMALL_SPLIT_MIN;
 constexpr int kSmallSplitHungry = QC_SMALL_SPLIT_HUNGRY;
 // at most this many branch ranges pushed by one task
 constexpr int kSmallSplitMax = 16;
+// fewest branches in one handed-out range
+#ifndef QC_SMALL_SPLIT_PER
+#define QC_SMALL_SPLIT_PER 4
+#endif
+constexpr int kSmallSplitPer = QC_SMALL_SPLIT_PER;
 
 // A task of at most 32 vertices on the register path.  A fresh task
 // (q_lo < 0) runs its lookahead and finds its branch range; when other warps
@@ -1907,7 +1946,7 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
             if ((unsigned long long)t > ws.sm->cnt.max_task) ws.sm->cnt.max_task = t;
         }
         // lookahead (main.cu:1349-1405)
-        int need_t = md_at(R, t);
+        int need_t = md_at<true>(R, t);
         if (!__any_sync(QC_FULL, in_set(Mm, lane) && in + ex < need_t)) {
             int nc = t - m;
             if (in_set(Cm, lane)) T.l2 = __popc(T.a2 & Cm);
@@ -1919,7 +1958,7 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
             }
         }
         // branches run until a member would fail on removal (main.cu:1092-1099)
-        int need = mindeg(R, m);
+        int need = mindeg<true>(R, m);
         int pos = 0;
         if (in_set(Mm, lane)) {
             int k = need - in;
@@ -1942,7 +1981,7 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
         const int hungry = ws.sm->hungry;
         if (hungry >= kSmallSplitHungry && nb >= kSmallSplitMin) {
             int parts = hungry + 1;
-            parts = parts > nb / 4 ? nb / 4 : parts; // ranges of at least 4 branches
+            parts = parts > nb / kSmallSplitPer ? nb / kSmallSplitPer : parts;
             parts = parts > kSmallSplitMax + 1 ? kSmallSplitMax + 1 : parts;
             const int per = (nb + parts - 1) / parts;
             const int extra = (nb - per + per - 1) / per;
@@ -1973,10 +2012,18 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
     for (int q = qhi; q >= qlo; q--) {
         // a sharded search's root: only this shard's branches
         if (sroot && (t - 1 - q) % P.nshards != P.shard) continue;
+#ifdef QC_EAGER_REFRESH
+        int idle_q = 0;
+        if (lane == 0 && q > qlo) idle_q = *(volatile int*)&P.ctl->idle_warps;
+#endif
         branch_small(P, R, ws, T, q);
+#ifdef QC_EAGER_REFRESH
+        if (lane == 0 && q > qlo) ws.sm->hungry = idle_q;
+        __syncwarp();
+#endif
         // children of this task can go to waiting warps before its last branch
         // when many warps wait (not for the odd one that will soon get work)
-        if (q > qlo && ws.sm->hungry >= kEagerHungry) donate(P, ws);
+        if (q > qlo && ws.sm->hungry >= kEagerHungry) donate(P, ws, kEagerKeep);
     }
     return pushed;
 }
@@ -2100,6 +2147,7 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     }
     R.md_s = ws.sm->md;
     R.ubt_s = ws.sm->ubt;
+    R.md_min = md_at(R, R.min_size);
     bool shared = it.q_lo >= 0;
     if (!(t <= 32 && P.small_path)) { // the register path checks its own ids
         int bad = 0;
@@ -2336,6 +2384,7 @@ __global__ void expand_kernel(ExpandParams P)
         sm->fhead[c] = 0;
         sm->fcount[c] = 0;
     }
+    if (lane == 0) sm->nsfree = 0;
     __syncwarp();
 #ifndef QC_EMULATION
     if (stage) stage_bar_init(sm);

@@ -679,7 +679,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaMemsetAsync(c->slot.p, 0, sizeof(int32_t) * (size_t)c->stack_slots, s));
 
         uint64_t rb = rec_bytes(t, W);
-        const int root_cls = arena_class(rb);
+        const int root_cls = arena_class(rec_block_bytes(t, W));
         const uint64_t root_block = arena_class_bytes(root_cls);
         if ((int64_t)root_block > c->arena_bytes) {
             c->arena_bytes = (int64_t)root_block * 4;
@@ -1339,7 +1339,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         M.W = words_for(M.t);
         M.cov = root_cov[(size_t)i];
         M.inst = i;
-        M.cls = arena_class(rec_bytes(M.t, M.W));
+        M.cls = arena_class(rec_block_bytes(M.t, M.W));
         M.vbase = rules[i].vbase;
         M.rec = arena_at;
         M.id_at = rules[i].vbase;

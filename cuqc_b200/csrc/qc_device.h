@@ -134,6 +134,13 @@ __host__ __device__ inline uint64_t rec_a2_off(int t, int W) {
 __host__ __device__ inline uint64_t rec_bytes(int t, int W) {
     return rec_a2_off(t, W) + align16(4ull * t * W);
 }
+// Every record of at most 32 vertices gets a block of one size, that of a
+// 32-vertex record, so a block freed by any small task can hold any small
+// child (children are smaller than their parents, and per-size classes
+// would leave the freed blocks in the wrong class).
+__host__ __device__ inline uint64_t rec_block_bytes(int t, int W) {
+    return W == 1 ? rec_bytes(32, 1) : rec_bytes(t, W);
+}
 
 // Per-instance rules: the gamma tables and CSR offsets of one mining
 // instance (a batched launch carries one entry per instance).
@@ -150,6 +157,8 @@ struct Rules {
     int32_t n;           // vertices of the instance (ids must be below it)
     const int32_t* md_s;  // shared-memory copies of md / ubt [0, kTabCache) (set on the
     const int32_t* ubt_s; //   device per warp; null in the table uploaded by the host)
+    int32_t md_min;       // md[min_size] (set on the device with md_s)
+    int32_t pad_;
 };
 
 constexpr int32_t kFreeMagic = 0x7ee7f00d; // refs of a block on a free list
@@ -191,6 +200,10 @@ struct WarpCount {
 // frees to the shared lists.
 constexpr int kPrivateFreeCap = 64;
 
+// Blocks of the small-record class (section below) a warp keeps in shared
+// memory, taken and returned without touching the arena.
+constexpr int kSmallFree = 32;
+
 // Entries of the gamma tables (md, ubt) a warp keeps in shared memory; the
 // tests of tasks up to this size never look further.
 constexpr int kTabCache = 128;
@@ -222,6 +235,8 @@ struct WarpSmem {
     int32_t tab_inst;            // instance whose gamma tables are cached (-1: none)
     unsigned long long fhead[kArenaClasses]; // private free lists: offset/16+1, 0 = empty
     int32_t fcount[kArenaClasses];
+    unsigned long long sfree[kSmallFree]; // free blocks of the small-record class
+    int32_t nsfree, pad2_;
     int32_t md[kTabCache];
     int32_t ubt[kTabCache];
     int32_t ebuf[kEmitInts];       // buffered sets, [k, ids..] each
