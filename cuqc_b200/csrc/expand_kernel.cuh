@@ -389,6 +389,21 @@ __device__ __forceinline__ long long top_sum(const Ws& ws, int vmax, int k)
     return ws.psum()[lo] + (long long)(k - ws.pcnt()[lo]) * (vmax - lo);
 }
 
+// The lower bound's search (main.cu:1877-1890): the first L >= mindeg(m) -
+// min_in with !(L <= min_in_ex && min_in + L < md[m+L]), for members whose
+// smallest indegree is min_in (min_in_ex: the smallest exdegree among them).
+__device__ __forceinline__ int lower_start(const Rules& R, int m, int min_in, int min_in_ex)
+{
+    const int lane = lane_id();
+    int lb = mindeg(R, m) - min_in;
+    for (int base = lb;; base += 32) {
+        int L = base + lane;
+        bool cont = (L <= min_in_ex) && (min_in + L < md_at(R, m + L));
+        unsigned stop = __ballot_sync(QC_FULL, !cont);
+        if (stop) return base + __ffs(stop) - 1;
+    }
+}
+
 // ------------------------------------------------------------------
 // lower / upper bounds (main.cu:1857-1972).  Members: mask mm (m of them).
 // The candidate histogram must be built.  Returns true when invalid.
@@ -427,17 +442,7 @@ __device__ QC_BOUNDS_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws
     bool invalid = false;
     b.med = mindeg(R, m + 1);
     if (min_in < md_at(R, m)) {
-        int lb = mindeg(R, m) - min_in;
-        // first L >= lb with !(L <= min_in_ex && min_in + L < md[m+L])
-        for (int base = lb;; base += 32) {
-            int L = base + lane;
-            bool cont = (L <= min_in_ex) && (min_in + L < md_at(R, m + L));
-            unsigned stop = __ballot_sync(QC_FULL, !cont);
-            if (stop) {
-                lb = base + __ffs(stop) - 1;
-                break;
-            }
-        }
+        int lb = lower_start(R, m, min_in, min_in_ex);
         if (min_in + lb < md_at(R, m + lb)) {
             lb = ncand + 1;
             invalid = true;
@@ -1344,6 +1349,10 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
     const uint32_t* r2q = T.A2 + (int64_t)q * W;
     for (int w = lane; w < W; w += 32) D[w] = PRE[w] & rec_ld(r2q + w);
     __syncwarp();
+    if (lane == 0) {
+        ws.sm->cnt.branches++;
+        ws.sm->cnt.parent_vertices += (unsigned long long)(q + 1);
+    }
     // degrees for members and PRE (add one vertex, main.cu:1465-1492); only the
     // members and the candidates that survive the diameter test are ever read
     {
@@ -1368,10 +1377,6 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
             ws.exdeg()[v] = ex;
         }
         __syncwarp();
-    }
-    if (lane == 0) {
-        ws.sm->cnt.branches++;
-        ws.sm->cnt.parent_vertices += (unsigned long long)(q + 1);
     }
 
     Bounds b = {0, 0, 0};
@@ -1784,6 +1789,9 @@ __device__ void branch_small(const ExpandParams& P, const Rules& R, Ws& ws, cons
             ws.sm->cnt.p_rows += (unsigned long long)rows;
         }
     }
+    // too few candidates survive the diameter test for any set of min_size
+    // (the bounds test finds U <= |D| too small; no clique, m1 < min_size)
+    if (m1 + __popc(D) < R.min_size) return;
     Bounds b = {0, 0, 0};
     unsigned Rm = 0;
     if (prune_small(P, R, T.a1, M1, m1, PRE, D, Rm, in, ex, b)) {
