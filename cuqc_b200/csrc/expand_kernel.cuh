@@ -114,6 +114,7 @@ __device__ __forceinline__ bool bit(const uint32_t* a, int v) { return (a[v >> 5
 // memory is read there.
 __device__ __forceinline__ uint32_t rec_ld(const uint32_t* p) { return __isGlobal(p) ? __ldcg(p) : *p; }
 __device__ __forceinline__ int32_t rec_ld(const int32_t* p) { return __isGlobal(p) ? __ldcg(p) : *p; }
+__device__ __forceinline__ uint8_t rec_ld(const uint8_t* p) { return __isGlobal(p) ? __ldcg(p) : *p; }
 __device__ __forceinline__ bool rec_bit(const uint32_t* a, int v) { return (rec_ld(a + (v >> 5)) >> (v & 31)) & 1u; }
 
 // |record row & mask| over W words (row in a task record, mask in the workspace)
@@ -174,7 +175,7 @@ __device__ __forceinline__ bool bs_empty(const uint32_t* a, int W)
 // ------------------------------------------------------------------
 
 struct TaskView {
-    int t, m, cov, W, inst;
+    int t, m, cov, W, inst, flags;
     const int32_t* ids;
     int32_t* l2;
     const uint32_t* A1;
@@ -193,6 +194,7 @@ __device__ __forceinline__ TaskView task_view(char* arena, unsigned long long re
     T.cov = h.cov;
     T.W = h.W;
     T.inst = h.inst;
+    T.flags = h.flags;
     T.ids = (const int32_t*)(arena + rec + rec_ids_off());
     T.l2 = (int32_t*)(arena + rec + rec_l2_off(T.t));
     T.A1 = (const uint32_t*)(arena + rec + rec_a1_off(T.t));
@@ -854,6 +856,11 @@ __device__ int take_slot(const ExpandParams& P, int s, int idx, StackEntry& out)
 // shard at or after the warp's home shard.  Returns (in every lane) 1 with
 // the entry in lane 0's `out`, 0 when the stack is empty and no warp holds
 // work, -1 on error or abort.
+#ifndef QC_IDLE_BACKOFF_MAX
+#define QC_IDLE_BACKOFF_MAX 4096
+#endif
+constexpr unsigned kIdleBackoffMax = QC_IDLE_BACKOFF_MAX; // ns
+
 __device__ int pop_shared(const ExpandParams& P, StackEntry& out, unsigned long long deadline)
 {
     const int lane = lane_id();
@@ -917,10 +924,10 @@ __device__ int pop_shared(const ExpandParams& P, StackEntry& out, unsigned long 
         done = __shfl_sync(QC_FULL, done, 0);
         if (done == 1) return 0;
         if (done < 0) return -1;
-        // idle: back off (64 ns doubling to ~4 us) so waiting warps leave the
-        // issue slots and the tops' cache line to the working ones
+        // idle: back off (64 ns doubling to kIdleBackoffMax) so waiting warps
+        // leave the issue slots and the tops' cache line to the working ones
         __nanosleep(backoff);
-        backoff = backoff < 4096 ? backoff * 2 : 4096;
+        backoff = backoff < kIdleBackoffMax ? backoff * 2 : kIdleBackoffMax;
     }
 }
 
@@ -961,7 +968,7 @@ __device__ QC_SMALL_FN int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out
 // `pending` counts shared-stack items plus warps that hold work, so local
 // children change it only when they are donated (push_item).
 __device__ void schedule_child(const ExpandParams& P, Ws& ws, unsigned long long rec, int t, int m,
-                               int W, int cls, int inst)
+                               int W, int cls, int inst, int flags)
 {
     if (ws.sm->lcount < kLocalStack) {
         LocalTask lt;
@@ -971,7 +978,7 @@ __device__ void schedule_child(const ExpandParams& P, Ws& ws, unsigned long long
         lt.W = W;
         lt.cls = cls;
         lt.inst = inst;
-        lt.pad = 0;
+        lt.flags = flags;
         ws.sm->lstack[ws.sm->lcount++] = lt;
         return;
     }
@@ -1054,7 +1061,7 @@ constexpr unsigned long long kOffMask = (1ull << 40) - 1;
 // the size class of every record of at most 32 vertices (rec_block_bytes)
 __device__ __forceinline__ int small_class() { return arena_class(rec_bytes(32, 1)); }
 
-__device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigned long long bytes, int& cls)
+__device__ unsigned long long arena_block(const ExpandParams& P, Ws& ws, unsigned long long bytes, int& cls)
 {
     cls = arena_class(bytes);
     if (cls >= kArenaClasses) {
@@ -1125,6 +1132,15 @@ __device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigne
         return ~0ull;
     }
     return at;
+}
+
+// lane 0: a block for a record of `bytes` (class in `cls`); ~0 on failure.
+// A reused block's old contents no longer stand for the warp's newest child.
+__device__ unsigned long long arena_alloc(const ExpandParams& P, Ws& ws, unsigned long long bytes, int& cls)
+{
+    const unsigned long long off = arena_block(P, ws, bytes, cls);
+    if (off == ws.sm->hot_rec) ws.sm->hot_rec = ~0ull;
+    return off;
 }
 
 // lane 0: return a block.  It goes to this warp's private list (reused by the
@@ -1271,7 +1287,7 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
         h->refs = 1;
         h->cls = cls;
         h->inst = T.inst;
-        h->shard_root = 0;
+        h->flags = 0;
     }
     int32_t* cid = (int32_t*)(rec + rec_ids_off());
     int32_t* cl2 = (int32_t*)(rec + rec_l2_off(tc));
@@ -1316,7 +1332,7 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     if (lane == 0) {
         ws.sm->cnt.children++;
         ws.sm->cnt.child_vertices += (unsigned long long)tc;
-        schedule_child(P, ws, at, tc, m, Wc, cls, T.inst);
+        schedule_child(P, ws, at, tc, m, Wc, cls, T.inst, 0);
     }
     __syncwarp();
 }
@@ -1728,6 +1744,12 @@ __device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, W
     unsigned sa1 = __shfl_sync(QC_FULL, T.a1, src);
     unsigned sa2 = __shfl_sync(QC_FULL, T.a2, src);
     int sid = __shfl_sync(QC_FULL, T.id, src);
+    // the child's id ranks from the parent's: a rank counts the larger ids,
+    // parent ranks are distinct, so a child vertex's rank counts the child's
+    // parent ranks below its own
+    const int prank = __shfl_sync(QC_FULL, T.idr, src);
+    const unsigned ranks = ror(lane < tc ? 1u << prank : 0u);
+    const int crank = __popc(ranks & ((1u << prank) - 1u));
     unsigned c1 = 0, c2 = 0;
     for (int j = 0; j < tc; j++) {
         int pj = __shfl_sync(QC_FULL, src, j);
@@ -1750,19 +1772,23 @@ __device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, W
         h->refs = 1;
         h->cls = cls;
         h->inst = T.inst;
-        h->shard_root = 0;
+        h->flags = kFlagRanked;
     }
     if (lane < tc) {
         ((int32_t*)(rec + rec_ids_off()))[lane] = sid;
         ((int32_t*)(rec + rec_l2_off(tc)))[lane] = 0;
         ((uint32_t*)(rec + rec_a1_off(tc)))[lane] = c1;
         ((uint32_t*)(rec + rec_a2_off(tc, 1)))[lane] = c2;
+        ((uint8_t*)(rec + rec_ranks_off()))[lane] = (uint8_t)crank;
     }
+    // the copy the warp reads if this child is its next task
+    ws.sm->hot[lane] = HotLane{sid, c1, c2, crank};
     __syncwarp();
     if (lane == 0) {
+        ws.sm->hot_rec = at;
         ws.sm->cnt.children++;
         ws.sm->cnt.child_vertices += (unsigned long long)tc;
-        schedule_child(P, ws, at, tc, m2, 1, cls, T.inst);
+        schedule_child(P, ws, at, tc, m2, 1, cls, T.inst, kFlagRanked);
     }
     __syncwarp();
 }
@@ -1924,7 +1950,7 @@ constexpr int kSmallSplitPer = QC_SMALL_SPLIT_PER;
 // task runs its branches only.  Returns true when this call pushed branch
 // ranges of the record, which is then shared.
 __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R, Ws& ws, const TaskView& V,
-                              int q_lo, int q_hi, bool sroot)
+                              int q_lo, int q_hi, bool sroot, bool hot)
 {
     int lane = lane_id();
     SmallTask T;
@@ -1933,10 +1959,26 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
     T.cov = V.cov;
     T.inst = V.inst;
     bool act = lane < T.t;
-    T.id = act ? rec_ld(V.ids + lane) : -1;
-    T.a1 = act ? rec_ld(V.A1 + lane) : 0u;
-    T.a2 = act ? rec_ld(V.A2 + lane) : 0u;
-    T.l2 = act ? rec_ld(V.l2 + lane) : 0;
+    // id ranks among the task's ids, largest first (the children's order):
+    // stored by the register path's writer, else counted below
+    const bool ranked = hot || (V.flags & kFlagRanked) != 0;
+    if (hot) {
+        // the child this warp wrote last, from its copy in shared memory (a
+        // fresh child: its l2 counts are still zero)
+        const HotLane h = ws.sm->hot[lane];
+        T.id = act ? h.id : -1;
+        T.a1 = act ? h.a1 : 0u;
+        T.a2 = act ? h.a2 : 0u;
+        T.l2 = 0;
+        T.idr = h.rank;
+    } else {
+        T.id = act ? rec_ld(V.ids + lane) : -1;
+        T.a1 = act ? rec_ld(V.A1 + lane) : 0u;
+        T.a2 = act ? rec_ld(V.A2 + lane) : 0u;
+        T.l2 = act ? rec_ld(V.l2 + lane) : 0;
+        T.idr = ranked && act ? (int)rec_ld((const uint8_t*)V.ids - rec_ids_off() + rec_ranks_off() + lane)
+                              : 0;
+    }
     if (__any_sync(QC_FULL, act && (T.id < 0 || T.id >= R.n))) {
         if (lane == 0) check_fail(P, 8, V.rec); // a vertex id outside the instance
         return false;
@@ -2011,24 +2053,16 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
     } else if (ws.sm->stat) {
         return false;
     }
-    // rank of each id among the task's, largest first (the children's order)
-    T.idr = 0;
-    for (int j = 0; j < 32; j++) {
-        const int o = __shfl_sync(QC_FULL, T.id, j);
-        T.idr += (j < t && o > T.id) ? 1 : 0;
+    if (!ranked) {
+        for (int j = 0; j < 32; j++) {
+            const int o = __shfl_sync(QC_FULL, T.id, j);
+            T.idr += (j < t && o > T.id) ? 1 : 0;
+        }
     }
     for (int q = qhi; q >= qlo; q--) {
         // a sharded search's root: only this shard's branches
         if (sroot && (t - 1 - q) % P.nshards != P.shard) continue;
-#ifdef QC_EAGER_REFRESH
-        int idle_q = 0;
-        if (lane == 0 && q > qlo) idle_q = *(volatile int*)&P.ctl->idle_warps;
-#endif
         branch_small(P, R, ws, T, q);
-#ifdef QC_EAGER_REFRESH
-        if (lane == 0 && q > qlo) ws.sm->hungry = idle_q;
-        __syncwarp();
-#endif
         // children of this task can go to waiting warps before its last branch
         // when many warps wait (not for the odd one that will soon get work)
         if (q > qlo && ws.sm->hungry >= kEagerHungry) donate(P, ws, kEagerKeep);
@@ -2133,7 +2167,7 @@ __device__ QC_BIG_FN bool stage_record(const ExpandParams& P, WarpSmem* sm, Task
 // warp's shared memory (`wss`, `stage`); larger ones use the global
 // workspace `wsg` and read the record through L2.
 __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stage, const WorkItem& it,
-                             const TaskHdr& hv)
+                             const TaskHdr& hv, bool hot)
 {
     TaskView T = task_view(P.arena, it.rec, hv);
     const int t = T.t, W = T.W, m = T.m;
@@ -2175,9 +2209,9 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
     int q_lo = it.q_lo, q_hi = it.q_hi;
     // the root of a search split by its branches: this launch expands only the
     // branches of its own shard (and emits an accepted root in shard 0 only)
-    const bool sroot = hv.shard_root != 0 && P.nshards > 1;
+    const bool sroot = (hv.flags & kFlagShardRoot) != 0 && P.nshards > 1;
     if (t <= 32 && P.small_path) {
-        if (process_small(P, R, ws, T, q_lo, q_hi, sroot)) shared = true;
+        if (process_small(P, R, ws, T, q_lo, q_hi, sroot, hot)) shared = true;
         return shared;
     }
     if (q_lo < 0) {
@@ -2315,7 +2349,7 @@ __device__ bool item_ok(const ExpandParams& P, const WorkItem& it, TaskHdr& hv)
         hv.W = W;
         hv.m = m;
         hv.inst = inst;
-        hv.shard_root = h->shard_root;
+        hv.flags = h->flags;
         hv.cov = cov;
         hv.cls = cls;
         hv.refs = refs;
@@ -2392,7 +2426,10 @@ __global__ void expand_kernel(ExpandParams P)
         sm->fhead[c] = 0;
         sm->fcount[c] = 0;
     }
-    if (lane == 0) sm->nsfree = 0;
+    if (lane == 0) {
+        sm->nsfree = 0;
+        sm->hot_rec = ~0ull;
+    }
     __syncwarp();
 #ifndef QC_EMULATION
     if (stage) stage_bar_init(sm);
@@ -2419,6 +2456,7 @@ __global__ void expand_kernel(ExpandParams P)
                     hv.W = lt.W;
                     hv.cls = lt.cls;
                     hv.inst = lt.inst;
+                    hv.flags = lt.flags;
                     hv.refs = 1;
                     r = 2;
                 }
@@ -2437,7 +2475,7 @@ __global__ void expand_kernel(ExpandParams P)
         hv.cov = __shfl_sync(QC_FULL, hv.cov, 0);
         hv.W = __shfl_sync(QC_FULL, hv.W, 0);
         hv.inst = __shfl_sync(QC_FULL, hv.inst, 0);
-        hv.shard_root = __shfl_sync(QC_FULL, hv.shard_root, 0);
+        hv.flags = __shfl_sync(QC_FULL, hv.flags, 0);
         // idle warps and run status, read now and looked at while the next
         // item is taken and run, so the reads overlap this item's work
         int idle_now = 0, stat_now = 0;
@@ -2445,7 +2483,9 @@ __global__ void expand_kernel(ExpandParams P)
             idle_now = *(volatile int*)&P.ctl->idle_warps;
             stat_now = *(volatile int*)&P.ctl->status;
         }
-        bool shared = process_item(P, ws, wss, stage, it, hv);
+        // a child this warp wrote last is read from its copy in shared memory
+        const bool hot = r == 2 && sm->hot_rec == it.rec;
+        bool shared = process_item(P, ws, wss, stage, it, hv, hot);
         __syncwarp();
         if (lane == 0) {
             sm->hungry = idle_now;

@@ -697,7 +697,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         hd.refs = 1;
         hd.cls = root_cls;
         hd.inst = 0;
-        hd.shard_root = nshards > 1 ? 1 : 0;
+        hd.flags = nshards > 1 ? kFlagShardRoot : 0;
         CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(rec + rec_ids_off(), c->ids.p, sizeof(int32_t) * t,
                            cudaMemcpyDeviceToDevice, s));
@@ -1053,7 +1053,7 @@ static qc_status tune_search(qc_context* ctx, int32_t repeats, Run run, qc_confi
     };
     static const int32_t kWpb[] = {4, 8};
     static const int32_t kBps[] = {1, 2};
-    static const int32_t kSplit[] = {2, 4};
+    static const int32_t kSplit[] = {1, 2, 4};
     for (int32_t wpb : kWpb)
         for (int32_t bps : kBps)
             for (int32_t split : kSplit) {
@@ -1173,7 +1173,7 @@ __global__ void batch_root_fill_kernel(const RootMeta* meta, int nroots, const i
         h->refs = 1;
         h->cls = M.cls;
         h->inst = M.inst;
-        h->shard_root = 0;
+        h->flags = 0;
     }
 }
 

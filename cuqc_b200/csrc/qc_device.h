@@ -93,6 +93,9 @@ struct StackEntry {
 //   int32 l2[t]             (lookahead 2-hop counts; 0 until computed)
 //   uint32 A1[t][W]         (A1[v] bit w: w in N(v))
 //   uint32 A2[t][W]         (A2[v] bit w: w in N2(v))
+// and, in a record of at most 32 vertices written by the register path
+// (flag kFlagRanked), at rec_ranks_off(): uint8 ranks[t], the number of the
+// task's vertices with a larger id than vertex i.
 struct TaskHdr {
     int32_t t;    // vertices
     int32_t m;    // members are positions [0, m)
@@ -101,8 +104,10 @@ struct TaskHdr {
     int32_t refs; // work items that still reference this record
     int32_t cls;  // arena size class of the record's block
     int32_t inst; // instance (batched runs) whose rules apply
-    int32_t shard_root; // 1: the root of a search split by its branches (see ExpandParams)
+    int32_t flags; // kFlagShardRoot, kFlagRanked
 };
+constexpr int32_t kFlagShardRoot = 1; // the root of a search split by its branches (ExpandParams)
+constexpr int32_t kFlagRanked = 2;    // id ranks stored at rec_ranks_off()
 
 // Arena blocks come in size classes: four steps per power of two from
 // 256 B (2^(e-1) + s*2^(e-3), s = 1..4).  Freed blocks go to a lock-free
@@ -135,11 +140,12 @@ __host__ __device__ inline uint64_t rec_bytes(int t, int W) {
     return rec_a2_off(t, W) + align16(4ull * t * W);
 }
 // Every record of at most 32 vertices gets a block of one size, that of a
-// 32-vertex record, so a block freed by any small task can hold any small
-// child (children are smaller than their parents, and per-size classes
-// would leave the freed blocks in the wrong class).
+// 32-vertex record and its ranks, so a block freed by any small task can hold
+// any small child (children are smaller than their parents, and per-size
+// classes would leave the freed blocks in the wrong class).
+__host__ __device__ inline uint64_t rec_ranks_off() { return rec_bytes(32, 1); }
 __host__ __device__ inline uint64_t rec_block_bytes(int t, int W) {
-    return W == 1 ? rec_bytes(32, 1) : rec_bytes(t, W);
+    return W == 1 ? rec_ranks_off() + 32 : rec_bytes(t, W);
 }
 
 // Per-instance rules: the gamma tables and CSR offsets of one mining
@@ -222,7 +228,16 @@ constexpr int kEmitSets = 64;
 // task taken from a donated bundle has t = 0 and is read and checked.
 struct LocalTask {
     unsigned long long rec;
-    int32_t t, m, W, cls, inst, pad;
+    int32_t t, m, W, cls, inst, flags;
+};
+
+// The register path's copy of the newest child a warp wrote (one lane's
+// vertex each): taken from shared memory instead of the arena when that
+// child is the warp's next task.
+struct HotLane {
+    int32_t id;
+    uint32_t a1, a2;
+    int32_t rank;
 };
 
 // Per-warp state in shared memory: everything a warp touches on every task.
@@ -237,6 +252,8 @@ struct WarpSmem {
     int32_t fcount[kArenaClasses];
     unsigned long long sfree[kSmallFree]; // free blocks of the small-record class
     int32_t nsfree, pad2_;
+    unsigned long long hot_rec;    // record whose copy is in hot (~0: none)
+    HotLane hot[32];
     int32_t md[kTabCache];
     int32_t ubt[kTabCache];
     int32_t ebuf[kEmitInts];       // buffered sets, [k, ids..] each
