@@ -21,6 +21,7 @@ from . import graphs
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqc.so")
 CLI_PATH = os.path.join(HERE, "cuQC")
+CONVERT_PATH = os.path.join(HERE, "qc_convert")  # graph-format tools (csrc/convert.cpp)
 
 # qc_status
 STATUS = {
@@ -39,7 +40,8 @@ EXPORTS = [
     "qc_result_sets", "qc_result_emitted", "qc_result_stats", "qc_result_write", "qc_result_free",
     "qc_twohop_noalloc", "qc_twohop_noalloc_max_vertices", "qc_tune", "qc_maximal_sets",
     "qc_context_last_stats", "qc_root", "qc_mine_shard", "qc_graph_read_binary",
-    "qc_graph_write_binary", "qc_graph_read", "qc_tune_batch",
+    "qc_graph_write_binary", "qc_graph_read", "qc_tune_batch", "qc_sets_write_async",
+    "qc_result_write_async", "qc_writer_wait",
 ]
 
 
@@ -136,6 +138,9 @@ def lib():
         L.qc_graph_read.argtypes = [C.c_char_p, C.POINTER(vp)]
         L.qc_mine_shard.argtypes = [vp, vp, C.c_double, C.c_int32, C.c_int32, C.c_int32,
                                     C.POINTER(vp)]
+        L.qc_sets_write_async.argtypes = [P32, C.c_int64, C.c_char_p, C.POINTER(vp)]
+        L.qc_result_write_async.argtypes = [vp, C.c_char_p, C.POINTER(vp)]
+        L.qc_writer_wait.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -152,6 +157,28 @@ def _p64(a):
 
 def _p32(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class Writer:
+    """A result file being written on a host thread (qc_sets_write_async);
+    wait() returns once it is on disk.  Holds the set array until then."""
+
+    def __init__(self, flat, path):
+        self._flat = np.ascontiguousarray(flat, np.int32)
+        self.h = C.c_void_p()
+        _check(lib().qc_sets_write_async(_p32(self._flat), int(self._flat.size),
+                                         os.fsencode(path), C.byref(self.h)))
+
+    def wait(self):
+        if self.h is not None:
+            h, self.h = self.h, None
+            _check(lib().qc_writer_wait(h))
+            self._flat = None
+
+
+def write_sets_async(flat, path):
+    """Write flat [k, ids..]* sets as a result file in the background."""
+    return Writer(flat, path)
 
 
 class DeviceGraph:
@@ -230,6 +257,14 @@ class Result:
     def text(self):
         return "".join("%d " % len(s) + "".join("%d " % v for v in s) + "\n" for s in self.sets)
 
+    def write(self, path):
+        """The result file (the reference's format), formatted by the library."""
+        write_sets_async(self.flat, path).wait()
+
+    def write_async(self, path):
+        """Start writing the result file on a host thread; returns a Writer."""
+        return write_sets_async(self.flat, path)
+
 
 def _flat_to_sets(flat):
     vals = flat.tolist()
@@ -288,6 +323,28 @@ class Context:
         r = C.c_void_p()
         _check(lib().qc_mine(self.h, dg.h, float(gamma), int(min_size), int(sched), C.byref(r)))
         return self._result(r)
+
+    def mine_files(self, jobs):
+        """Mine a stream of graph files, each into its result file: jobs is an
+        iterable of (graph path, gamma, min_size, result path).  Every result
+        file is written on a host thread while the next graph is read and
+        mined; returns each job's counters."""
+        pending, stats = [], []
+        try:
+            for gpath, gamma, min_size, out in jobs:
+                dg = DeviceGraph.read(os.fsdecode(gpath))
+                try:
+                    r = self.mine(dg, gamma, min_size)
+                finally:
+                    dg.close()
+                pending.append(r.write_async(out))
+                stats.append(r.stats)
+                if len(pending) > 4:  # bound the results held in memory
+                    pending.pop(0).wait()
+        finally:
+            for w in pending:
+                w.wait()
+        return stats
 
     def last_stats(self):
         """Counters of the most recent expansion on this context (dict), also

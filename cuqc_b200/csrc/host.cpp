@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 namespace qcb {
 
@@ -437,13 +438,13 @@ void maximal_sets(const int32_t* flat, int64_t nints, std::vector<int32_t>& out,
     }
 }
 
-std::string write_result(const int32_t* flat, int64_t nints, const char* path)
+// the lines of sets [a, b) of the flat array (a, b at set starts)
+static void format_sets(const int32_t* flat, int64_t a, int64_t b, std::string& s)
 {
-    FILE* f = fopen(path, "wb");
-    if (!f) return std::string("cannot open ") + path + " for writing";
-    std::string s;
-    for (int64_t p = 0; p < nints;) {
-        int32_t k = flat[p];
+    s.clear();
+    s.reserve((size_t)(b - a) * 7);
+    for (int64_t p = a; p < b;) {
+        const int32_t k = flat[p];
         put_num(s, k);
         s += ' ';
         for (int32_t i = 0; i < k; i++) {
@@ -452,14 +453,46 @@ std::string write_result(const int32_t* flat, int64_t nints, const char* path)
         }
         s += '\n';
         p += 1 + k;
-        if (s.size() > (1u << 20)) {
-            fwrite(s.data(), 1, s.size(), f);
-            s.clear();
+    }
+}
+
+std::string write_result(const int32_t* flat, int64_t nints, const char* path)
+{
+    // chunks of about 256 K ints at set boundaries, formatted by up to 16 host
+    // threads at a time and written in order
+    constexpr int64_t kChunk = 1 << 18;
+    std::vector<int64_t> cuts(1, 0);
+    for (int64_t p = 0; p < nints;) {
+        const int32_t k = flat[p];
+        if (k < 0 || p + 1 + k > nints) return "malformed result record";
+        p += 1 + k;
+        if (p - cuts.back() >= kChunk || p == nints) cuts.push_back(p);
+    }
+    FILE* f = fopen(path, "wb");
+    if (!f) return std::string("cannot open ") + path + " for writing";
+    const int64_t nchunks = (int64_t)cuts.size() - 1;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int par = (int)std::min<int64_t>({nchunks, (int64_t)hw, 16});
+    std::vector<std::string> bufs((size_t)std::max(par, 1));
+    bool ok = true;
+    for (int64_t c0 = 0; c0 < nchunks; c0 += std::max(par, 1)) {
+        const int64_t c1 = std::min<int64_t>(nchunks, c0 + std::max(par, 1));
+        if (c1 - c0 == 1) {
+            format_sets(flat, cuts[(size_t)c0], cuts[(size_t)c0 + 1], bufs[0]);
+        } else {
+            std::vector<std::thread> th;
+            for (int64_t c = c0; c < c1; c++)
+                th.emplace_back(format_sets, flat, cuts[(size_t)c], cuts[(size_t)c + 1],
+                                std::ref(bufs[(size_t)(c - c0)]));
+            for (auto& t : th) t.join();
+        }
+        for (int64_t c = c0; c < c1; c++) {
+            const std::string& b = bufs[(size_t)(c - c0)];
+            ok = ok && fwrite(b.data(), 1, b.size(), f) == b.size();
         }
     }
-    fwrite(s.data(), 1, s.size(), f);
-    fclose(f);
-    return "";
+    ok = (fclose(f) == 0) && ok;
+    return ok ? "" : std::string("write to ") + path + " failed";
 }
 
 } // namespace qcb

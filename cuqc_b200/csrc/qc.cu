@@ -19,6 +19,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
@@ -1600,6 +1601,38 @@ extern "C" qc_status qc_result_write(const qc_result* r, const char* path)
     return e.empty() ? QC_OK : fail(QC_ERR_IO, e);
 }
 extern "C" void qc_result_free(qc_result* r) { delete r; }
+
+struct qc_writer {
+    std::thread th;
+    std::string err;
+};
+
+extern "C" qc_status qc_sets_write_async(const int32_t* flat, int64_t n_ints, const char* path,
+                                         qc_writer** out)
+{
+    if (!path || !out || n_ints < 0 || (n_ints > 0 && !flat)) return fail(QC_ERR_ARGS, "bad arguments");
+    qc_writer* w = new qc_writer;
+    const std::string p(path);
+    w->th = std::thread([w, flat, n_ints, p] { w->err = write_result(flat, n_ints, p.c_str()); });
+    *out = w;
+    return QC_OK;
+}
+
+extern "C" qc_status qc_result_write_async(const qc_result* r, const char* path, qc_writer** out)
+{
+    if (!r) return fail(QC_ERR_ARGS, "NULL result");
+    return qc_sets_write_async(r->sets.data(), (int64_t)r->sets.size(), path, out);
+}
+
+extern "C" qc_status qc_writer_wait(qc_writer* w)
+{
+    if (!w) return fail(QC_ERR_ARGS, "NULL writer");
+    w->th.join();
+    const std::string e = w->err;
+    delete w;
+    if (e.empty()) return QC_OK;
+    return fail(e == "malformed result record" ? QC_ERR_FORMAT : QC_ERR_IO, e);
+}
 
 // qc_graph_from_csr (device 2-hop builder) lives in twohop.cu
 

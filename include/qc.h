@@ -70,8 +70,10 @@ qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int32_t* adj, q
  * For callers that cannot call cudaMalloc: applications whose device memory
  * is owned by their own pool or a fixed memory plan, or that must not
  * allocate while serving requests.  The caller passes device buffers:
- * d_off (int64[n+1]) and d_adj (int32[d_off[n]]) hold a sorted, symmetric
- * 1-hop CSR; d_off2 (int64[n+1]) receives the two-hop offsets and d_adj2
+ * d_off (int64[n+1]) and d_adj (int32[d_off[n]]) hold a 1-hop CSR (the
+ * miner wants sorted symmetric rows; these lists follow the rows as given,
+ * repeats and one-way rows included, and a self loop keeps v, as adjToSer
+ * does); d_off2 (int64[n+1]) receives the two-hop offsets and d_adj2
  * (int32[adj2_cap]) the rows sorted(N(v) u N(N(v)) minus {v}).  With
  * d_adj2 == NULL only d_off2 and *total_out are filled (a size query); if
  * the rows need more than adj2_cap entries the call returns
@@ -286,9 +288,27 @@ const int32_t* qc_result_sets(const qc_result* r, int64_t* n_ints);
 /* Raw emitted multiset (only with keep_emitted), flat [k, ids..]. */
 const int32_t* qc_result_emitted(const qc_result* r, int64_t* n_sets, int64_t* n_ints);
 const qc_stats* qc_result_stats(const qc_result* r);
-/* Write "<k> v1 .. vk \n" lines (main.cu:4641-4652). */
+/* Write "<k> v1 .. vk \n" lines (main.cu:4641-4652).  Large results are
+ * formatted by several host threads, in chunks written in order. */
 qc_status qc_result_write(const qc_result* r, const char* path);
 void qc_result_free(qc_result* r);
+
+/* Result files written on a host thread while the caller goes on (mines
+ * the next instance, say).  The reference spills every emitted set to
+ * temp.txt during enumeration and rebuilds its result file from that spill
+ * (main.cu:1218-1246, 4939-4960); here the device filter hands back the
+ * maximal sets already in file order, so only their formatting and the
+ * write remain, and they overlap the next device work. */
+typedef struct qc_writer qc_writer;
+/* Start writing sets flat [k, id_1 .. id_k]* (n_ints ints) in the result
+ * format.  The array must stay alive and unchanged until qc_writer_wait. */
+qc_status qc_sets_write_async(const int32_t* flat, int64_t n_ints, const char* path,
+                              qc_writer** out);
+/* The same for a result (r must outlive the write). */
+qc_status qc_result_write_async(const qc_result* r, const char* path, qc_writer** out);
+/* Wait for the write; returns its status (QC_ERR_IO, QC_ERR_FORMAT) and
+ * frees the writer. */
+qc_status qc_writer_wait(qc_writer* w);
 
 #ifdef __cplusplus
 }
