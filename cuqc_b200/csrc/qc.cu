@@ -163,7 +163,53 @@ struct qc_context {
     int64_t arena_bytes = 0, stack_slots = 0, result_ints = 0;
     int64_t launches = 0;
     qc_stats last{}; // counters of the most recent expansion, also of one that stopped
+    // page-locked staging for the small copies of a call (the Control head,
+    // the root's header, stack entry and slot, the rules): copies from it are
+    // plain DMA, with no staging by the driver
+    char* pin = nullptr;
+    size_t pin_n = 0, pin_at = 0;
+    // md / ubt as last uploaded: the same tables are not copied again
+    std::vector<int32_t> md_up, ubt_up;
 };
+
+// The Control fields up to the free-list heads; the heads (most of the
+// block) start at zero on every launch and are cleared on the device.
+static constexpr size_t kControlHead = offsetof(Control, free_head);
+
+// A page-locked copy of `bytes` bytes for this call's host-to-device copies
+// (the buffer is reused once the call has synchronised).
+static void* pin_stage(qc_context* c, const void* src, size_t bytes)
+{
+    const size_t at = (c->pin_at + 15) & ~(size_t)15;
+    if (!c->pin || at + bytes > c->pin_n) return nullptr;
+    std::memcpy(c->pin + at, src, bytes);
+    c->pin_at = at + bytes;
+    return c->pin + at;
+}
+
+// host-to-device copy of a small host object through the staging buffer
+// (a plain copy when it does not fit)
+static cudaError_t put_small(qc_context* c, void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    const void* p = pin_stage(c, src, bytes);
+    return cudaMemcpyAsync(dst, p ? p : src, bytes, cudaMemcpyHostToDevice, s);
+}
+
+// The Control block for a launch: the head from `ctl`, the free lists zeroed
+static cudaError_t put_control(qc_context* c, const Control& ctl, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(c->ctl.as<char>() + kControlHead, 0, sizeof(Control) - kControlHead, s);
+    if (e != cudaSuccess) return e;
+    return put_small(c, c->ctl.p, &ctl, kControlHead, s);
+}
+
+// The launch's Control head back into `ctl` (free lists left out); the
+// caller synchronises before reading it
+static cudaError_t get_control(qc_context* c, Control& ctl, cudaStream_t s)
+{
+    std::memset(&ctl, 0, sizeof(ctl));
+    return cudaMemcpyAsync(&ctl, c->ctl.p, kControlHead, cudaMemcpyDeviceToHost, s);
+}
 
 extern "C" void qc_config_default(qc_config* c)
 {
@@ -189,6 +235,8 @@ extern "C" qc_status qc_context_create(const qc_config* cfg, qc_context** out)
     CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->cfg.device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) CK(cudaEventCreate(&e));
+    CK(cudaHostAlloc((void**)&c->pin, 64 << 10, cudaHostAllocDefault));
+    c->pin_n = 64 << 10;
     c->arena_bytes = c->cfg.arena_bytes > 0 ? c->cfg.arena_bytes : (256ll << 20);
     c->stack_slots = c->cfg.stack_slots > 0 ? c->cfg.stack_slots : (1ll << 20);
     c->result_ints = c->cfg.result_ints > 0 ? c->cfg.result_ints : (16ll << 20);
@@ -220,6 +268,7 @@ extern "C" void qc_context_free(qc_context* c)
         b->release();
     c->filt.release();
     c->batch.release();
+    if (c->pin) cudaFreeHost(c->pin);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -384,6 +433,21 @@ template <class T> cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaSt
 }
 
 } // namespace
+
+// A table upload that is skipped when the device buffer still holds the
+// values it was last given (`last`); a reallocated buffer is filled again.
+template <class T>
+static cudaError_t upload_cached(qc_context* c, DevBuf& b, std::vector<T>& last, const std::vector<T>& v,
+                                 cudaStream_t s)
+{
+    void* before = b.p;
+    cudaError_t e = b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (e != cudaSuccess) return e;
+    if (b.p == before && last == v) return cudaSuccess;
+    last = v;
+    if (v.empty()) return cudaSuccess;
+    return put_small(c, b.p, v.data(), v.size() * sizeof(T), s);
+}
 
 // stack slots rounded up so that every shard's capacity is a power of two
 // (the FIFO form of the shards indexes its ring by a wrapping count)
@@ -654,8 +718,9 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         return QC_OK;
     }
     const int W = words_for(t);
-    CK(upload(c->md, md, s));
-    CK(upload(c->ubt, ubt, s));
+    c->pin_at = 0;
+    CK(upload_cached(c, c->md, c->md_up, md, s));
+    CK(upload_cached(c, c->ubt, c->ubt_up, ubt, s));
 
     Shape sh;
     {
@@ -670,6 +735,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
 
     std::vector<int32_t> flat;
     for (int attempt = 0;; attempt++) {
+        if (attempt > 0) c->pin_at = 0; // the previous attempt synchronised
         CK(c->arena.ensure((size_t)c->arena_bytes));
         c->stack_slots = shard_slots(std::max<int64_t>(c->stack_slots, 2 * kStackShards));
         CK(c->stack.ensure(sizeof(StackEntry) * (size_t)c->stack_slots));
@@ -699,7 +765,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         hd.cls = root_cls;
         hd.inst = 0;
         hd.flags = nshards > 1 ? kFlagShardRoot : 0;
-        CK(cudaMemcpyAsync(rec, &hd, sizeof(hd), cudaMemcpyHostToDevice, s));
+        CK(put_small(c, rec, &hd, sizeof(hd), s));
         CK(cudaMemcpyAsync(rec + rec_ids_off(), c->ids.p, sizeof(int32_t) * t,
                            cudaMemcpyDeviceToDevice, s));
         root_pos_kernel<<<(t + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), t,
@@ -721,15 +787,15 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots / kStackShards, INT32_MAX);
         ctl.stack_top[0] = 1;
         ctl.pending = 1;
-        CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
+        CK(put_control(c, ctl, s));
         StackEntry root{};
         root.rec[0] = 0;
         root.n = 1;
         root.q_lo = -1;
         root.q_hi = -1;
-        CK(cudaMemcpyAsync(c->stack.p, &root, sizeof(root), cudaMemcpyHostToDevice, s));
+        CK(put_small(c, c->stack.p, &root, sizeof(root), s));
         int one = 1;
-        CK(cudaMemcpyAsync(c->slot.p, &one, sizeof(one), cudaMemcpyHostToDevice, s));
+        CK(put_small(c, c->slot.p, &one, sizeof(one), s));
 
         Rules rule{};
         rule.off = rg->off.as<int64_t>();
@@ -743,7 +809,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         rule.vbase = 0;
         rule.n = h.n;
         CK(c->rules.ensure(sizeof(Rules)));
-        CK(cudaMemcpyAsync(c->rules.p, &rule, sizeof(rule), cudaMemcpyHostToDevice, s));
+        CK(put_small(c, c->rules.p, &rule, sizeof(rule), s));
         ExpandParams P{};
         P.rules = c->rules.as<Rules>();
         P.nrules = 1;
@@ -771,7 +837,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaGetLastError());
         c->launches += 1;
         CK(cudaEventRecord(c->ev[2], s));
-        CK(cudaMemcpyAsync(&ctl, c->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+        CK(get_control(c, ctl, s));
         CK(cudaStreamSynchronize(s));
         float kms = 0;
         cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
@@ -1380,7 +1446,9 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
 
     Control ctl{};
     float kms = 0;
+    c->pin_at = 0;
     for (int attempt = 0;; attempt++) {
+        if (attempt > 0) c->pin_at = 0; // the previous attempt synchronised
         if ((int64_t)arena_at * 2 > c->arena_bytes) c->arena_bytes = (int64_t)arena_at * 2;
         c->stack_slots = std::max<int64_t>(c->stack_slots, (int64_t)nroots * 2 + 64 * kStackShards);
         CK(c->arena.ensure((size_t)c->arena_bytes));
@@ -1440,7 +1508,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
             }
             filled += cnt;
         }
-        CK(cudaMemcpyAsync(c->ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
+        CK(put_control(c, ctl, s));
         ExpandParams P{};
         P.rules = B.rules.as<Rules>();
         P.nrules = count;
@@ -1466,7 +1534,7 @@ static qc_status mine_batch(qc_context* c, const qc_graph* const* graphs, const 
         CK(cudaGetLastError());
         c->launches += 1;
         CK(cudaEventRecord(c->ev[2], s));
-        CK(cudaMemcpyAsync(&ctl, c->ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+        CK(get_control(c, ctl, s));
         CK(cudaStreamSynchronize(s));
         cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
         record_last(c, ctl, kms, 0);
