@@ -149,6 +149,24 @@ __global__ void __launch_bounds__(1024) level0_kernel(const int64_t* off, const 
     level0_block(off, adj, off2, n, need, min_size, exdeg, label, l2, keys, ids, info);
 }
 
+// Graphs of at most this many vertices keep level 0's arrays (exdeg, label,
+// 2-hop sizes, sort keys: level0_scratch_bytes, 40 KB at this size) in the
+// block's shared memory instead of global scratch.
+constexpr int kLevel0SmemMax = 2048;
+
+#ifndef QC_EMULATION
+extern __shared__ __align__(16) unsigned char qc_l0_smem[];
+__global__ void __launch_bounds__(1024) level0_smem_kernel(const int64_t* off, const int32_t* adj,
+                                                           const int64_t* off2, int n, int need,
+                                                           int min_size, int32_t* ids, int32_t* info)
+{
+    char* z = (char*)qc_l0_smem;
+    const int64_t nb = level0_array_bytes(n);
+    level0_block(off, adj, off2, n, need, min_size, (int32_t*)z, (int32_t*)(z + nb),
+                 (int32_t*)(z + 2 * nb), (unsigned long long*)(z + 3 * nb), ids, info);
+}
+#endif
+
 // Level 0 of many instances at once, one block per instance (batched mining):
 // info[2i], info[2i+1] = root size and covered count of instance i.
 __global__ void __launch_bounds__(256) level0_batch_kernel(const Level0Job* jobs, char* scratch,

@@ -389,6 +389,105 @@ __global__ void root_pos_kernel(const int32_t* ids, int t, int32_t* pos, int set
     if (i < t) pos[ids[i]] = set ? i : -1;
 }
 
+// The root's set-up when level 0 ran on the device and its size stays there
+// (info = {root size t, covered count}): one block writes the Control block
+// (the head as the host prepared it, free-list heads zeroed, then the root's
+// arena use, stack entry and size), the root record's header and ids with its
+// rows zeroed, the shared stack's root entry, the rules, and each root
+// vertex's position.  A root whose block exceeds the arena is not written: the
+// launch then ends at once with ST_TASK_OVERFLOW and the host grows the arena.
+struct RootSetup {
+    unsigned long long head[offsetof(Control, free_head) / 8];
+    Rules rule;
+    int32_t flags, pad;
+};
+__global__ void __launch_bounds__(256) root_setup_kernel(RootSetup S, const int32_t* info,
+                                                         const int32_t* ids, char* arena,
+                                                         unsigned long long arena_cap, Control* ctl,
+                                                         StackEntry* stack, int32_t* slot,
+                                                         Rules* rules, int32_t* pos)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int t = info[0], cov = info[1];
+    const int W = words_for(t);
+    const unsigned long long block = t > 0 ? arena_class_bytes(arena_class(rec_block_bytes(t, W))) : 0;
+    const bool fits = t > 0 && block <= arena_cap;
+    unsigned long long* c8 = (unsigned long long*)ctl;
+    constexpr int kHead = (int)(offsetof(Control, free_head) / 8);
+    for (int i = tid; i < (int)(sizeof(Control) / 8); i += nt) c8[i] = i < kHead ? S.head[i] : 0ull;
+    if (fits) {
+        uint4* z = (uint4*)arena;
+        const int64_t n16 = (int64_t)(rec_bytes(t, W) / 16);
+        for (int64_t i = tid; i < n16; i += nt) z[i] = make_uint4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    for (int i = tid; i < t; i += nt) {
+        const int v = ids[i];
+        pos[v] = i;
+        if (fits) ((int32_t*)(arena + rec_ids_off()))[i] = v;
+    }
+    if (tid == 0) {
+        if (fits) {
+            TaskHdr* h = (TaskHdr*)arena;
+            h->t = t;
+            h->m = 0;
+            h->cov = cov;
+            h->W = W;
+            h->refs = 1;
+            h->cls = arena_class(rec_block_bytes(t, W));
+            h->inst = 0;
+            h->flags = S.flags;
+            StackEntry e{};
+            e.rec[0] = 0;
+            e.n = 1;
+            e.q_lo = -1;
+            e.q_hi = -1;
+            stack[0] = e;
+            slot[0] = 1;
+        }
+        ctl->arena_top = block;
+        ctl->stack_top[0] = fits ? 1 : 0;
+        ctl->pending = fits ? 1 : 0;
+        if (t > 0 && !fits) ctl->status = ST_TASK_OVERFLOW;
+        ctl->root_t = t;
+        ctl->root_cov = cov;
+        *rules = S.rule;
+    }
+}
+
+// root_rows_kernel and the positions' reset for a root whose size is on the
+// device (root_setup_kernel wrote the record when it fits the arena)
+__global__ void root_rows_dev_kernel(const int64_t* off, const int32_t* adj, const int64_t* off2,
+                                     const int32_t* adj2, const int32_t* ids, const int32_t* info,
+                                     const int32_t* pos, char* arena, unsigned long long arena_cap)
+{
+    const int t = info[0], W = words_for(t);
+    if (t <= 0 || arena_class_bytes(arena_class(rec_block_bytes(t, W))) > arena_cap) return;
+    uint32_t* A1 = (uint32_t*)(arena + rec_a1_off(t));
+    uint32_t* A2 = (uint32_t*)(arena + rec_a2_off(t, W));
+    int lane = threadIdx.x & 31;
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < t; i += nw) {
+        int u = ids[i];
+        uint32_t* r1 = A1 + (int64_t)i * W;
+        uint32_t* r2 = A2 + (int64_t)i * W;
+        for (int64_t e = off[u] + lane; e < off[u + 1]; e += 32) {
+            int p = pos[adj[e]];
+            if (p >= 0) atomicOr(&r1[p >> 5], 1u << (p & 31));
+        }
+        for (int64_t e = off2[u] + lane; e < off2[u + 1]; e += 32) {
+            int p = pos[adj2[e]];
+            if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
+        }
+    }
+}
+__global__ void root_unpos_dev_kernel(const int32_t* ids, const int32_t* info, int32_t* pos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < info[0]) pos[ids[i]] = -1;
+}
+
 // one warp per root vertex: mark its 1-hop and 2-hop neighbours inside the root
 __global__ void root_rows_kernel(const int64_t* off, const int32_t* adj, const int64_t* off2,
                                  const int32_t* adj2, const int32_t* ids, int t, int W,
@@ -485,15 +584,14 @@ static qc_status launch_shape(qc_context* c, int max_t, Shape& sh)
     const size_t sm_budget = 220u << 10; // of the 228 KB of shared memory per SM
     sh.smem_t = 0;
     if (max_t > 32 && c->cfg.stage_max >= 0) {
-        for (int cand : {256, 192, 128, 96, 64}) {
-            int tt = std::min(cand, max_t);
-            if (c->cfg.stage_max > 0) tt = std::min(tt, c->cfg.stage_max);
-            if (tt <= 32) break;
+        // the largest task size (up to 256) whose buffers fit
+        int hi = std::min(256, max_t);
+        if (c->cfg.stage_max > 0) hi = std::min(hi, c->cfg.stage_max);
+        for (int tt = hi; tt > 32; tt--)
             if (warp_smem_bytes(tt) * sh.wpb * want_bps <= sm_budget) {
                 sh.smem_t = tt;
                 break;
             }
-        }
     }
     sh.smem_bytes = expand_smem_bytes(sh.wpb, sh.smem_t);
     {
@@ -611,6 +709,50 @@ static void record_last(qc_context* c, const Control& ctl, float kms, int root_s
 // device for graphs of up to kLevel0DeviceMax vertices (one block) and up to
 // kLevel0GridMax (the whole grid, one cooperative launch); on the host above.
 // *on_device tells which.
+// Level 0 of a graph of at most kLevel0DeviceMax vertices on one block, with
+// nothing read back: the root's ids go to c->ids and {size, covered count} to
+// *info (device memory).
+static qc_status launch_level0(qc_context* c, const HostGraph& h, ResidentGraph* rg,
+                               const std::vector<int32_t>& md, int32_t min_size, int32_t** info_out)
+{
+    cudaStream_t s = c->stream;
+    int P = 1;
+    while (P < h.n) P <<= 1;
+    // int32 arrays of n (exdeg, label, 2-hop size), then the 64-bit sort keys,
+    // then two ints of results: every array starts 16-byte aligned
+    const size_t nb = ((size_t)h.n * 4 + 15) & ~(size_t)15;
+    CK(c->lvl0.ensure(3 * nb + 8 * (size_t)P + 64));
+    CK(c->ids.ensure(std::max<size_t>((size_t)h.n * 4, 16)));
+    char* z = c->lvl0.as<char>();
+    int32_t* info = (int32_t*)(z + 3 * nb + 8 * (size_t)P);
+    if (h.n <= kLevel0SmemMax)
+        level0_smem_kernel<<<1, 1024, (size_t)level0_scratch_bytes(h.n), s>>>(
+            rg->off.as<int64_t>(), rg->adj.as<int32_t>(), rg->off2.as<int64_t>(), h.n,
+            md[(size_t)min_size], min_size, c->ids.as<int32_t>(), info);
+    else
+        level0_kernel<<<1, 1024, 0, s>>>(rg->off.as<int64_t>(), rg->adj.as<int32_t>(),
+                                         rg->off2.as<int64_t>(), h.n, md[(size_t)min_size],
+                                         min_size, (int32_t*)z, (int32_t*)(z + nb),
+                                         (int32_t*)(z + 2 * nb), (unsigned long long*)(z + 3 * nb),
+                                         c->ids.as<int32_t>(), info);
+    CK(cudaGetLastError());
+    c->launches += 1;
+    *info_out = info;
+    return QC_OK;
+}
+
+// The vertices level 0 keeps at first (deg >= need, |N2| >= min_size - 1): the
+// root is a subset of them (initialize_tasks, main.cu:846-998)
+static int root_bound(const HostGraph& h, int need, int32_t min_size)
+{
+    int k = 0;
+    for (int32_t v = 0; v < h.n; v++)
+        if (h.off[(size_t)v + 1] - h.off[(size_t)v] >= need &&
+            h.off2[(size_t)v + 1] - h.off2[(size_t)v] >= min_size - 1)
+            k++;
+    return k;
+}
+
 static qc_status compute_root(qc_context* c, const HostGraph& h, ResidentGraph* rg,
                               const std::vector<int32_t>& md, int32_t min_size, int& t, int& cov,
                               bool* on_device)
@@ -624,22 +766,11 @@ static qc_status compute_root(qc_context* c, const HostGraph& h, ResidentGraph* 
     if (l0_dev) {
         // root ids straight into c->ids; only the root size and the covered
         // count come back
-        int P = 1;
-        while (P < h.n) P <<= 1;
-        // int32 arrays of n (exdeg, label, 2-hop size), then the 64-bit sort
-        // keys, then two ints of results: every array starts 16-byte aligned
-        const size_t nb = ((size_t)h.n * 4 + 15) & ~(size_t)15;
-        CK(c->lvl0.ensure(3 * nb + 8 * (size_t)P + 64));
-        CK(c->ids.ensure(std::max<size_t>((size_t)h.n * 4, 16)));
-        char* z = c->lvl0.as<char>();
-        int32_t* info = (int32_t*)(z + 3 * nb + 8 * (size_t)P);
-        level0_kernel<<<1, 1024, 0, s>>>(rg->off.as<int64_t>(), rg->adj.as<int32_t>(),
-                                         rg->off2.as<int64_t>(), h.n, md[(size_t)min_size],
-                                         min_size, (int32_t*)z, (int32_t*)(z + nb),
-                                         (int32_t*)(z + 2 * nb), (unsigned long long*)(z + 3 * nb),
-                                         c->ids.as<int32_t>(), info);
-        CK(cudaGetLastError());
-        c->launches += 1;
+        int32_t* info = nullptr;
+        {
+            qc_status ls = launch_level0(c, h, rg, md, min_size, &info);
+            if (ls != QC_OK) return ls;
+        }
         int32_t hinfo[2] = {0, 0};
         CK(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -706,13 +837,28 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
     gamma_tables(gamma, h.n, min_size, md, ubt);
     int cov = 0, t = 0;
     bool l0_on_device = false;
-    {
+    // A graph level 0 handles in one block keeps its root on the device: the
+    // root's size comes back with the expansion's counters, and the launches
+    // are sized for the vertices level 0 keeps at first (tmax), so the host
+    // does not wait for level 0 before setting up the expansion.
+    const bool root_dev = h.n > 0 && h.n <= kLevel0DeviceMax && h.off2.size() == (size_t)h.n + 1;
+    int tmax = 0;
+    int32_t* d_info = nullptr;
+    if (root_dev) {
+        tmax = root_bound(h, md[(size_t)min_size], min_size);
+        l0_on_device = true;
+        if (tmax > 0) {
+            qc_status ls = launch_level0(c, h, rg, md, min_size, &d_info);
+            if (ls != QC_OK) return ls;
+        }
+    } else {
         qc_status ls = compute_root(c, h, rg, md, min_size, t, cov, &l0_on_device);
         if (ls != QC_OK) return ls;
+        tmax = t;
     }
     r->st.level0_on_device = l0_on_device ? 1 : 0;
     r->st.root_size = (int64_t)t;
-    if (t == 0) {
+    if (tmax == 0) {
         r->st.enum_ms = ms_since(t_enum);
         r->st.total_ms = ms_since(t_all);
         return QC_OK;
@@ -724,12 +870,12 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
 
     Shape sh;
     {
-        qc_status ss = launch_shape(c, t, sh);
+        qc_status ss = launch_shape(c, tmax, sh);
         if (ss != QC_OK) return ss;
     }
     const int wpb = sh.wpb, blocks = sh.blocks;
     int nwarps = blocks * wpb;
-    WsLayout L = ws_layout(t);
+    WsLayout L = ws_layout(tmax);
     CK(c->ws.ensure((size_t)L.total * nwarps));
     CK(c->ctl.ensure(sizeof(Control)));
 
@@ -745,6 +891,42 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(c->starts.ensure(sizeof(unsigned long long) * (size_t)set_cap));
         CK(cudaMemsetAsync(c->slot.p, 0, sizeof(int32_t) * (size_t)c->stack_slots, s));
 
+        Rules rule{};
+        rule.off = rg->off.as<int64_t>();
+        rule.off2 = rg->off2.as<int64_t>();
+        rule.adj = rg->adj.as<int32_t>();
+        rule.adj2 = rg->adj2.as<int32_t>();
+        rule.md = c->md.as<int32_t>();
+        rule.ubt = c->ubt.as<int32_t>();
+        rule.mdlen = (int32_t)md.size();
+        rule.min_size = min_size;
+        rule.vbase = 0;
+        rule.n = h.n;
+        CK(c->rules.ensure(sizeof(Rules)));
+        Control ctl{};
+        ctl.arena_cap = (unsigned long long)c->arena_bytes;
+        ctl.result_cap = (unsigned long long)c->result_ints;
+        ctl.set_cap = (unsigned long long)set_cap;
+        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots / kStackShards, INT32_MAX);
+        if (root_dev) {
+            CK(cudaEventRecord(c->ev[0], s));
+            RootSetup S{};
+            std::memcpy(S.head, &ctl, sizeof(S.head));
+            S.rule = rule;
+            S.flags = nshards > 1 ? kFlagShardRoot : 0;
+            root_setup_kernel<<<1, 256, 0, s>>>(S, d_info, c->ids.as<int32_t>(), c->arena.as<char>(),
+                                                (unsigned long long)c->arena_bytes, c->ctl.as<Control>(),
+                                                c->stack.as<StackEntry>(), c->slot.as<int32_t>(),
+                                                c->rules.as<Rules>(), c->pos.as<int32_t>());
+            root_rows_dev_kernel<<<std::max(1, std::min(blocks * 4, (tmax + 7) / 8)), 256, 0, s>>>(
+                rg->off.as<int64_t>(), rg->adj.as<int32_t>(), rg->off2.as<int64_t>(),
+                rg->adj2.as<int32_t>(), c->ids.as<int32_t>(), d_info, c->pos.as<int32_t>(),
+                c->arena.as<char>(), (unsigned long long)c->arena_bytes);
+            root_unpos_dev_kernel<<<(tmax + 255) / 256, 256, 0, s>>>(c->ids.as<int32_t>(), d_info,
+                                                                    c->pos.as<int32_t>());
+            CK(cudaGetLastError());
+            c->launches += 3;
+        } else {
         uint64_t rb = rec_bytes(t, W);
         const int root_cls = arena_class(rec_block_bytes(t, W));
         const uint64_t root_block = arena_class_bytes(root_cls);
@@ -779,12 +961,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaGetLastError());
         c->launches += 3;
 
-        Control ctl{};
         ctl.arena_top = root_block;
-        ctl.arena_cap = (unsigned long long)c->arena_bytes;
-        ctl.result_cap = (unsigned long long)c->result_ints;
-        ctl.set_cap = (unsigned long long)set_cap;
-        ctl.stack_cap = (int)std::min<int64_t>(c->stack_slots / kStackShards, INT32_MAX);
         ctl.stack_top[0] = 1;
         ctl.pending = 1;
         CK(put_control(c, ctl, s));
@@ -796,20 +973,8 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(put_small(c, c->stack.p, &root, sizeof(root), s));
         int one = 1;
         CK(put_small(c, c->slot.p, &one, sizeof(one), s));
-
-        Rules rule{};
-        rule.off = rg->off.as<int64_t>();
-        rule.off2 = rg->off2.as<int64_t>();
-        rule.adj = rg->adj.as<int32_t>();
-        rule.adj2 = rg->adj2.as<int32_t>();
-        rule.md = c->md.as<int32_t>();
-        rule.ubt = c->ubt.as<int32_t>();
-        rule.mdlen = (int32_t)md.size();
-        rule.min_size = min_size;
-        rule.vbase = 0;
-        rule.n = h.n;
-        CK(c->rules.ensure(sizeof(Rules)));
         CK(put_small(c, c->rules.p, &rule, sizeof(rule), s));
+        }
         ExpandParams P{};
         P.rules = c->rules.as<Rules>();
         P.nrules = 1;
@@ -822,7 +987,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.ws = c->ws.as<char>();
         P.ws_stride = L.total;
         P.arena_cap = (unsigned long long)c->arena_bytes;
-        P.max_t = t;
+        P.max_t = tmax;
         P.smem_t = sh.smem_t;
         P.split = c->cfg.split > 0 ? c->cfg.split : 2;
         P.small_path = 1;
@@ -841,6 +1006,13 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         CK(cudaStreamSynchronize(s));
         float kms = 0;
         cudaEventElapsedTime(&kms, c->ev[1], c->ev[2]);
+        if (root_dev) {
+            t = ctl.root_t;
+            cov = ctl.root_cov;
+            if (t < 0 || t > tmax || cov < 0 || cov > t)
+                return fail(QC_ERR_CUDA, "level 0 size out of range");
+            r->st.root_size = (int64_t)t;
+        }
         record_last(c, ctl, kms, t);
 
         if (ctl.status & ST_TASK_OVERFLOW) {

@@ -67,6 +67,7 @@ struct Control {
     unsigned long long wait_fail_where; // diagnostic: which wait gave up
     unsigned long long check_site;      // first failed self-check: site id
     unsigned long long check_value;     //   ... and the offending value
+    int root_t, root_cov;          // the root task's size and covered count (device set-up)
     alignas(128) unsigned long long free_head[kArenaClasses * kArenaShards]; // [tag:24 | offset/16+1:40]
 };
 
