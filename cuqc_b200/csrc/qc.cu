@@ -989,7 +989,10 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = tmax;
         P.smem_t = sh.smem_t;
-        P.split = c->cfg.split > 0 ? c->cfg.split : 2;
+        // single instance: every branch of a large task its own item, so the
+        // root's branches start at once (the batched form keeps 2: there the
+        // work, not the start, bounds the run)
+        P.split = c->cfg.split > 0 ? c->cfg.split : 1;
         P.small_path = 1;
         P.shard = shard;
         P.nshards = nshards;
