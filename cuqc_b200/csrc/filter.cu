@@ -487,15 +487,33 @@ __global__ void maximal_kernel(const int32_t* srt, const unsigned long long* sta
 // and every maximal set is in the residual.
 // ---------------------------------------------------------------------------
 
-// every set into the table (slot = set index, -1 empty), by its hash
-__global__ void set_insert_kernel(const unsigned long long* hsh, int64_t nsets, int32_t* table,
-                                  unsigned long long mask)
+// A table entry: the set's index (low 32 bits), its size (capped at 255) and
+// 24 more bits of its hash, so that a probe rejects most sets that are not a
+// hit without reading them (all ones: an empty slot).
+__device__ __forceinline__ unsigned long long slot_entry(unsigned long long h, int k, int64_t s)
+{
+    return (((h >> 32) & 0xffffffull) << 40) | ((unsigned long long)(k < 255 ? k : 255) << 32) |
+           (unsigned long long)(uint32_t)s;
+}
+// does entry e stand for a set of hash h and size k (a candidate to check)?
+__device__ __forceinline__ bool slot_may_be(unsigned long long e, unsigned long long h, int k)
+{
+    return (e >> 32) == ((((h >> 32) & 0xffffffull) << 8) | (unsigned long long)(k < 255 ? k : 255));
+}
+constexpr unsigned long long kSlotEmpty = ~0ull;
+
+// every set into the table by its hash
+__global__ void set_insert_kernel(const unsigned long long* hsh, const int32_t* srt,
+                                  const unsigned long long* starts, int64_t nsets,
+                                  unsigned long long* table, unsigned long long mask)
 {
     const int64_t nt = (int64_t)gridDim.x * blockDim.x;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nsets; s += nt) {
-        unsigned long long p = hsh[s] & mask;
+        const unsigned long long h = hsh[s];
+        const unsigned long long e = slot_entry(h, srt[starts[s]], s);
+        unsigned long long p = h & mask;
         for (unsigned long long it = 0; it <= mask; it++) { // the table is never full
-            if (atomicCAS(&table[p], -1, (int32_t)s) == -1) break;
+            if (atomicCAS(&table[p], kSlotEmpty, e) == kSlotEmpty) break;
             p = (p + 1) & mask;
         }
     }
@@ -518,7 +536,7 @@ __device__ __forceinline__ bool thread_subset(const int32_t* A, int ka, const in
 // ids i, i+32, ..) and mark every emitted set equal to it; lane 0 also looks
 // up T's own hash for an exact copy of smaller index, which marks T.
 __global__ void one_less_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
-                                const unsigned long long* hsh, const int32_t* table,
+                                const unsigned long long* hsh, const unsigned long long* table,
                                 unsigned long long mask, int32_t* dead)
 {
     const int lane = threadIdx.x & 31;
@@ -534,9 +552,10 @@ __global__ void one_less_kernel(const int32_t* srt, const unsigned long long* st
                 const unsigned long long h = hT - id_mix(T[i]);
                 unsigned long long p = h & mask;
                 for (unsigned long long it = 0; it <= mask; it++) {
-                    const int32_t c = table[p];
-                    if (c < 0) break;
-                    if (hsh[c] == h) {
+                    const unsigned long long e = table[p];
+                    if (e == kSlotEmpty) break;
+                    const int32_t c = (int32_t)(uint32_t)e;
+                    if (slot_may_be(e, h, k - 1) && hsh[c] == h) {
                         const unsigned long long b = starts[c];
                         if (srt[b] == k - 1 && thread_subset(srt + b + 1, k - 1, T, k)) dead[c] = 1;
                     }
@@ -546,9 +565,10 @@ __global__ void one_less_kernel(const int32_t* srt, const unsigned long long* st
             if (lane == 0) {
                 unsigned long long p = hT & mask;
                 for (unsigned long long it = 0; it <= mask; it++) {
-                    const int32_t c = table[p];
-                    if (c < 0) break;
-                    if (c < s && hsh[c] == hT) {
+                    const unsigned long long e = table[p];
+                    if (e == kSlotEmpty) break;
+                    const int32_t c = (int32_t)(uint32_t)e;
+                    if (c < s && slot_may_be(e, hT, k) && hsh[c] == hT) {
                         const unsigned long long b = starts[c];
                         if (srt[b] == k && thread_subset(srt + b + 1, k, T, k)) {
                             dead[s] = 1;
@@ -573,13 +593,17 @@ __global__ void one_less_kernel(const int32_t* srt, const unsigned long long* st
         bool walking = prober;
         for (unsigned long long it = 0; it <= mask && __any_sync(0xffffffffu, walking); it++) {
             int32_t c = -1;
+            bool may = false;
             if (walking) {
-                c = table[p];
-                if (c < 0) walking = false;
-                else p = (p + 1) & mask;
+                const unsigned long long e = table[p];
+                if (e == kSlotEmpty) walking = false;
+                else {
+                    c = (int32_t)(uint32_t)e;
+                    may = slot_may_be(e, h, want);
+                    p = (p + 1) & mask;
+                }
             }
-            const bool hit = c >= 0 && hsh[c] == h && (lane < k || c < s) &&
-                             srt[starts[c]] == want;
+            const bool hit = may && (lane < k || c < s) && hsh[c] == h && srt[starts[c]] == want;
             unsigned pend = __ballot_sync(0xffffffffu, hit);
             while (pend) {
                 const int i = __ffs(pend) - 1;
@@ -600,16 +624,18 @@ __global__ void one_less_kernel(const int32_t* srt, const unsigned long long* st
 // (ctr[0] counts them, ctr[1] their ints)
 __global__ void residual_kernel(const int32_t* srt, const unsigned long long* starts, int64_t nsets,
                                 const int32_t* dead, const uint4* sig, unsigned long long* rstarts,
-                                uint4* rsig, unsigned long long* ctr)
+                                uint4* rsig, int32_t* rsz, unsigned long long* ctr)
 {
     const int64_t nt = (int64_t)gridDim.x * blockDim.x;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nsets; s += nt) {
         if (dead[s]) continue;
         const unsigned long long j = atomicAdd(&ctr[0], 1ull);
-        atomicAdd(&ctr[1], (unsigned long long)(srt[starts[s]] + 1));
+        const int k = srt[starts[s]];
+        atomicAdd(&ctr[1], (unsigned long long)(k + 1));
         rstarts[j] = starts[s];
         rsig[2 * j] = sig[2 * s];
         rsig[2 * j + 1] = sig[2 * s + 1];
+        rsz[j] = k;
     }
 }
 
@@ -622,8 +648,8 @@ constexpr int64_t kPairsMax = 4096;
 // unless a larger residual set contains it (signature test, then exact).
 // Maximal sets are appended to the output with their ordering entry.
 __global__ void residual_pairs_kernel(const int32_t* srt, const unsigned long long* rstarts,
-                                      const uint4* rsig, unsigned long long* ctr, int32_t* out,
-                                      SetEnt* ents)
+                                      const uint4* rsig, const int32_t* rsz, unsigned long long* ctr,
+                                      int32_t* out, SetEnt* ents)
 {
     const int64_t nr = (int64_t)ctr[4];
     if (nr > kPairsMax) return;
@@ -631,21 +657,30 @@ __global__ void residual_pairs_kernel(const int32_t* srt, const unsigned long lo
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nr; s += nw) {
         const unsigned long long a = rstarts[s];
-        const int k = srt[a];
+        const int k = rsz[s];
         const uint4 s0 = rsig[2 * s], s1 = rsig[2 * s + 1];
         bool covered = false;
-        for (int64_t base = 0; base < nr && !covered; base += 32) {
-            const int64_t t = base + lane;
-            bool pass = false;
-            if (t < nr && t != s && srt[rstarts[t]] > k) {
-                const uint4 t0 = rsig[2 * t], t1 = rsig[2 * t + 1];
-                pass = sig_covers(s0, s1, t0, t1);
+        // four chunks of 32 candidates per step, their sizes and signatures
+        // loaded together
+        for (int64_t base = 0; base < nr && !covered; base += 128) {
+            bool pass[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int64_t t = base + 32 * u + lane;
+                pass[u] = false;
+                if (t < nr && t != s && rsz[t] > k) {
+                    const uint4 t0 = rsig[2 * t], t1 = rsig[2 * t + 1];
+                    pass[u] = sig_covers(s0, s1, t0, t1);
+                }
             }
-            unsigned pb = __ballot_sync(0xffffffffu, pass);
-            while (pb && !covered) {
-                const int c = __ffs(pb) - 1;
-                pb &= pb - 1;
-                covered = warp_subset(srt, a, k, rstarts[base + c], lane);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                unsigned pb = __ballot_sync(0xffffffffu, pass[u]);
+                while (pb && !covered) {
+                    const int c = __ffs(pb) - 1;
+                    pb &= pb - 1;
+                    covered = warp_subset(srt, a, k, rstarts[base + 32 * u + c], lane);
+                }
             }
         }
         if (covered) continue;
@@ -708,12 +743,12 @@ void FilterScratch::release()
     host = nullptr;
     host_n = 0;
     for (auto* pp : {&sorted, &sig, &poff, &post, &ctr, &ents, &bents, &temp, &ikey, &ikey2,
-                     &ival, &rsig, &hsh, &table, &dead, &rstarts, &ikey3, &bents2}) {
+                     &ival, &rsig, &hsh, &table, &dead, &rstarts, &ikey3, &bents2, &rsz}) {
         if (*pp) cudaFree(*pp);
         *pp = nullptr;
     }
     sorted_n = sig_n = poff_n = post_n = ctr_n = ents_n = bents_n = temp_n = ikey_n = ikey2_n =
-        ival_n = rsig_n = hsh_n = table_n = dead_n = rstarts_n = ikey3_n = bents2_n = 0;
+        ival_n = rsig_n = hsh_n = table_n = dead_n = rstarts_n = ikey3_n = bents2_n = rsz_n = 0;
 }
 
 std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints,
@@ -736,9 +771,10 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     ENS(sig, sig_n, 2 * sizeof(uint4) * nsets);
     ENS(rsig, rsig_n, 2 * sizeof(uint4) * nsets);
     ENS(hsh, hsh_n, sizeof(unsigned long long) * nsets);
-    ENS(table, table_n, sizeof(int32_t) * cap);
+    ENS(table, table_n, sizeof(unsigned long long) * cap);
     ENS(dead, dead_n, sizeof(int32_t) * nsets);
     ENS(rstarts, rstarts_n, sizeof(unsigned long long) * nsets);
+    ENS(rsz, rsz_n, sizeof(int32_t) * nsets);
     ENS(poff, poff_n, sizeof(int64_t) * (nv + 1));
     ENS(ctr, ctr_n, 8 * sizeof(unsigned long long));
     ENS(ents, ents_n, sizeof(SetEnt) * nsets);
@@ -751,23 +787,25 @@ std::string filter_maximal(FilterScratch& F, const int32_t* d_res, int64_t nints
     int64_t nlaunch = 0;
     sort_sig_kernel<<<blocks, 256, 0, s>>>(d_res, d_starts, nsets, (int32_t*)F.sorted,
                                            (uint4*)F.sig, (unsigned long long*)F.hsh);
-    FCK(cudaMemsetAsync(F.table, 0xff, sizeof(int32_t) * cap, s));
+    FCK(cudaMemsetAsync(F.table, 0xff, sizeof(unsigned long long) * cap, s));
     FCK(cudaMemsetAsync(F.dead, 0, sizeof(int32_t) * nsets, s));
     FCK(cudaMemsetAsync(ctr, 0, 8 * sizeof(unsigned long long), s));
-    set_insert_kernel<<<blocks, 256, 0, s>>>((const unsigned long long*)F.hsh, nsets,
-                                             (int32_t*)F.table, (unsigned long long)(cap - 1));
+    set_insert_kernel<<<blocks, 256, 0, s>>>((const unsigned long long*)F.hsh, (const int32_t*)F.sorted,
+                                             d_starts, nsets, (unsigned long long*)F.table,
+                                             (unsigned long long)(cap - 1));
     one_less_kernel<<<blocks, 256, 0, s>>>((const int32_t*)F.sorted, d_starts, nsets,
                                            (const unsigned long long*)F.hsh,
-                                           (const int32_t*)F.table, (unsigned long long)(cap - 1),
+                                           (const unsigned long long*)F.table, (unsigned long long)(cap - 1),
                                            (int32_t*)F.dead);
     residual_kernel<<<blocks, 256, 0, s>>>((const int32_t*)F.sorted, d_starts, nsets,
                                            (const int32_t*)F.dead, (const uint4*)F.sig,
                                            (unsigned long long*)F.rstarts, (uint4*)F.rsig,
-                                           ctr + 4);
+                                           (int32_t*)F.rsz, ctr + 4);
     int32_t* d_out = (int32_t*)F.ikey;
     residual_pairs_kernel<<<blocks, 256, 0, s>>>((const int32_t*)F.sorted,
                                                  (const unsigned long long*)F.rstarts,
-                                                 (const uint4*)F.rsig, ctr, d_out, (SetEnt*)F.ents);
+                                                 (const uint4*)F.rsig, (const int32_t*)F.rsz, ctr,
+                                                 d_out, (SetEnt*)F.ents);
     nlaunch += 5;
     // the survivors' universe: presence bitmap and ranks over the vertex range
     // (in the posting-list offsets' buffer)

@@ -13,10 +13,10 @@ struct FilterScratch {
     void *sorted = nullptr, *sig = nullptr, *poff = nullptr, *post = nullptr, *ctr = nullptr, *ents = nullptr, *bents = nullptr,
          *temp = nullptr, *ikey = nullptr, *ikey2 = nullptr, *ival = nullptr, *rsig = nullptr,
          *hsh = nullptr, *table = nullptr, *dead = nullptr, *rstarts = nullptr, *ikey3 = nullptr,
-         *bents2 = nullptr;
+         *bents2 = nullptr, *rsz = nullptr;
     size_t sorted_n = 0, sig_n = 0, poff_n = 0, post_n = 0, ctr_n = 0, ents_n = 0, bents_n = 0,
            temp_n = 0, ikey_n = 0, ikey2_n = 0, ival_n = 0, rsig_n = 0, hsh_n = 0, table_n = 0,
-           dead_n = 0, rstarts_n = 0, ikey3_n = 0, bents2_n = 0;
+           dead_n = 0, rstarts_n = 0, ikey3_n = 0, bents2_n = 0, rsz_n = 0;
     // page-locked host buffer the survivors are read back into (grown on demand)
     int32_t* host = nullptr;
     size_t host_n = 0;

@@ -115,6 +115,21 @@ __device__ void level0_block(const int64_t* off, const int32_t* adj, const int64
     }
     __syncthreads();
     const int t = cnt;
+    if ((int64_t)t * t <= 4096ll * nt) {
+        // few survivors: each key's place is the number of smaller keys (the
+        // keys are distinct: they end in the vertex id)
+        for (int i = tid; i < t; i += nt) {
+            const unsigned long long k = keys[i];
+            int r = 0;
+            for (int j = 0; j < t; j++) r += keys[j] < k ? 1 : 0;
+            ids[r] = 0x1ffff - (int)(k & 0x1ffffull);
+        }
+        if (tid == 0) {
+            info[0] = t;
+            info[1] = ncov;
+        }
+        return;
+    }
     int N = 1;
     while (N < t) N <<= 1;
     for (int i = t + tid; i < N; i += nt) keys[i] = ~0ull;

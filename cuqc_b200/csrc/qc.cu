@@ -456,28 +456,30 @@ __global__ void __launch_bounds__(256) root_setup_kernel(RootSetup S, const int3
 }
 
 // root_rows_kernel and the positions' reset for a root whose size is on the
-// device (root_setup_kernel wrote the record when it fits the arena)
-__global__ void root_rows_dev_kernel(const int64_t* off, const int32_t* adj, const int64_t* off2,
-                                     const int32_t* adj2, const int32_t* ids, const int32_t* info,
-                                     const int32_t* pos, char* arena, unsigned long long arena_cap)
+// device (root_setup_kernel wrote the record when it fits the arena).  A
+// block per root vertex (blocks beyond the root's size return at once): its
+// threads share the vertex's 1-hop and 2-hop rows, so the long 2-hop rows
+// are read by many loads in flight.
+__global__ void __launch_bounds__(256) root_rows_dev_kernel(const int64_t* off, const int32_t* adj,
+                                                            const int64_t* off2, const int32_t* adj2,
+                                                            const int32_t* ids, const int32_t* info,
+                                                            const int32_t* pos, char* arena,
+                                                            unsigned long long arena_cap)
 {
     const int t = info[0], W = words_for(t);
     if (t <= 0 || arena_class_bytes(arena_class(rec_block_bytes(t, W))) > arena_cap) return;
     uint32_t* A1 = (uint32_t*)(arena + rec_a1_off(t));
     uint32_t* A2 = (uint32_t*)(arena + rec_a2_off(t, W));
-    int lane = threadIdx.x & 31;
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < t; i += nw) {
-        int u = ids[i];
+    for (int i = blockIdx.x; i < t; i += gridDim.x) {
+        const int u = ids[i];
         uint32_t* r1 = A1 + (int64_t)i * W;
         uint32_t* r2 = A2 + (int64_t)i * W;
-        for (int64_t e = off[u] + lane; e < off[u + 1]; e += 32) {
-            int p = pos[adj[e]];
+        for (int64_t e = off[u] + threadIdx.x; e < off[u + 1]; e += blockDim.x) {
+            const int p = pos[adj[e]];
             if (p >= 0) atomicOr(&r1[p >> 5], 1u << (p & 31));
         }
-        for (int64_t e = off2[u] + lane; e < off2[u + 1]; e += 32) {
-            int p = pos[adj2[e]];
+        for (int64_t e = off2[u] + threadIdx.x; e < off2[u + 1]; e += blockDim.x) {
+            const int p = pos[adj2[e]];
             if (p >= 0) atomicOr(&r2[p >> 5], 1u << (p & 31));
         }
     }
@@ -918,7 +920,7 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
                                                 (unsigned long long)c->arena_bytes, c->ctl.as<Control>(),
                                                 c->stack.as<StackEntry>(), c->slot.as<int32_t>(),
                                                 c->rules.as<Rules>(), c->pos.as<int32_t>());
-            root_rows_dev_kernel<<<std::max(1, std::min(blocks * 4, (tmax + 7) / 8)), 256, 0, s>>>(
+            root_rows_dev_kernel<<<std::max(1, std::min(tmax, c->sms * 8)), 256, 0, s>>>(
                 rg->off.as<int64_t>(), rg->adj.as<int32_t>(), rg->off2.as<int64_t>(),
                 rg->adj2.as<int32_t>(), c->ids.as<int32_t>(), d_info, c->pos.as<int32_t>(),
                 c->arena.as<char>(), (unsigned long long)c->arena_bytes);
