@@ -1239,6 +1239,9 @@ __device__ QC_BIG_FN void sort_keys(Ws& ws, int n)
     }
 }
 
+// children of at most this many vertices are ordered by counting ranks
+constexpr int kRankOrderMax = 256;
+
 __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
                             int m, const uint32_t* Rm, int nr)
 {
@@ -1269,7 +1272,27 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
         written += __popc(bal);
     }
     __syncwarp();
-    sort_keys(ws, tc);
+    // The child's order.  A child of up to kRankOrderMax vertices: each
+    // vertex's place is the number of smaller keys (the keys are distinct:
+    // they end in the id), with the keys read by all lanes at once; a larger
+    // one: the bitonic sort of the keys.
+    const int32_t* order = ws.sel();
+    if (tc <= kRankOrderMax) {
+        int32_t* dst = ws.vlist();
+        for (int e = lane; e < tc; e += 32) {
+            const unsigned long long h = ws.khi()[e], l = ws.klo()[e];
+            int r = 0;
+            for (int j = 0; j < tc; j++) {
+                const unsigned long long hj = ws.khi()[j], lj = ws.klo()[j];
+                r += (hj < h || (hj == h && lj < l)) ? 1 : 0;
+            }
+            dst[r] = ws.sel()[e];
+        }
+        __syncwarp();
+        order = dst;
+    } else {
+        sort_keys(ws, tc);
+    }
     int Wc = words_for(tc);
     unsigned long long bytes = rec_block_bytes(tc, Wc);
     unsigned long long at = 0;
@@ -1294,37 +1317,76 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     uint32_t* c1 = (uint32_t*)(rec + rec_a1_off(tc));
     uint32_t* c2 = (uint32_t*)(rec + rec_a2_off(tc, Wc));
     for (int i = lane; i < tc; i += 32) {
-        cid[i] = rec_ld(T.ids + ws.sel()[i]);
+        cid[i] = rec_ld(T.ids + order[i]);
         cl2[i] = 0;
     }
-    // compacted rows: child bit j of row i = parent bit sel[j] of row sel[i].
-    // Column word w: lane k holds the parent column sel[w*32+k]; rows go by in
-    // groups of 32 (lane r holds the parent row of child row i0+r), and the
-    // reads of different rows do not depend on each other.
-    for (int w = 0; w < Wc; w++) {
-        const int j = w * 32 + lane;
-        const int pj = j < tc ? ws.sel()[j] : 0;
-        const int pw = pj >> 5, pb = pj & 31;
-        const bool col = j < tc;
+    // compacted rows: child bit j of row i = parent bit order[j] of row
+    // order[i].  A parent of at most 8 words a row: lane r takes child row
+    // i0 + r, holds its parent row's words in registers and picks the child's
+    // columns from them, the columns' parent positions passed round the warp.
+    if (T.W <= 8) {
         for (int i0 = 0; i0 < tc; i0 += 32) {
-            const int rows = tc - i0 < 32 ? tc - i0 : 32;
-            const int my_row = lane < rows ? ws.sel()[i0 + lane] : 0;
-            unsigned o1 = 0, o2 = 0;
-#pragma unroll 4
-            for (int r = 0; r < rows; r++) {
-                const int64_t base = (int64_t)__shfl_sync(QC_FULL, my_row, r) * T.W + pw;
-                const uint32_t x1 = col ? rec_ld(T.A1 + base) : 0u;
-                const uint32_t x2 = col ? rec_ld(T.A2 + base) : 0u;
-                const unsigned w1 = __ballot_sync(QC_FULL, (x1 >> pb) & 1u);
-                const unsigned w2 = __ballot_sync(QC_FULL, (x2 >> pb) & 1u);
-                if (lane == r) {
-                    o1 = w1;
-                    o2 = w2;
+            const int row = i0 + lane;
+            const int src = row < tc ? order[row] : -1;
+            uint32_t a1w[8], a2w[8];
+#pragma unroll
+            for (int w = 0; w < 8; w++) {
+                const bool ok = src >= 0 && w < T.W;
+                a1w[w] = ok ? rec_ld(T.A1 + (int64_t)src * T.W + w) : 0u;
+                a2w[w] = ok ? rec_ld(T.A2 + (int64_t)src * T.W + w) : 0u;
+            }
+            for (int cw = 0; cw < Wc; cw++) {
+                const int jn = tc - cw * 32 < 32 ? tc - cw * 32 : 32;
+                const int my_col = lane < jn ? order[cw * 32 + lane] : 0;
+                uint32_t o1 = 0, o2 = 0;
+                for (int b = 0; b < jn; b++) {
+                    const int pj = __shfl_sync(QC_FULL, my_col, b);
+                    const int pw = pj >> 5, pb = pj & 31;
+                    uint32_t x1 = a1w[0], x2 = a2w[0];
+#pragma unroll
+                    for (int w = 1; w < 8; w++)
+                        if (pw == w) {
+                            x1 = a1w[w];
+                            x2 = a2w[w];
+                        }
+                    o1 |= ((x1 >> pb) & 1u) << b;
+                    o2 |= ((x2 >> pb) & 1u) << b;
+                }
+                if (row < tc) {
+                    c1[(int64_t)row * Wc + cw] = o1;
+                    c2[(int64_t)row * Wc + cw] = o2;
                 }
             }
-            if (lane < rows) {
-                c1[(int64_t)(i0 + lane) * Wc + w] = o1;
-                c2[(int64_t)(i0 + lane) * Wc + w] = o2;
+        }
+    } else {
+        // Column word w: lane k holds the parent column order[w*32+k]; rows go by in
+        // groups of 32 (lane r holds the parent row of child row i0+r), and the
+        // reads of different rows do not depend on each other.
+        for (int w = 0; w < Wc; w++) {
+            const int j = w * 32 + lane;
+            const int pj = j < tc ? order[j] : 0;
+            const int pw = pj >> 5, pb = pj & 31;
+            const bool col = j < tc;
+            for (int i0 = 0; i0 < tc; i0 += 32) {
+                const int rows = tc - i0 < 32 ? tc - i0 : 32;
+                const int my_row = lane < rows ? order[i0 + lane] : 0;
+                unsigned o1 = 0, o2 = 0;
+    #pragma unroll 4
+                for (int r = 0; r < rows; r++) {
+                    const int64_t base = (int64_t)__shfl_sync(QC_FULL, my_row, r) * T.W + pw;
+                    const uint32_t x1 = col ? rec_ld(T.A1 + base) : 0u;
+                    const uint32_t x2 = col ? rec_ld(T.A2 + base) : 0u;
+                    const unsigned w1 = __ballot_sync(QC_FULL, (x1 >> pb) & 1u);
+                    const unsigned w2 = __ballot_sync(QC_FULL, (x2 >> pb) & 1u);
+                    if (lane == r) {
+                        o1 = w1;
+                        o2 = w2;
+                    }
+                }
+                if (lane < rows) {
+                    c1[(int64_t)(i0 + lane) * Wc + w] = o1;
+                    c2[(int64_t)(i0 + lane) * Wc + w] = o2;
+                }
             }
         }
     }
