@@ -205,10 +205,10 @@ std::string write_binary(const HostGraph& g, const char* path)
 // ids in [0, n), checked with branch-free passes the compiler vectorises (a
 // row's ids are in range when its first and last are); the exact message is
 // looked up only for a failing row.
-static std::string check_rows(const int64_t* off, const int32_t* adj, int32_t n, bool no_self,
-                              const char* what)
+static std::string check_rows_range(const int64_t* off, const int32_t* adj, int32_t n, int32_t v0,
+                                    int32_t v1, bool no_self, const char* what)
 {
-    for (int32_t v = 0; v < n; v++) {
+    for (int32_t v = v0; v < v1; v++) {
         const int64_t a = off[v], b = off[(size_t)v + 1];
         if (b < a) return std::string(what) + " offsets decrease";
         if (a == b) continue;
@@ -226,6 +226,38 @@ static std::string check_rows(const int64_t* off, const int32_t* adj, int32_t n,
                 return std::string(what) + " rows must be sorted ascending without duplicates";
         }
     }
+    return "";
+}
+
+// The rows of vertices [0, n): sorted, without repeats, ids in range (and no
+// self loop).  Large arrays are checked by several host threads, each a
+// range of vertices; the first failing range's message is returned.
+static std::string check_rows(const int64_t* off, const int32_t* adj, int32_t n, bool no_self,
+                              const char* what)
+{
+    // offsets first: every row must lie inside the array before it is read
+    for (int32_t v = 0; v < n; v++)
+        if (off[(size_t)v + 1] < off[v]) return std::string(what) + " offsets decrease";
+    const int64_t entries = n > 0 ? off[n] - off[0] : 0;
+    const int par = entries >= (1 << 22) ? (int)std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    if (par <= 1) return check_rows_range(off, adj, n, 0, n, no_self, what);
+    std::vector<std::string> err((size_t)par);
+    std::vector<std::thread> th;
+    // ranges of about equal entry counts
+    int32_t v0 = 0;
+    for (int p = 0; p < par; p++) {
+        int32_t v1 = n;
+        if (p + 1 < par) {
+            const int64_t want = off[0] + entries * (p + 1) / par;
+            v1 = (int32_t)(std::lower_bound(off, off + n + 1, want) - off);
+            v1 = std::max(v0, std::min(v1, n));
+        }
+        th.emplace_back([&, p, v0, v1] { err[(size_t)p] = check_rows_range(off, adj, n, v0, v1, no_self, what); });
+        v0 = v1;
+    }
+    for (auto& t : th) t.join();
+    for (auto& e : err)
+        if (!e.empty()) return e;
     return "";
 }
 

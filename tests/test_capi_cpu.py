@@ -165,3 +165,15 @@ def test_binary_round_trip_through_abi():
             h = Q.C.c_void_p()
             Q._check(Q.lib().qc_graph_read_binary(bad.encode(), Q.C.byref(h)))
         assert e.value.status == 3 and msg in str(e.value)
+
+
+def test_an_offset_past_the_rows_is_rejected_before_any_row_is_read():
+    # a middle offset beyond the array's end (the total still right): the
+    # offsets are checked before a row is read, so nothing past the array is
+    g = graphs.random_small(24, 0.3, 5)
+    off2 = g.off2.copy()
+    off2[3] = int(g.off2[-1]) + 1000
+    bad = graphs.Graph(n=g.n, off=g.off, adj=g.adj, off2=off2, adj2=g.adj2)
+    with pytest.raises(Q.QCError) as e:
+        Q.DeviceGraph.from_graph(bad)
+    assert e.value.status == 3 and "offsets decrease" in str(e.value)
