@@ -2351,17 +2351,21 @@ __device__ bool process_item(const ExpandParams& P, Ws& wsg, Ws& wss, char* stag
         q_hi = t - 1;
         if (m + T.cov >= t) return shared; // no branchable candidate
         int nb = q_hi - q_lo + 1;
-        if (nb > P.split) {
+        // branches per item: as configured, else one for a task of up to 256
+        // vertices (its branches start at once) and two above (a huge root's
+        // thousands of branches would otherwise crowd out its own children)
+        const int split = P.split > 0 ? P.split : (t <= 256 ? 1 : 2);
+        if (nb > split) {
             __syncwarp();
             __threadfence();
             // every range but the first goes to the shared stack, all at once;
             // the references are counted before any range is published
-            const int extra = (q_hi - P.split - q_lo) / P.split + 1;
+            const int extra = (q_hi - split - q_lo) / split + 1;
             if (lane == 0) atomicAdd(&((TaskHdr*)(P.arena + it.rec))->refs, extra);
             __syncwarp();
-            push_ranges(P, it.rec, q_lo, q_hi - P.split, P.split, extra);
+            push_ranges(P, it.rec, q_lo, q_hi - split, split, extra);
             __syncwarp();
-            q_lo = q_hi - P.split + 1;
+            q_lo = q_hi - split + 1;
             shared = true;
         }
     }

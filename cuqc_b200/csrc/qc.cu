@@ -586,14 +586,20 @@ static qc_status launch_shape(qc_context* c, int max_t, Shape& sh)
     const size_t sm_budget = 220u << 10; // of the 228 KB of shared memory per SM
     sh.smem_t = 0;
     if (max_t > 32 && c->cfg.stage_max >= 0) {
-        // the largest task size (up to 256) whose buffers fit
-        int hi = std::min(256, max_t);
-        if (c->cfg.stage_max > 0) hi = std::min(hi, c->cfg.stage_max);
-        for (int tt = hi; tt > 32; tt--)
+        // the first of these sizes whose buffers fit; no finer: the shared
+        // memory staging takes is the L1 cache's loss, and tasks too large to
+        // stage keep their workspace in global memory, read through L1 (a
+        // stage fitted to the last vertex, 156 for 8 warps, left config 2's
+        // large tasks 26 times slower)
+        for (int cand : {256, 192, 128, 96, 64}) {
+            int tt = std::min(cand, max_t);
+            if (c->cfg.stage_max > 0) tt = std::min(tt, c->cfg.stage_max);
+            if (tt <= 32) break;
             if (warp_smem_bytes(tt) * sh.wpb * want_bps <= sm_budget) {
                 sh.smem_t = tt;
                 break;
             }
+        }
     }
     sh.smem_bytes = expand_smem_bytes(sh.wpb, sh.smem_t);
     {
@@ -991,10 +997,10 @@ static qc_status mine_one(qc_context* c, const qc_graph* g, double gamma, int32_
         P.arena_cap = (unsigned long long)c->arena_bytes;
         P.max_t = tmax;
         P.smem_t = sh.smem_t;
-        // single instance: every branch of a large task its own item, so the
-        // root's branches start at once (the batched form keeps 2: there the
-        // work, not the start, bounds the run)
-        P.split = c->cfg.split > 0 ? c->cfg.split : 1;
+        // single instance: 0 lets the kernel choose by task size (one branch
+        // an item up to 256 vertices, two above); the batched form keeps 2,
+        // since there the work, not the start, bounds the run
+        P.split = c->cfg.split > 0 ? c->cfg.split : 0;
         P.small_path = 1;
         P.shard = shard;
         P.nshards = nshards;

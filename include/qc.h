@@ -144,7 +144,8 @@ typedef struct {
     int32_t wait_limit_ms;       /* bound on any device wait without progress; 0: 10000 */
     int32_t time_limit_ms;       /* stop a run after this long (QC_ERR_ITER_LIMIT); 0: none */
     int32_t split;               /* branches per work item of a task over 32 vertices;
-                                    0: 1 for qc_mine, 2 for qc_mine_batch */
+                                    0: for qc_mine 1 up to 256 vertices and 2 above,
+                                    for qc_mine_batch 2 */
     int32_t max_blocks;          /* cap on the persistent grid (share the GPU between
                                     contexts running at once); 0: every resident block */
     int32_t stage_max;           /* largest task (vertices) worked on in shared memory;
