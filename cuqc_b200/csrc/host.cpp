@@ -205,6 +205,11 @@ std::string write_binary(const HostGraph& g, const char* path)
 // ids in [0, n), checked with branch-free passes the compiler vectorises (a
 // row's ids are in range when its first and last are); the exact message is
 // looked up only for a failing row.
+// (built twice, for AVX2 and for any x86-64, and picked when the library
+// loads: the sortedness test is one compare per entry over every row)
+#if defined(__x86_64__) && defined(__GNUC__)
+__attribute__((target_clones("avx2", "default")))
+#endif
 static std::string check_rows_range(const int64_t* off, const int32_t* adj, int32_t n, int32_t v0,
                                     int32_t v1, bool no_self, const char* what)
 {
