@@ -94,6 +94,26 @@ def test_small_arena_grows_and_stays_exact():
     assert res.sets == oracle.solve(g, 0.8, 10)[0]
 
 
+def test_root_larger_than_the_arena_grows_it():
+    # the root's record is set up on the device: a block larger than the arena
+    # stops the launch at once and the host grows the arena and runs again
+    g = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
+    with Q.Context(device=0, arena_bytes=1 << 10) as c:
+        res = c.mine(g, 0.8, 10)
+    assert res.sets == oracle.solve(g, 0.8, 10)[0]
+    assert res.stats["root_size"] == len(oracle.root(g, 0.8, 10)[0])
+
+
+def test_root_emptied_by_peeling(ctx):
+    # a star: the centre passes level 0's first test (degree and two-hop size)
+    # but keeps no neighbour, so the root is empty only after peeling, which
+    # the device learns after the host has set up the launch
+    n = 21
+    g = graphs.from_edges(n, [0] * (n - 1), list(range(1, n)))
+    res = ctx.mine(g, 1.0, 3)
+    assert res.sets == [] and res.stats["root_size"] == 0 and res.stats["tasks"] == 0
+
+
 def test_repeated_calls_reuse_context(ctx):
     g = graphs.erdos_renyi_planted(300, 0.03, 3, 16, 0.95, seed=11)
     a = ctx.mine(g, 0.8, 10).sets
