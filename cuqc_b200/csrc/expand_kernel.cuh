@@ -1239,9 +1239,6 @@ __device__ QC_BIG_FN void sort_keys(Ws& ws, int n)
     }
 }
 
-// children of at most this many vertices are ordered by counting ranks
-constexpr int kRankOrderMax = 256;
-
 __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, const TaskView& T, Ws& ws, const uint32_t* M,
                             int m, const uint32_t* Rm, int nr)
 {

@@ -583,15 +583,19 @@ static qc_status launch_shape(qc_context* c, int max_t, Shape& sh)
     // sub-partition, so one hides the other's latency).
     sh.wpb = c->cfg.warps_per_block > 0 ? std::min(c->cfg.warps_per_block, 8) : 8;
     const int want_bps = c->cfg.blocks_per_sm > 0 ? c->cfg.blocks_per_sm : 1;
-    const size_t sm_budget = 220u << 10; // of the 228 KB of shared memory per SM
+    // Of the SM's 256 KB of L1 and shared memory, the 196 KB carve-out (195
+    // KB for the blocks plus 1 KB each reserved) leaves 60 KB of L1; the
+    // next, 228 KB, leaves 28 KB.
+    const size_t sm_budget = 195u << 10;
     sh.smem_t = 0;
     if (max_t > 32 && c->cfg.stage_max >= 0) {
         // the first of these sizes whose buffers fit; no finer: the shared
         // memory staging takes is the L1 cache's loss, and tasks too large to
         // stage keep their workspace in global memory, read through L1 (a
-        // stage fitted to the last vertex, 156 for 8 warps, left config 2's
-        // large tasks 26 times slower)
-        for (int cand : {256, 192, 128, 96, 64}) {
+        // stage fitted to the last vertex, 156 for 8 warps in the 228 KB
+        // carve-out, left config 2's large tasks 26 times slower).  Eight
+        // warps stage 160 vertices: config 1's 150-vertex root among them.
+        for (int cand : {256, 192, 160, 128, 96, 64}) {
             int tt = std::min(cand, max_t);
             if (c->cfg.stage_max > 0) tt = std::min(tt, c->cfg.stage_max);
             if (tt <= 32) break;

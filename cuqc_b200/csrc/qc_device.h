@@ -273,13 +273,23 @@ struct WsLayout {
     int64_t total;
 };
 
+// Children of at most this many vertices are ordered by counting ranks, larger
+// ones by a bitonic sort of their keys.
+constexpr int kRankOrderMax = 256;
+
+// Every array is indexed by a position below max_t, the histograms and their
+// prefixes by a bin up to max_t + 1; the sort keys of a child larger than
+// kRankOrderMax pad to a power of two.  No slack beyond that: a workspace of
+// 160 vertices then fits 8 warps within the 196 KB shared-memory carve-out.
 __host__ __device__ inline WsLayout ws_layout(int max_t)
 {
     WsLayout L;
-    int64_t t = max_t + 64;
-    int64_t tp = 1; // the child sort pads to a power of two
-    while (tp < max_t) tp <<= 1;
-    tp += 64;
+    int64_t t = max_t + 2;
+    int64_t tp = max_t;
+    if (max_t > kRankOrderMax) {
+        tp = 1;
+        while (tp < max_t) tp <<= 1;
+    }
     int64_t W = words_for(max_t) + 2;
     int64_t o = 0;
     L.indeg = o;    o += align16(4 * t);
