@@ -94,6 +94,27 @@ def test_small_arena_grows_and_stays_exact():
     assert res.sets == oracle.solve(g, 0.8, 10)[0]
 
 
+@pytest.mark.parametrize("wpb", [8, 2])
+def test_children_above_the_counting_rank_limit(ctx, wpb):
+    # one group of 300 at density 0.88 with min_size 270: every child keeps at
+    # least 270 vertices, so each is ordered by the bitonic sort of keys padded
+    # to a power of two (children of up to 256 vertices take counting ranks)
+    # and worked on with its workspace in global memory (8 warps stage tasks of
+    # up to 160 vertices, 2 warps up to 256)
+    g = graphs.erdos_renyi_planted(600, 0.02, 1, 300, 0.88, seed=1)
+    want_flat, st = oracle.mine(g, 0.9, 270, "clean")
+    assert st["children"] > 0 and st["child_vertices"] >= 270 * st["children"]
+    if wpb == 8:
+        res = ctx.mine(g, 0.9, 270)
+    else:
+        with Q.Context(device=0, warps_per_block=wpb, keep_emitted=True) as c:
+            res = c.mine(g, 0.9, 270)
+    assert canon(res.emitted) == canon(want_flat)
+    assert res.sets == oracle.maximal(want_flat)
+    for k in ("tasks", "branches", "children", "parent_vertices", "p_rows", "child_vertices"):
+        assert res.stats[k] == st[k], k
+
+
 def test_root_larger_than_the_arena_grows_it():
     # the root's record is set up on the device: a block larger than the arena
     # stops the launch at once and the host grows the arena and runs again
