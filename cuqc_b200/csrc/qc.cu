@@ -14,10 +14,12 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -295,6 +297,27 @@ extern "C" qc_status qc_graph_read_serialized(const char* path, qc_graph** out)
     return QC_OK;
 }
 
+// Copy one caller CSR (n + 1 offsets, then off[n] ids) into the graph.  The
+// offsets' ends are checked before anything is copied: a negative or
+// impossible entry count would otherwise size the copy itself.  With n = 0
+// the offsets may be NULL (one offset, 0).
+static qc_status adopt_rows(int32_t n, const int64_t* off, const int32_t* adj, const char* what,
+                            const char* adj_name, std::vector<int64_t>& o, std::vector<int32_t>& a)
+{
+    static const int64_t zero = 0;
+    if (n == 0 && !off) off = &zero;
+    if (off[0] != 0 || off[n] < 0 || off[n] > (int64_t)(PTRDIFF_MAX / sizeof(int32_t)))
+        return fail(QC_ERR_FORMAT, std::string(what) + " offsets must start at 0 and end at the entry count");
+    if (off[n] > 0 && !adj) return fail(QC_ERR_ARGS, std::string(adj_name) + " is NULL");
+    try {
+        o.assign(off, off + n + 1);
+        a.assign(adj, adj + off[n]);
+    } catch (const std::bad_alloc&) {
+        return fail(QC_ERR_NOMEM, std::string("host copy of the ") + what + " lists");
+    }
+    return QC_OK;
+}
+
 extern "C" qc_status qc_graph_from_csr2(int32_t n, const int64_t* off, const int32_t* adj,
                                         const int64_t* off2, const int32_t* adj2, qc_graph** out)
 {
@@ -302,12 +325,10 @@ extern "C" qc_status qc_graph_from_csr2(int32_t n, const int64_t* off, const int
     *out = nullptr;
     std::unique_ptr<qc_graph> g(new qc_graph());
     g->h.n = n;
-    g->h.off.assign(off, off + n + 1);
-    if (off[n] > 0 && !adj) return fail(QC_ERR_ARGS, "adj is NULL");
-    g->h.adj.assign(adj, adj + off[n]);
-    g->h.off2.assign(off2, off2 + n + 1);
-    if (off2[n] > 0 && !adj2) return fail(QC_ERR_ARGS, "adj2 is NULL");
-    g->h.adj2.assign(adj2, adj2 + off2[n]);
+    qc_status as = adopt_rows(n, off, adj, "1-hop", "adj", g->h.off, g->h.adj);
+    if (as != QC_OK) return as;
+    as = adopt_rows(n, off2, adj2, "2-hop", "adj2", g->h.off2, g->h.adj2);
+    if (as != QC_OK) return as;
     std::string e = validate(g->h, true);
     if (!e.empty()) return fail(QC_ERR_FORMAT, e);
     *out = g.release();
@@ -1925,9 +1946,8 @@ extern "C" qc_status qc_graph_from_csr(int32_t n, const int64_t* off, const int3
     *out = nullptr;
     std::unique_ptr<qc_graph> g(new qc_graph());
     g->h.n = n;
-    g->h.off.assign(off, off + n + 1);
-    if (off[n] > 0 && !adj) return fail(QC_ERR_ARGS, "adj is NULL");
-    g->h.adj.assign(adj, adj + off[n]);
+    qc_status as = adopt_rows(n, off, adj, "1-hop", "adj", g->h.off, g->h.adj);
+    if (as != QC_OK) return as;
     std::string e = validate(g->h, false);
     if (!e.empty()) return fail(QC_ERR_FORMAT, e);
     int ndev = 0;

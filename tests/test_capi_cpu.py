@@ -117,6 +117,25 @@ def test_malformed_twohop_lists_are_rejected(mutate, msg):
     assert e.value.status == 3 and msg in str(e.value)
 
 
+@pytest.mark.parametrize("which,end", [("1-hop", -1), ("2-hop", -5), ("1-hop", 1 << 62),
+                                        ("2-hop", "start")])
+def test_offsets_are_checked_before_the_rows_are_copied(which, end):
+    # a negative or impossible entry count, or offsets not starting at 0, is a
+    # format error returned before any row is read (the count would otherwise
+    # size the copy of the caller's ids)
+    g = graphs.random_small(16, 0.3, 2)
+    off, off2 = g.off.copy(), g.off2.copy()
+    o = off if which == "1-hop" else off2
+    if end == "start":
+        o[0] = 1
+    else:
+        o[-1] = end
+    bad = graphs.Graph(n=g.n, off=off, adj=g.adj, off2=off2, adj2=g.adj2)
+    with pytest.raises(Q.QCError) as e:
+        Q.DeviceGraph.from_graph(bad)
+    assert e.value.status == 3 and which + " offsets" in str(e.value)
+
+
 def test_truncated_file_is_a_format_error():
     g = graphs.random_small(20, 0.3, 4)
     d = tempfile.mkdtemp()
