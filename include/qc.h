@@ -149,7 +149,8 @@ typedef struct {
     int32_t max_blocks;          /* cap on the persistent grid (share the GPU between
                                     contexts running at once); 0: every resident block */
     int32_t stage_max;           /* largest task (vertices) worked on in shared memory;
-                                    0: as large as the shared memory allows, -1: none */
+                                    0: the largest of 256, 192, 160, 128, 96, 64 whose
+                                    buffers fit 195 KB a block (L1 keeps 60 KB), -1: none */
     int32_t shared_order;        /* which donated task an idle warp takes: 1 the newest
                                     (depth first), 2 the oldest (the largest subtrees
                                     first); 0: newest for qc_mine, oldest for
