@@ -30,6 +30,14 @@ namespace qcb {
 // Inlining of the large-task path's and the register path's routines, left to
 // the compiler unless a build sets these (__noinline__ keeps one copy of a
 // routine that several call sites share, which shrinks the kernel's code).
+//
+// Every loop in those routines is kept rolled (`#pragma unroll 1`): the warps
+// of an SM run the large-task path, the register path and the scheduler at
+// once, and their code together overflows the instruction cache (instruction
+// fetch is the batched workload's top stall).  Rolled, the batch of 64
+// instances takes 108 ms instead of 136; config 1 is unchanged (1.165 against
+// 1.179 ms).  The scheduler's loops stay unrolled: rolling them too made
+// config 1 1.4 times slower.
 #ifndef QC_BIG_FN
 #define QC_BIG_FN
 #endif
@@ -335,9 +343,11 @@ __device__ QC_BOUNDS_FN int build_hist(const ExpandParams& P, const Rules& R, Ws
                           bool filter_valid, int m, const Bounds& b)
 {
     int lane = lane_id();
+    #pragma unroll 1
     for (int j = lane; j <= vmax + 1; j += 32) ws.hist()[j] = 0;
     __syncwarp();
     int cnt = 0;
+    #pragma unroll 1
     for (int base = 0; base < t; base += 32) {
         const uint32_t cw = cm[base >> 5];
         if (cw == 0) continue; // no vertex of this chunk (the word is the same in every lane)
@@ -359,6 +369,7 @@ __device__ QC_BOUNDS_FN int build_hist(const ExpandParams& P, const Rules& R, Ws
     // exclusive prefix over bins 0..vmax+1
     int carry = 0;
     long long carry_s = 0;
+    #pragma unroll 1
     for (int base = 0; base <= vmax + 1; base += 32) {
         int j = base + lane;
         int c = (j <= vmax + 1) ? ws.hist()[j] : 0;
@@ -419,6 +430,7 @@ __device__ QC_BOUNDS_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws
     // its members with that indegree, the smallest exdegree
     int mi = 0x7fffffff, mt = 0x7fffffff, me = 0x7fffffff;
     long long si = 0;
+    #pragma unroll 1
     for (int base = 0; base < t; base += 32) {
         const uint32_t mw = mm[base >> 5];
         if (mw == 0) continue;
@@ -454,6 +466,7 @@ __device__ QC_BOUNDS_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws
         if (lb < ub) {
             // first k in [lb, ub] with k == ub || sum_in + S(k) >= m*md[m+k]
             int idx = ub;
+            #pragma unroll 1
             for (int base = lb; base <= ub; base += 32) {
                 int k = base + lane;
                 bool ok = false;
@@ -473,6 +486,7 @@ __device__ QC_BOUNDS_FN bool lu_bounds(const ExpandParams& P, const Rules& R, Ws
             } else {
                 lb = idx;
                 int tub = idx;
+                #pragma unroll 1
                 for (int base = idx + 1; base <= ub; base += 32) {
                     int k = base + lane;
                     bool ok = (k <= ub) &&
@@ -501,6 +515,7 @@ __device__ QC_BIG_FN bool members_ok(const ExpandParams& P, const Rules& R, Ws& 
 {
     int lane = lane_id();
     int bad = 0;
+    #pragma unroll 1
     for (int base = 0; base < t; base += 32) {
         const uint32_t mw = mm[base >> 5];
         if (mw == 0) continue;
@@ -533,6 +548,7 @@ __device__ int compact(Ws& ws, const uint32_t* mask, int t)
 __device__ QC_BIG_FN void recount_exdeg(const TaskView& T, Ws& ws, const uint32_t* who, const uint32_t* R)
 {
     int n = compact(ws, who, T.t);
+    #pragma unroll 1
     for (int i = lane_id(); i < n; i += 32) {
         int v = ws.vlist()[i];
         ws.exdeg()[v] = popc_and(T.A1 + (int64_t)v * T.W, R, T.W);
@@ -545,6 +561,7 @@ __device__ QC_BIG_FN void filter_valid(const ExpandParams& P, const Rules& R, Ws
                              int m, const Bounds& b, uint32_t* out, uint32_t* rem)
 {
     int lane = lane_id();
+    #pragma unroll 1
     for (int base = 0; base < t; base += 32) {
         const uint32_t iw = in_mask[base >> 5];
         if (iw == 0) {
@@ -564,6 +581,7 @@ __device__ QC_BIG_FN void filter_valid(const ExpandParams& P, const Rules& R, Ws
             if (rem) rem[base >> 5] = br;
         }
     }
+    #pragma unroll 1
     for (int w = words_for(t) + lane; w < W; w += 32) {
         out[w] = 0;
         if (rem) rem[w] = 0;
@@ -596,10 +614,12 @@ __device__ QC_PRUNE_FN int degree_prune(const ExpandParams& P, const Rules& R, c
     if (!members_ok(P, R, ws, M, t, m, b)) return DP_INVALID;
     filter_valid(P, R, ws, D, t, W, m, b, Rm, nullptr);
     // X = Call \ Rm
+    #pragma unroll 1
     for (int w = lane_id(); w < W; w += 32) X[w] = Call[w] & ~Rm[w];
     __syncwarp();
     while (!bs_empty(Rm, W) && !bs_empty(X, W)) {
         if (may_switch && m + bs_count(Rm, W) <= 32) return DP_SWITCH;
+        #pragma unroll 1
         for (int w = lane_id(); w < W; w += 32) who[w] = M[w] | Rm[w];
         __syncwarp();
         recount_exdeg(T, ws, who, Rm);
@@ -649,6 +669,7 @@ __device__ QC_BIG_FN void emit_mask(const ExpandParams& P, const Rules& R, const
     if (at == ~0ull) return;
     if (lane == 0) P.results[at] = k;
     int written = 0;
+    #pragma unroll 1
     for (int base = 0; base < T.t; base += 32) {
         int v = base + lane;
         bool in = v < T.t && bit(mm, v);
@@ -668,6 +689,7 @@ __device__ QC_BIG_FN void check_clique(const ExpandParams& P, const Rules& R, co
     int lane = lane_id();
     int need = md_at(R, m);
     int bad = 0;
+    #pragma unroll 1
     for (int base = 0; base < T.t; base += 32) {
         int v = base + lane;
         if (v < T.t && bit(mm, v) && ws.indeg()[v] < need) bad = 1;
@@ -770,6 +792,7 @@ __device__ QC_SMALL_FN bool push_ranges(const ExpandParams& P, unsigned long lon
     if (lane == 0) atomicAdd(&P.ctl->pending, count);
     __syncwarp();
     int ok = 1;
+    #pragma unroll 1
     for (int c = lane; c < count; c += 32) {
         const int shard = (home + c) % kStackShards;
         const long long at = reserve_push(P, shard);
@@ -798,6 +821,7 @@ __device__ QC_SMALL_FN bool push_ranges(const ExpandParams& P, unsigned long lon
         }
         const int hi = hi_first - c * split;
         StackEntry e;
+        #pragma unroll 1
         for (int i = 0; i < kBundle; i++) e.rec[i] = 0;
         e.rec[0] = rec;
         e.n = 1;
@@ -951,6 +975,7 @@ __device__ QC_SMALL_FN int pop_item(const ExpandParams& P, Ws& ws, WorkItem& out
                 out.rec = e.rec[0];
                 out.q_lo = e.q_lo;
                 out.q_hi = e.q_hi;
+                #pragma unroll 1
                 for (int i = e.n - 1; i >= 1 && ws.sm->lcount < kLocalStack; i--) {
                     LocalTask lt{};
                     lt.rec = e.rec[i]; // header read and checked when taken
@@ -1025,6 +1050,7 @@ __device__ QC_SMALL_FN void donate(const ExpandParams& P, Ws& ws, int keep = 1)
         const int first = lane * per;
         const int k = give - first < per ? give - first : per;
         StackEntry e;
+        #pragma unroll 1
         for (int i = 0; i < kBundle; i++) e.rec[i] = i < k ? ws.sm->lstack[first + i].rec : 0ull;
         e.n = k;
         e.q_lo = -1;
@@ -1038,6 +1064,7 @@ __device__ QC_SMALL_FN void donate(const ExpandParams& P, Ws& ws, int keep = 1)
         // keep, in order, the tasks of bundles that were not pushed (a failed
         // push has stopped the run) and the tasks past the last bundle
         int keep = 0;
+        #pragma unroll 1
         for (int i = 0; i < n; i++) {
             const int b = i / per;
             if (i < give && b < nb && ((ok >> b) & 1u)) continue;
@@ -1212,14 +1239,18 @@ __device__ QC_BIG_FN void sort_keys(Ws& ws, int n)
     int lane = lane_id();
     int N = 1;
     while (N < n) N <<= 1;
+    #pragma unroll 1
     for (int i = n + lane; i < N; i += 32) {
         ws.khi()[i] = ~0ull;
         ws.klo()[i] = ~0ull;
         ws.sel()[i] = -1;
     }
     __syncwarp();
+    #pragma unroll 1
     for (int k = 2; k <= N; k <<= 1) {
+        #pragma unroll 1
         for (int j = k >> 1; j > 0; j >>= 1) {
+            #pragma unroll 1
             for (int i = lane; i < N; i += 32) {
                 int p = i ^ j;
                 if (p > i) {
@@ -1250,6 +1281,7 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     }
     // gather (key, position)
     int written = 0;
+    #pragma unroll 1
     for (int base = 0; base < T.t; base += 32) {
         int v = base + lane;
         bool isM = v < T.t && bit(M, v);
@@ -1276,9 +1308,11 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     const int32_t* order = ws.sel();
     if (tc <= kRankOrderMax) {
         int32_t* dst = ws.vlist();
+        #pragma unroll 1
         for (int e = lane; e < tc; e += 32) {
             const unsigned long long h = ws.khi()[e], l = ws.klo()[e];
             int r = 0;
+            #pragma unroll 1
             for (int j = 0; j < tc; j++) {
                 const unsigned long long hj = ws.khi()[j], lj = ws.klo()[j];
                 r += (hj < h || (hj == h && lj < l)) ? 1 : 0;
@@ -1313,6 +1347,7 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     int32_t* cl2 = (int32_t*)(rec + rec_l2_off(tc));
     uint32_t* c1 = (uint32_t*)(rec + rec_a1_off(tc));
     uint32_t* c2 = (uint32_t*)(rec + rec_a2_off(tc, Wc));
+    #pragma unroll 1
     for (int i = lane; i < tc; i += 32) {
         cid[i] = rec_ld(T.ids + order[i]);
         cl2[i] = 0;
@@ -1322,6 +1357,7 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
     // i0 + r, holds its parent row's words in registers and picks the child's
     // columns from them, the columns' parent positions passed round the warp.
     if (T.W <= 8) {
+        #pragma unroll 1
         for (int i0 = 0; i0 < tc; i0 += 32) {
             const int row = i0 + lane;
             const int src = row < tc ? order[row] : -1;
@@ -1332,10 +1368,12 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
                 a1w[w] = ok ? rec_ld(T.A1 + (int64_t)src * T.W + w) : 0u;
                 a2w[w] = ok ? rec_ld(T.A2 + (int64_t)src * T.W + w) : 0u;
             }
+            #pragma unroll 1
             for (int cw = 0; cw < Wc; cw++) {
                 const int jn = tc - cw * 32 < 32 ? tc - cw * 32 : 32;
                 const int my_col = lane < jn ? order[cw * 32 + lane] : 0;
                 uint32_t o1 = 0, o2 = 0;
+                #pragma unroll 1
                 for (int b = 0; b < jn; b++) {
                     const int pj = __shfl_sync(QC_FULL, my_col, b);
                     const int pw = pj >> 5, pb = pj & 31;
@@ -1359,11 +1397,13 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
         // Column word w: lane k holds the parent column order[w*32+k]; rows go by in
         // groups of 32 (lane r holds the parent row of child row i0+r), and the
         // reads of different rows do not depend on each other.
+        #pragma unroll 1
         for (int w = 0; w < Wc; w++) {
             const int j = w * 32 + lane;
             const int pj = j < tc ? order[j] : 0;
             const int pw = pj >> 5, pb = pj & 31;
             const bool col = j < tc;
+            #pragma unroll 1
             for (int i0 = 0; i0 < tc; i0 += 32) {
                 const int rows = tc - i0 < 32 ? tc - i0 : 32;
                 const int my_row = lane < rows ? order[i0 + lane] : 0;
@@ -1422,6 +1462,7 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
     int m1 = T.m + 1;
     // diameter pruning (main.cu:1709-1732): PRE & N2(q)
     const uint32_t* r2q = T.A2 + (int64_t)q * W;
+    #pragma unroll 1
     for (int w = lane; w < W; w += 32) D[w] = PRE[w] & rec_ld(r2q + w);
     __syncwarp();
     if (lane == 0) {
@@ -1432,16 +1473,19 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
     // members and the candidates that survive the diameter test are ever read
     {
         uint32_t* MD = ws.mk(MK_U);
+        #pragma unroll 1
         for (int w = lane; w < W; w += 32) MD[w] = M[w] | D[w];
         __syncwarp();
         int n = compact(ws, MD, t);
         // members are positions [0, m) and q, the earlier candidates [m, q):
         // both counts come from the row's words up to q's, read once
         const int mt = T.m, qw = q >> 5;
+        #pragma unroll 1
         for (int i = lane; i < n; i += 32) {
             int v = ws.vlist()[i];
             const uint32_t* row = T.A1 + (int64_t)v * W;
             int in = 0, ex = 0;
+            #pragma unroll 1
             for (int w = 0; w <= qw; w++) {
                 const uint32_t x = rec_ld(row + w);
                 in += __popc(x & range_word(w, 0, mt));
@@ -1469,17 +1513,21 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
 
     // critical-vertex pruning (main.cu:1526-1707)
     int critv = md_at(R, m1 + b.L);
+    #pragma unroll 1
     for (int base = 0; base < t; base += 32) {
         int v = base + lane;
         bool k = v < t && bit(M, v) && ws.indeg()[v] + ws.exdeg()[v] == critv && ws.exdeg()[v] > 0;
         unsigned bal = __ballot_sync(QC_FULL, k);
         if (lane == 0) Kc[base >> 5] = bal;
     }
+    #pragma unroll 1
     for (int w = words_for(t) + lane; w < W; w += 32) Kc[w] = 0;
     __syncwarp();
     // CA = R & OR over critical members of A1 rows
+    #pragma unroll 1
     for (int w = lane; w < W; w += 32) {
         uint32_t acc = 0;
+        #pragma unroll 1
         for (int base = 0; base < t; base += 32) {
             uint32_t kw = Kc[base >> 5];
             while (kw) {
@@ -1498,6 +1546,7 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
     if (nca > 0) {
         // add the critical-adjacent candidates; 2-hop counts to them
         int bad = 0;
+        #pragma unroll 1
         for (int base = 0; base < t; base += 32) {
             int v = base + lane;
             if (v < t && (bit(M, v) || bit(Rm, v))) {
@@ -1511,6 +1560,7 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
             }
         }
         if (__any_sync(QC_FULL, bad)) return;
+        #pragma unroll 1
         for (int w = lane; w < W; w += 32) {
             M[w] |= CA[w];
             C2[w] = Rm[w] & ~CA[w];
@@ -1518,12 +1568,14 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
         __syncwarp();
         m2 = m1 + nca;
         // diameter pruning against the added vertices (main.cu:1689-1697)
+        #pragma unroll 1
         for (int base = 0; base < t; base += 32) {
             int v = base + lane;
             bool in = v < t && bit(C2, v) && ws.aux()[v] == nca;
             unsigned bal = __ballot_sync(QC_FULL, in);
             if (lane == 0) D2[base >> 5] = bal;
         }
+        #pragma unroll 1
         for (int w = words_for(t) + lane; w < W; w += 32) D2[w] = 0;
         __syncwarp();
     } else {
@@ -1635,6 +1687,7 @@ __device__ QC_SMALL_FN bool lu_small(const ExpandParams& P, const Rules& R, unsi
     b.med = mindeg<true>(R, m + 1);
     if (min_in < md_at<true>(R, m)) {
         int lb = mindeg<true>(R, m) - min_in;
+        #pragma unroll 1
         for (int base = lb;; base += 32) {
             int L = base + lane;
             bool cont = (L <= min_in_ex) && (min_in + L < md_at<true>(R, m + L));
@@ -1736,7 +1789,9 @@ __device__ QC_SMALL_FN void emit_flush(const ExpandParams& P, Ws& ws)
     at = __shfl_sync(QC_FULL, at, 0);
     idx = __shfl_sync(QC_FULL, idx, 0);
     if (at != ~0ull) {
+        #pragma unroll 1
         for (int i = lane; i < n; i += 32) P.results[at + i] = ws.sm->ebuf[i];
+        #pragma unroll 1
         for (int j = lane; j < ns; j += 32) P.set_starts[idx + j] = at + ws.sm->eset[j];
     }
     __syncwarp();
@@ -1791,7 +1846,9 @@ __device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, W
               ((unsigned)(31 - T.l2) << 10) | ((unsigned)T.idr << 5) | (unsigned)lane;
     }
     // bitonic sort ascending
+    #pragma unroll 1
     for (int k = 2; k <= 32; k <<= 1)
+        #pragma unroll 1
         for (int j = k >> 1; j > 0; j >>= 1) {
             const unsigned o = __shfl_xor_sync(QC_FULL, key, j);
             const bool up = (lane & k) == 0;
@@ -1810,6 +1867,7 @@ __device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, W
     const unsigned ranks = ror(lane < tc ? 1u << prank : 0u);
     const int crank = __popc(ranks & ((1u << prank) - 1u));
     unsigned c1 = 0, c2 = 0;
+    #pragma unroll 1
     for (int j = 0; j < tc; j++) {
         int pj = __shfl_sync(QC_FULL, src, j);
         c1 |= ((sa1 >> pj) & 1u) << j;
@@ -1933,6 +1991,7 @@ __device__ QC_SMALL_FN void branch_rest_small(const ExpandParams& P, const Rules
     const int lane = lane_id();
     const int W = T.W;
     uint32_t* S = ws.mk(MK_U);
+    #pragma unroll 1
     for (int w = lane; w < W; w += 32) S[w] = M[w] | Rm[w];
     __syncwarp();
     const int n = compact(ws, S, T.t); // m1 + |Rm| <= 32
@@ -1949,6 +2008,7 @@ __device__ QC_SMALL_FN void branch_rest_small(const ExpandParams& P, const Rules
     const uint32_t* r1 = T.A1 + (int64_t)pos * W;
     const uint32_t* r2 = T.A2 + (int64_t)pos * W;
     unsigned a1 = 0, a2 = 0;
+    #pragma unroll 1
     for (int j = 0; j < n; j++) {
         const int pj = __shfl_sync(QC_FULL, pos, j);
         if (act) {
@@ -1959,6 +2019,7 @@ __device__ QC_SMALL_FN void branch_rest_small(const ExpandParams& P, const Rules
     C.a1 = a1;
     C.a2 = a2;
     int idr = 0, l2r = 0;
+    #pragma unroll 1
     for (int j = 0; j < 32; j++) {
         const int oid = __shfl_sync(QC_FULL, C.id, j);
         const int ol2 = __shfl_sync(QC_FULL, l2v, j);
@@ -2073,6 +2134,7 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
             int k = need - in;
             if (k > 0) {
                 unsigned x = T.a1 & Cm;
+                #pragma unroll 1
                 for (int s = 1; s < k; s++) x &= x - 1;
                 pos = x ? __ffs(x) - 1 : t - 1;
             }
@@ -2113,11 +2175,13 @@ __device__ QC_SMALL_FN bool process_small(const ExpandParams& P, const Rules& R,
         return false;
     }
     if (!ranked) {
+        #pragma unroll 1
         for (int j = 0; j < 32; j++) {
             const int o = __shfl_sync(QC_FULL, T.id, j);
             T.idr += (j < t && o > T.id) ? 1 : 0;
         }
     }
+    #pragma unroll 1
     for (int q = qhi; q >= qlo; q--) {
         // a sharded search's root: only this shard's branches
         if (sroot && (t - 1 - q) % P.nshards != P.shard) continue;
@@ -2204,6 +2268,7 @@ __device__ QC_BIG_FN bool stage_record(const ExpandParams& P, WarpSmem* sm, Task
 #else
     const uint4* s4 = (const uint4*)src;
     uint4* d4 = (uint4*)buf;
+    #pragma unroll 1
     for (uint64_t i = lane_id(); i < body / 16; i += 32) d4[i] = __ldcg(s4 + i);
     __syncwarp();
 #endif
