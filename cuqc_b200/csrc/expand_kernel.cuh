@@ -31,13 +31,16 @@ namespace qcb {
 // the compiler unless a build sets these (__noinline__ keeps one copy of a
 // routine that several call sites share, which shrinks the kernel's code).
 //
-// Every loop in those routines is kept rolled (`#pragma unroll 1`): the warps
+// The loops in those routines are kept rolled (`#pragma unroll 1`): the warps
 // of an SM run the large-task path, the register path and the scheduler at
 // once, and their code together overflows the instruction cache (instruction
 // fetch is the batched workload's top stall).  Rolled, the batch of 64
-// instances takes 108 ms instead of 136; config 1 is unchanged (1.165 against
-// 1.179 ms).  The scheduler's loops stay unrolled: rolling them too made
-// config 1 1.4 times slower.
+// instances takes 113 ms instead of 137; config 1 is unchanged (1.14 against
+// 1.15 ms).  Left to the compiler: the loops over a row's words (the degree
+// counts of a branch and the child's row compaction), which stream the rows
+// of tasks of thousands of vertices with several loads in flight, the child's
+// rank count over its keys, and the scheduler's loops (rolling those too made
+// config 1 1.4 times slower).
 #ifndef QC_BIG_FN
 #define QC_BIG_FN
 #endif
@@ -1312,7 +1315,6 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
         for (int e = lane; e < tc; e += 32) {
             const unsigned long long h = ws.khi()[e], l = ws.klo()[e];
             int r = 0;
-            #pragma unroll 1
             for (int j = 0; j < tc; j++) {
                 const unsigned long long hj = ws.khi()[j], lj = ws.klo()[j];
                 r += (hj < h || (hj == h && lj < l)) ? 1 : 0;
@@ -1368,12 +1370,10 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
                 a1w[w] = ok ? rec_ld(T.A1 + (int64_t)src * T.W + w) : 0u;
                 a2w[w] = ok ? rec_ld(T.A2 + (int64_t)src * T.W + w) : 0u;
             }
-            #pragma unroll 1
             for (int cw = 0; cw < Wc; cw++) {
                 const int jn = tc - cw * 32 < 32 ? tc - cw * 32 : 32;
                 const int my_col = lane < jn ? order[cw * 32 + lane] : 0;
                 uint32_t o1 = 0, o2 = 0;
-                #pragma unroll 1
                 for (int b = 0; b < jn; b++) {
                     const int pj = __shfl_sync(QC_FULL, my_col, b);
                     const int pw = pj >> 5, pb = pj & 31;
@@ -1397,7 +1397,6 @@ __device__ QC_BIG_FN void write_child(const ExpandParams& P, const Rules& R, con
         // Column word w: lane k holds the parent column order[w*32+k]; rows go by in
         // groups of 32 (lane r holds the parent row of child row i0+r), and the
         // reads of different rows do not depend on each other.
-        #pragma unroll 1
         for (int w = 0; w < Wc; w++) {
             const int j = w * 32 + lane;
             const int pj = j < tc ? order[j] : 0;
@@ -1485,7 +1484,6 @@ __device__ QC_BIG_FN void expand_branch(const ExpandParams& P, const Rules& R, c
             int v = ws.vlist()[i];
             const uint32_t* row = T.A1 + (int64_t)v * W;
             int in = 0, ex = 0;
-            #pragma unroll 1
             for (int w = 0; w <= qw; w++) {
                 const uint32_t x = rec_ld(row + w);
                 in += __popc(x & range_word(w, 0, mt));
@@ -1867,7 +1865,6 @@ __device__ QC_SMALL_FN void child_small(const ExpandParams& P, const Rules& R, W
     const unsigned ranks = ror(lane < tc ? 1u << prank : 0u);
     const int crank = __popc(ranks & ((1u << prank) - 1u));
     unsigned c1 = 0, c2 = 0;
-    #pragma unroll 1
     for (int j = 0; j < tc; j++) {
         int pj = __shfl_sync(QC_FULL, src, j);
         c1 |= ((sa1 >> pj) & 1u) << j;
