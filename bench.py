@@ -296,12 +296,15 @@ def run_batch(args, standalone=True):
     gms = [float(x[1]) for x in inst]
     mss = [x[2] for x in inst]
     # the batched launch on its own context, its settings picked by the
-    # library's tuner (qc_tune_batch) on the first 32 instances; the plain
-    # launches on another context with the defaults
+    # library's tuner (qc_tune_batch) on the first 64 instances, each candidate
+    # timed twice after a warm-up (a sample of 32 timed once picked 4 or 8
+    # warps a block from run to run); the plain launches on another context
+    # with the defaults
     ctx = Q.Context(device=0)
     pctx = Q.Context(device=0)
     dgs = [Q.DeviceGraph.from_graph(g) for g in gs]
-    tuned = ctx.tune_batch(dgs[:32], gms[:32], mss[:32], repeats=1) if args.tune else None
+    ns = min(64, len(dgs))
+    tuned = ctx.tune_batch(dgs[:ns], gms[:ns], mss[:ns], repeats=2) if args.tune else None
     dev = torch.device("cuda", 0)
     streams = {id(ctx): torch.cuda.ExternalStream(ctx.stream, device=dev),
                id(pctx): torch.cuda.ExternalStream(pctx.stream, device=dev)}
